@@ -1,0 +1,228 @@
+/* C ABI of the B200 cloth hot path.
+ *
+ * This is the drop-in boundary for the per-step simulation path of
+ * iiiian/silk_physics: each entry point replaces one method of silk::World
+ * (silk/include/silk/silk.hpp:83-239, implemented by
+ * silk/src/backend/cuda/cuda_backend.cu) with plain pointers and sizes.
+ * Spans become (pointer, element count) pairs, handles stay opaque uint32
+ * values (0 = failure), and every call returns a silk_status that maps 1:1
+ * onto silk::ErrorCode (silk/include/silk/result.hpp:22-35) shifted by one
+ * so that 0 means success.  Nothing here throws across the ABI.
+ *
+ * Calls are synchronous like the reference's (cuda_backend.cu:87-96): the
+ * world's stream is synchronised before a call returns.  A world is not
+ * thread-safe.
+ */
+#ifndef SILK_B200_H
+#define SILK_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct silk_world silk_world;
+
+/* silk::ErrorCode + 1; SILK_OK == 0. */
+typedef enum {
+  SILK_OK = 0,
+  SILK_ERR_UNKNOWN = 1,
+  SILK_ERR_NOT_INITIALIZED = 2,
+  SILK_ERR_INVALID_CONFIG = 3,
+  SILK_ERR_TOO_MANY_BODY = 4,
+  SILK_ERR_INVALID_HANDLE = 5,
+  SILK_ERR_INVALID_MESH = 6,
+  SILK_ERR_INVALID_PIN = 7,
+  SILK_ERR_INVALID_POSITION = 8,
+  SILK_ERR_CHOLESKY_DECOMPOSITION_FAIL = 9,
+  SILK_ERR_NEED_INIT_SOLVER_FIRST = 10,
+  SILK_ERR_ITERATIVE_SOLVE_FAIL = 11,
+  SILK_ERR_NO_CUDA_SUPPORT = 12
+} silk_status;
+
+/* silk::Backend (silk.hpp:80). Only SILK_BACKEND_GPU is provided. */
+typedef enum { SILK_BACKEND_CPU = 0, SILK_BACKEND_GPU = 1 } silk_backend;
+
+/* silk::GlobalConfig (silk.hpp:47-77), same field order and defaults. */
+typedef struct {
+  float acceleration_x;          /* 0 */
+  float acceleration_y;          /* 0 */
+  float acceleration_z;          /* -10 */
+  int32_t max_outer_iteration;   /* 100 */
+  int32_t max_inner_iteration;   /* 100 */
+  float dt;                      /* 1/60 */
+  float linear_solver_abs_tol;   /* 1e-7 */
+  float linear_solver_rel_tol_min; /* 1e-6 */
+  float linear_solver_rel_tol_max; /* 1e-3 */
+  float initial_linear_rel_tol;  /* 1e-2 */
+  float admm_abs_tol;            /* 1e-5 */
+  float admm_rel_tol;            /* 1e-3 */
+} silk_global_config;
+
+/* silk::ClothConfig (silk.hpp:35-45). */
+typedef struct {
+  float elastic_stiffness; /* 100 */
+  float bending_stiffness; /* 1e-4 */
+  float density;           /* 0.1 */
+  float damping;           /* 0.01 */
+} silk_cloth_config;
+
+/* silk::CollisionConfig (silk.hpp:26-33); bools as int32. */
+typedef struct {
+  int32_t is_collision_on;      /* 1 */
+  int32_t is_self_collision_on; /* 1 */
+  int32_t group;                /* 0 */
+  float restitution;            /* 0.3 */
+  float friction;               /* 0.3 */
+} silk_collision_config;
+
+/* Solver options with no field in silk::GlobalConfig (bench and precision
+ * switches).  Defaults reproduce the reference behaviour. */
+typedef struct {
+  float fixed_linear_rel_tol; /* > 0: CG relative tolerance fixed (1e-5 in
+                                 the headline benchmark); 0: adaptive rule of
+                                 admm_solver.cu:228-233 */
+  int32_t cg_max_iter;        /* 1000 (mas_cg_solver.cuh:25) */
+  int32_t mas_bf16;           /* 0: FP32 bank inverses; 1: BF16 storage */
+  int32_t reserved[5];
+} silk_solver_options;
+
+/* Statistics of the last solver_step. */
+typedef struct {
+  int32_t outer_iterations;
+  int32_t admm_iterations;
+  int32_t cg_iterations;
+  int32_t cg_solves;
+  int32_t contacts;
+  int32_t colors;
+  int32_t ccd_queries;
+  int32_t ccd_hits;
+  float min_toi;
+  int32_t broadphase_candidates;
+  int64_t kernel_launches;
+  int32_t reserved[6];
+} silk_step_stats;
+
+/* --- World lifetime (silk.hpp:92-100) ---------------------------------- */
+silk_world* silk_world_create(void);
+void silk_world_destroy(silk_world* w);
+/* Human-readable detail of the last error of this world ("" if none). */
+const char* silk_world_last_error(const silk_world* w);
+
+/* --- Global API (silk.hpp:106-118; world.cpp:29-56) --------------------- */
+silk_status silk_world_init(silk_world* w, int32_t backend);
+silk_status silk_set_global_config(silk_world* w, const silk_global_config* c);
+void silk_global_config_default(silk_global_config* c);
+void silk_clear(silk_world* w);
+
+/* --- Solver API (silk.hpp:124-133) -------------------------------------- */
+silk_status silk_solver_step(silk_world* w);
+silk_status silk_solver_reset(silk_world* w);
+
+/* --- Cloth API (silk.hpp:139-204) --------------------------------------- */
+silk_status silk_add_cloth(silk_world* w, const silk_cloth_config* cloth,
+                           const silk_collision_config* collision,
+                           const float* verts, int64_t verts_len,
+                           const int32_t* faces, int64_t faces_len,
+                           const int32_t* pins, int64_t pins_len,
+                           uint32_t* handle);
+silk_status silk_remove_cloth(silk_world* w, uint32_t handle);
+silk_status silk_get_cloth_position(const silk_world* w, uint32_t handle,
+                                    float* position, int64_t position_len);
+silk_status silk_set_cloth_config(silk_world* w, uint32_t handle,
+                                  const silk_cloth_config* config);
+silk_status silk_set_cloth_collision_config(silk_world* w, uint32_t handle,
+                                            const silk_collision_config* c);
+silk_status silk_set_cloth_pin_index(silk_world* w, uint32_t handle,
+                                     const int32_t* pins, int64_t pins_len);
+silk_status silk_set_cloth_pin_position(silk_world* w, uint32_t handle,
+                                        const float* position,
+                                        int64_t position_len);
+
+/* --- Obstacle API (silk.hpp:210-239) ------------------------------------ */
+silk_status silk_add_obstacle(silk_world* w,
+                              const silk_collision_config* collision,
+                              const float* verts, int64_t verts_len,
+                              const int32_t* faces, int64_t faces_len,
+                              uint32_t* handle);
+silk_status silk_remove_obstacle(silk_world* w, uint32_t handle);
+silk_status silk_set_obstacle_collision_config(silk_world* w, uint32_t handle,
+                                               const silk_collision_config* c);
+silk_status silk_set_obstacle_position(silk_world* w, uint32_t handle,
+                                       const float* position,
+                                       int64_t position_len);
+
+/* --- Extensions (no reference counterpart) ------------------------------ */
+void silk_solver_options_default(silk_solver_options* o);
+silk_status silk_set_solver_options(silk_world* w, const silk_solver_options* o);
+silk_status silk_get_step_stats(const silk_world* w, silk_step_stats* s);
+/* Launch all device work of this world on the given cudaStream_t (NULL =
+ * the world's own stream).  Lets a caller time steps with its own events. */
+silk_status silk_set_stream(silk_world* w, void* cuda_stream);
+
+/* --- Inspection entry points used by the parity tests ------------------- */
+/* Solver-order permutation (original -> solver) and partition offsets. */
+silk_status silk_debug_cloth_partition(const silk_world* w, uint32_t handle,
+                                       int32_t* perm, int64_t perm_len,
+                                       int32_t* part_offsets,
+                                       int64_t offsets_cap, int32_t* nparts);
+/* Scalar system matrix L (H = L (x) I3) as dense row-major, solver order. */
+silk_status silk_debug_cloth_matrix(const silk_world* w, uint32_t handle,
+                                    double* dense, int64_t n_len);
+/* Refit every collider to (t0 = current state, t1 = current + disp) where
+ * disp is per cloth in original vertex order, concatenated. */
+silk_status silk_debug_refit(silk_world* w, const float* disp,
+                             int64_t disp_len);
+/* Broadphase candidates of the current refit: rows of
+ * (kind, object_a, index_a, object_b, index_b); returns count in *n. */
+silk_status silk_debug_candidates(silk_world* w, int32_t* out, int64_t cap,
+                                  int32_t* n);
+/* DCD contact keys at collider time t: rows of (type, obj_a, obj_b, i0..i3)
+ * sorted; count in *n. */
+silk_status silk_debug_dcd(silk_world* w, float t, float activation,
+                           int32_t* keys, int64_t cap, int32_t* n);
+/* Minimum time of impact over the current refit. */
+silk_status silk_debug_min_toi(silk_world* w, float time_start,
+                               float max_time, float min_separation,
+                               float* toi, int32_t* n_queries,
+                               int32_t* n_hits);
+
+/* --- Host-side setup (no GPU needed) ------------------------------------ */
+/* Vertex partition used as the MAS banks: connected parts of <= 32
+ * vertices (replaces MeshPartition, backend/cuda/mesh_partition.cu:56-105,
+ * whose KaMinPar/METIS partitioner is not available here). */
+silk_status silk_partition_mesh(const float* verts, int64_t verts_len,
+                                const int32_t* faces, int64_t faces_len,
+                                int32_t* perm, int32_t* part_offsets,
+                                int64_t offsets_cap, int32_t* nparts);
+/* Static assembly of one cloth in solver order (ClothAssemblyL2Cache +
+ * ClothAssemblyL1Cache, cloth_assembly_l2_cache.cpp:71-136,
+ * cloth_assembly_l1_cache.cu:16-97): dense scalar matrix L (nv x nv, may be
+ * NULL), mass (nv), contact weight (nv), bending rhs (3 nv). */
+silk_status silk_assemble_cloth_host(const silk_cloth_config* cloth,
+                                     const float* verts, int64_t verts_len,
+                                     const int32_t* faces, int64_t faces_len,
+                                     float dt, double* dense_L, double* mass,
+                                     double* contact_weight,
+                                     double* bending_rhs);
+
+/* --- Standalone operators ---------------------------------------------- */
+/* Tight-Inclusion CCD of n queries on the GPU.  x: n x 24 floats (4 points
+ * at t0 then 4 at t1; point-triangle: point first).  Writes hit (0/1) and
+ * the time of impact (lower bound of the accepted interval; the refined
+ * minimum-separation interval when the first starts at 0). */
+silk_status silk_ccd_batch(int32_t is_vertex_face, const float* x, int64_t n,
+                           const float* err3, const float* min_separation,
+                           float tolerance, int32_t max_iter, float max_time,
+                           int32_t* hit, float* toi, float* t_upper);
+/* Contact colouring of n contacts given 4 vertex ids each (-1 = immovable)
+ * and 64-bit priorities: greedy colouring in decreasing priority order. */
+silk_status silk_color_contacts(const int32_t* verts4, const uint64_t* prio,
+                                int64_t n, int32_t* colors, int32_t* ncolors);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SILK_B200_H */

@@ -1,0 +1,332 @@
+// extern "C" boundary: every entry point of include/silk_b200.h.  Exceptions
+// never cross the ABI; they become SILK_ERR_UNKNOWN with a detail string.
+#include <cstring>
+#include <exception>
+
+#include "../../include/silk_b200.h"
+#include "collision.cuh"
+#include "world.hpp"
+
+using silkb::World;
+
+struct silk_world {
+  World impl;
+};
+
+namespace {
+
+template <class F>
+silk_status guard(silk_world* w, F&& f) {
+  if (!w) return SILK_ERR_INVALID_CONFIG;
+  try {
+    return f(w->impl);
+  } catch (const std::exception& e) {
+    w->impl.last_error = e.what();
+    return SILK_ERR_UNKNOWN;
+  }
+}
+
+template <class F>
+silk_status guard_init(silk_world* w, F&& f) {
+  if (!w) return SILK_ERR_INVALID_CONFIG;
+  if (!w->impl.initialized) return SILK_ERR_NOT_INITIALIZED;
+  return guard(w, f);
+}
+
+}  // namespace
+
+extern "C" {
+
+silk_world* silk_world_create(void) {
+  try {
+    return new silk_world();
+  } catch (...) {
+    return nullptr;
+  }
+}
+
+void silk_world_destroy(silk_world* w) { delete w; }
+
+const char* silk_world_last_error(const silk_world* w) {
+  return w ? w->impl.last_error.c_str() : "";
+}
+
+void silk_global_config_default(silk_global_config* c) {
+  c->acceleration_x = 0.0f;
+  c->acceleration_y = 0.0f;
+  c->acceleration_z = -10.0f;
+  c->max_outer_iteration = 100;
+  c->max_inner_iteration = 100;
+  c->dt = 1.0f / 60.0f;
+  c->linear_solver_abs_tol = 1e-7f;
+  c->linear_solver_rel_tol_min = 1e-6f;
+  c->linear_solver_rel_tol_max = 1e-3f;
+  c->initial_linear_rel_tol = 1e-2f;
+  c->admm_abs_tol = 1e-5f;
+  c->admm_rel_tol = 1e-3f;
+}
+
+void silk_solver_options_default(silk_solver_options* o) {
+  std::memset(o, 0, sizeof(*o));
+  o->fixed_linear_rel_tol = 0.0f;
+  o->cg_max_iter = 1000;
+  o->mas_bf16 = 0;
+}
+
+silk_status silk_world_init(silk_world* w, int32_t backend) {
+  return guard(w, [&](World& W) { return W.init(backend); });
+}
+
+silk_status silk_set_global_config(silk_world* w, const silk_global_config* c) {
+  if (!c) return SILK_ERR_INVALID_CONFIG;
+  return guard_init(w, [&](World& W) { return W.set_global_config(*c); });
+}
+
+void silk_clear(silk_world* w) {
+  if (w) w->impl.clear();
+}
+
+silk_status silk_solver_step(silk_world* w) {
+  return guard_init(w, [&](World& W) { return W.solver_step(); });
+}
+
+silk_status silk_solver_reset(silk_world* w) {
+  return guard_init(w, [&](World& W) { return W.solver_reset(); });
+}
+
+silk_status silk_add_cloth(silk_world* w, const silk_cloth_config* cloth,
+                           const silk_collision_config* collision,
+                           const float* verts, int64_t verts_len,
+                           const int32_t* faces, int64_t faces_len,
+                           const int32_t* pins, int64_t pins_len,
+                           uint32_t* handle) {
+  if (handle) *handle = 0;
+  if (!cloth || !collision || !handle) return SILK_ERR_INVALID_CONFIG;
+  return guard_init(w, [&](World& W) {
+    return W.add_cloth(*cloth, *collision, verts, verts_len, faces, faces_len,
+                       pins, pins_len, handle);
+  });
+}
+
+silk_status silk_remove_cloth(silk_world* w, uint32_t handle) {
+  return guard_init(w, [&](World& W) { return W.remove_cloth(handle); });
+}
+
+silk_status silk_get_cloth_position(const silk_world* w, uint32_t handle,
+                                    float* position, int64_t position_len) {
+  silk_world* mw = const_cast<silk_world*>(w);
+  if (!position && position_len != 0) return SILK_ERR_INVALID_POSITION;
+  return guard_init(mw, [&](World& W) {
+    return W.get_cloth_position(handle, position, position_len);
+  });
+}
+
+silk_status silk_set_cloth_config(silk_world* w, uint32_t handle,
+                                  const silk_cloth_config* config) {
+  if (!config) return SILK_ERR_INVALID_CONFIG;
+  return guard_init(w, [&](World& W) { return W.set_cloth_config(handle, *config); });
+}
+
+silk_status silk_set_cloth_collision_config(silk_world* w, uint32_t handle,
+                                            const silk_collision_config* c) {
+  if (!c) return SILK_ERR_INVALID_CONFIG;
+  return guard_init(w, [&](World& W) {
+    return W.set_cloth_collision_config(handle, *c);
+  });
+}
+
+silk_status silk_set_cloth_pin_index(silk_world* w, uint32_t handle,
+                                     const int32_t* pins, int64_t pins_len) {
+  if (!pins && pins_len != 0) return SILK_ERR_INVALID_PIN;
+  return guard_init(w, [&](World& W) {
+    return W.set_cloth_pin_index(handle, pins, pins_len);
+  });
+}
+
+silk_status silk_set_cloth_pin_position(silk_world* w, uint32_t handle,
+                                        const float* position,
+                                        int64_t position_len) {
+  if (!position && position_len != 0) return SILK_ERR_INVALID_PIN;
+  return guard_init(w, [&](World& W) {
+    return W.set_cloth_pin_position(handle, position, position_len);
+  });
+}
+
+silk_status silk_add_obstacle(silk_world* w,
+                              const silk_collision_config* collision,
+                              const float* verts, int64_t verts_len,
+                              const int32_t* faces, int64_t faces_len,
+                              uint32_t* handle) {
+  if (handle) *handle = 0;
+  if (!collision || !handle) return SILK_ERR_INVALID_CONFIG;
+  return guard_init(w, [&](World& W) {
+    return W.add_obstacle(*collision, verts, verts_len, faces, faces_len, handle);
+  });
+}
+
+silk_status silk_remove_obstacle(silk_world* w, uint32_t handle) {
+  return guard_init(w, [&](World& W) { return W.remove_obstacle(handle); });
+}
+
+silk_status silk_set_obstacle_collision_config(silk_world* w, uint32_t handle,
+                                               const silk_collision_config* c) {
+  if (!c) return SILK_ERR_INVALID_CONFIG;
+  return guard_init(w, [&](World& W) {
+    return W.set_obstacle_collision_config(handle, *c);
+  });
+}
+
+silk_status silk_set_obstacle_position(silk_world* w, uint32_t handle,
+                                       const float* position,
+                                       int64_t position_len) {
+  if (!position && position_len != 0) return SILK_ERR_INVALID_POSITION;
+  return guard_init(w, [&](World& W) {
+    return W.set_obstacle_position(handle, position, position_len);
+  });
+}
+
+silk_status silk_set_solver_options(silk_world* w, const silk_solver_options* o) {
+  if (!o) return SILK_ERR_INVALID_CONFIG;
+  return guard(w, [&](World& W) { return W.set_solver_options(*o); });
+}
+
+silk_status silk_get_step_stats(const silk_world* w, silk_step_stats* s) {
+  if (!w || !s) return SILK_ERR_INVALID_CONFIG;
+  *s = w->impl.stats;
+  return SILK_OK;
+}
+
+silk_status silk_set_stream(silk_world* w, void* cuda_stream) {
+  return guard_init(w, [&](World& W) { return W.set_stream(cuda_stream); });
+}
+
+silk_status silk_debug_cloth_partition(const silk_world* w, uint32_t handle,
+                                       int32_t* perm, int64_t perm_len,
+                                       int32_t* part_offsets,
+                                       int64_t offsets_cap, int32_t* nparts) {
+  return guard_init(const_cast<silk_world*>(w), [&](World& W) {
+    return W.debug_partition(handle, perm, perm_len, part_offsets, offsets_cap,
+                             nparts);
+  });
+}
+
+silk_status silk_debug_cloth_matrix(const silk_world* w, uint32_t handle,
+                                    double* dense, int64_t n_len) {
+  return guard_init(const_cast<silk_world*>(w), [&](World& W) {
+    return W.debug_matrix(handle, dense, n_len);
+  });
+}
+
+silk_status silk_debug_refit(silk_world* w, const float* disp, int64_t len) {
+  return guard_init(w, [&](World& W) { return W.debug_refit(disp, len); });
+}
+
+silk_status silk_debug_candidates(silk_world* w, int32_t* out, int64_t cap,
+                                  int32_t* n) {
+  return guard_init(w, [&](World& W) { return W.debug_candidates(out, cap, n); });
+}
+
+silk_status silk_debug_dcd(silk_world* w, float t, float activation,
+                           int32_t* keys, int64_t cap, int32_t* n) {
+  return guard_init(w, [&](World& W) {
+    return W.debug_dcd(t, activation, keys, cap, n);
+  });
+}
+
+silk_status silk_debug_min_toi(silk_world* w, float time_start, float max_time,
+                               float min_separation, float* toi,
+                               int32_t* n_queries, int32_t* n_hits) {
+  return guard_init(w, [&](World& W) {
+    return W.debug_min_toi(time_start, max_time, min_separation, toi, n_queries,
+                           n_hits);
+  });
+}
+
+silk_status silk_partition_mesh(const float* verts, int64_t verts_len,
+                                const int32_t* faces, int64_t faces_len,
+                                int32_t* perm, int32_t* part_offsets,
+                                int64_t offsets_cap, int32_t* nparts) {
+  if (!verts || !faces || !perm || !part_offsets || !nparts)
+    return SILK_ERR_INVALID_CONFIG;
+  try {
+    std::vector<int> p, off;
+    int nv = (int)(verts_len / 3), nf = (int)(faces_len / 3);
+    silkb::partition_mesh(verts, nv, faces, nf, p, off);
+    *nparts = (int)off.size() - 1;
+    if ((int64_t)off.size() > offsets_cap) return SILK_ERR_INVALID_CONFIG;
+    std::memcpy(perm, p.data(), sizeof(int) * nv);
+    std::memcpy(part_offsets, off.data(), sizeof(int) * off.size());
+    return SILK_OK;
+  } catch (...) {
+    return SILK_ERR_UNKNOWN;
+  }
+}
+
+silk_status silk_assemble_cloth_host(const silk_cloth_config* cloth,
+                                     const float* verts, int64_t verts_len,
+                                     const int32_t* faces, int64_t faces_len,
+                                     float dt, double* dense_L, double* mass,
+                                     double* contact_weight,
+                                     double* bending_rhs) {
+  if (!cloth || !verts || !faces) return SILK_ERR_INVALID_CONFIG;
+  try {
+    std::string why = silkb::check_cloth_mesh(verts, verts_len, faces, faces_len);
+    if (!why.empty()) return SILK_ERR_INVALID_MESH;
+    silkb::ClothParams prm;
+    prm.elastic_stiffness = cloth->elastic_stiffness;
+    prm.bending_stiffness = cloth->bending_stiffness;
+    prm.density = cloth->density;
+    prm.damping = cloth->damping;
+    silkb::ClothSetup S;
+    silkb::build_cloth_setup(verts, (int)(verts_len / 3), faces,
+                             (int)(faces_len / 3), prm, S);
+    int nv = S.nv;
+    if (dense_L) {
+      std::memset(dense_L, 0, sizeof(double) * (size_t)nv * nv);
+      for (int i = 0; i < nv; ++i)
+        for (int k = S.Lrows[i]; k < S.Lrows[i + 1]; ++k)
+          dense_L[(size_t)i * nv + S.Lcols[k]] = S.Lvals[k];
+    }
+    if (mass)
+      for (int i = 0; i < nv; ++i) mass[i] = S.mass[i];
+    if (contact_weight) {
+      std::vector<double> w;
+      silkb::contact_weights(S, dt, w);
+      for (int i = 0; i < nv; ++i) contact_weight[i] = w[i];
+    }
+    if (bending_rhs)
+      for (int i = 0; i < 3 * nv; ++i) bending_rhs[i] = S.bending_rhs[i];
+    return SILK_OK;
+  } catch (...) {
+    return SILK_ERR_UNKNOWN;
+  }
+}
+
+silk_status silk_ccd_batch(int32_t is_vertex_face, const float* x, int64_t n,
+                           const float* err3, const float* min_separation,
+                           float tolerance, int32_t max_iter, float max_time,
+                           int32_t* hit, float* toi, float* t_upper) {
+  if (n < 0 || (n > 0 && (!x || !err3 || !min_separation || !hit || !toi)))
+    return SILK_ERR_INVALID_CONFIG;
+  try {
+    silkb::ccd_batch_host(is_vertex_face != 0, x, n, err3, min_separation,
+                          tolerance, max_iter, max_time, hit, toi, t_upper);
+    return SILK_OK;
+  } catch (...) {
+    return SILK_ERR_UNKNOWN;
+  }
+}
+
+silk_status silk_color_contacts(const int32_t* verts4, const uint64_t* prio,
+                                int64_t n, int32_t* colors, int32_t* ncolors) {
+  if (n < 0 || (n > 0 && (!verts4 || !prio || !colors)) || !ncolors)
+    return SILK_ERR_INVALID_CONFIG;
+  try {
+    *ncolors = silkb::color_contacts_host(verts4, prio, n, colors);
+    return *ncolors >= 0 ? SILK_OK : SILK_ERR_UNKNOWN;
+  } catch (...) {
+    return SILK_ERR_UNKNOWN;
+  }
+}
+
+}  // extern "C"

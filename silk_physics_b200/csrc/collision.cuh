@@ -1,0 +1,60 @@
+// Collision pipeline: colliders, OIBVH-style broadphase, DCD active contacts,
+// Tight-Inclusion CCD and the coloured Gauss-Seidel contact projection.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+
+namespace silkb {
+
+class World;
+struct CollisionImpl;
+
+class CollisionSystem {
+ public:
+  explicit CollisionSystem(World& w);
+  ~CollisionSystem();
+
+  // Rebuild colliders after a change of the world layout.
+  void rebuild();
+  // Smallest bbox padding over all colliders (main_loop.cu:156-162).
+  float scene_padding() const;
+  bool has_colliders() const;
+  // Obstacle positions for this step (obstacle_assembler.cu:50-63).
+  void refresh_obstacles();
+  // Cloth collider trajectories t0 -> t1 (global solver-order states).
+  void refit(const float4* cloth_t1, const float4* cloth_t0);
+  // New step: empty contact set (contact_constraints.cu:413-434).
+  void begin_step();
+  // DCD at collider time t; appends new contacts.  Returns the number added.
+  int append_active(float time, float activation);
+  // Earliest time of impact over [time_start, time_start + max_time].
+  float min_toi(float time_start, float max_time, float min_separation,
+                int* n_queries, int* n_hits);
+  // Contact projection of one ADMM iteration (after contact_init).
+  void contact_solve();
+  int contact_count() const;
+  int color_count() const;
+  const int* active_dof_device() const;
+  int last_candidates() const;
+
+  // Inspection.
+  int debug_candidates(int* out, int64_t cap);
+  int debug_dcd(float t, float dact, int* keys, int64_t cap);
+
+ private:
+  World& w_;
+  std::unique_ptr<CollisionImpl> impl_;
+};
+
+// Standalone operators.
+void ccd_batch_host(bool vf, const float* x, int64_t n, const float* err3,
+                    const float* ms, float tol, int max_iter, float max_time,
+                    int* hit, float* toi, float* t_upper);
+int color_contacts_host(const int* verts4, const uint64_t* prio, int64_t n,
+                        int* colors);
+
+}  // namespace silkb

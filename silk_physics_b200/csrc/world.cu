@@ -1,0 +1,878 @@
+// Host orchestration of the per-step pipeline (reference:
+// backend/cuda/cuda_backend.cu:31-352, main_loop.cu:24-278,
+// admm_solver.cu:173-342, cloth_admm_helper.cu:306-347,
+// assembly/cloth_assembler.cu:64-172, pin_constraints.cu:50-107).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "collision.cuh"
+#include "world.hpp"
+
+namespace silkb {
+
+namespace {
+
+std::vector<float4> to_float4(const std::vector<float>& v3, const std::vector<int>& perm) {
+  int n = (int)perm.size();
+  std::vector<float4> out(n);
+  for (int i = 0; i < n; ++i)
+    out[perm[i]] = make_float4(v3[3 * i], v3[3 * i + 1], v3[3 * i + 2], 0.f);
+  return out;
+}
+
+}  // namespace
+
+World::World() {
+  silk_global_config_default(&g);
+  silk_solver_options_default(&opt);
+}
+
+World::~World() {
+  coll_.reset();
+  if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+void World::ensure_stream() {
+  if (!stream) {
+    CUDA_CHECK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    own_stream = true;
+  }
+}
+
+void World::sync() { CUDA_CHECK(cudaStreamSynchronize(stream)); }
+
+silk_status World::init(int backend) {
+  if (backend != SILK_BACKEND_GPU) {
+    last_error = "only the GPU backend is provided";
+    return SILK_ERR_INVALID_CONFIG;
+  }
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    last_error = "CUDA runtime/device not available";
+    return SILK_ERR_NO_CUDA_SUPPORT;
+  }
+  ensure_stream();
+  if (!coll_) coll_ = std::make_unique<CollisionSystem>(*this);
+  initialized = true;
+  return SILK_OK;
+}
+
+silk_status World::set_global_config(const silk_global_config& c) {
+  if (c.dt != g.dt) invalidate_layout();
+  g = c;
+  return SILK_OK;
+}
+
+void World::clear() {
+  if (stream) cudaStreamSynchronize(stream);
+  coll_.reset();
+  cloths.clear();
+  obstacles.clear();
+  initialized = false;
+  layout_valid_ = false;
+  nv_total = nf_total = 0;
+}
+
+silk_status World::set_solver_options(const silk_solver_options& o) {
+  opt = o;
+  if (opt.cg_max_iter <= 0) opt.cg_max_iter = 1000;
+  return SILK_OK;
+}
+
+silk_status World::set_stream(void* s) {
+  if (stream) cudaStreamSynchronize(stream);
+  if (own_stream && stream) cudaStreamDestroy(stream);
+  own_stream = false;
+  stream = (cudaStream_t)s;
+  if (!stream) ensure_stream();
+  return SILK_OK;
+}
+
+Cloth* World::find_cloth(uint32_t h) {
+  for (auto& c : cloths)
+    if (c->handle == h) return c.get();
+  return nullptr;
+}
+
+Obstacle* World::find_obstacle(uint32_t h) {
+  for (auto& o : obstacles)
+    if (o->handle == h) return o.get();
+  return nullptr;
+}
+
+void World::invalidate_layout() {
+  if (!layout_valid_) return;
+  // Keep the simulated states on the host while the layout is rebuilt.
+  sync();
+  for (auto& c : cloths) {
+    if (!c->on_device) continue;
+    int nv = c->nv();
+    std::vector<float4> xs(nv), vs(nv);
+    CUDA_CHECK(cudaMemcpy(xs.data(), sx.p + c->voff, nv * sizeof(float4),
+                          cudaMemcpyDeviceToHost));
+    CUDA_CHECK(cudaMemcpy(vs.data(), sv.p + c->voff, nv * sizeof(float4),
+                          cudaMemcpyDeviceToHost));
+    c->x_host.resize(3 * nv);
+    c->v_host.resize(3 * nv);
+    for (int i = 0; i < nv; ++i) {
+      int s = c->setup->perm[i];
+      c->x_host[3 * i] = xs[s].x;
+      c->x_host[3 * i + 1] = xs[s].y;
+      c->x_host[3 * i + 2] = xs[s].z;
+      c->v_host[3 * i] = vs[s].x;
+      c->v_host[3 * i + 1] = vs[s].y;
+      c->v_host[3 * i + 2] = vs[s].z;
+    }
+    c->on_device = false;
+  }
+  layout_valid_ = false;
+}
+
+silk_status World::solver_reset() {
+  if (stream) sync();
+  for (auto& c : cloths) {
+    c->x_host = c->rest;
+    c->v_host.assign(c->rest.size(), 0.0f);
+    c->on_device = false;
+    c->pin_pos.clear();
+    for (int p : c->pins)
+      for (int d = 0; d < 3; ++d) c->pin_pos.push_back(c->rest[3 * p + d]);
+  }
+  for (auto& o : obstacles) {
+    o->is_static = true;
+    o->is_static_twice = true;
+  }
+  layout_valid_ = false;
+  return SILK_OK;
+}
+
+silk_status World::add_cloth(const silk_cloth_config& cc,
+                             const silk_collision_config& col, const float* v,
+                             int64_t nvf, const int* f, int64_t nfi,
+                             const int* pins, int64_t npins, uint32_t* handle) {
+  if (handle) *handle = 0;
+  std::string why = check_cloth_mesh(v, nvf, f, nfi);
+  if (!why.empty()) {
+    last_error = why;
+    return SILK_ERR_INVALID_MESH;
+  }
+  int nv = (int)(nvf / 3);
+  if (npins > nv || (npins > 0 && pins == nullptr)) {
+    last_error = "too many pins";
+    return SILK_ERR_INVALID_PIN;
+  }
+  for (int64_t i = 0; i < npins; ++i)
+    if (pins[i] < 0 || pins[i] >= nv) {
+      last_error = "pin index out of range";
+      return SILK_ERR_INVALID_PIN;
+    }
+  invalidate_layout();
+  auto c = std::make_unique<Cloth>();
+  c->handle = next_handle_++;
+  c->cfg = cc;
+  c->coll = col;
+  c->rest.assign(v, v + nvf);
+  c->faces.assign(f, f + nfi);
+  c->pins.assign(pins, pins + npins);
+  for (int p : c->pins)
+    for (int d = 0; d < 3; ++d) c->pin_pos.push_back(c->rest[3 * p + d]);
+  c->x_host = c->rest;
+  c->v_host.assign(c->rest.size(), 0.0f);
+  *handle = c->handle;
+  cloths.push_back(std::move(c));
+  return SILK_OK;
+}
+
+silk_status World::remove_cloth(uint32_t h) {
+  Cloth* c = find_cloth(h);
+  if (!c) return SILK_ERR_INVALID_HANDLE;
+  invalidate_layout();
+  cloths.erase(std::remove_if(cloths.begin(), cloths.end(),
+                              [h](auto& p) { return p->handle == h; }),
+               cloths.end());
+  return SILK_OK;
+}
+
+silk_status World::get_cloth_position(uint32_t h, float* out, int64_t n) {
+  Cloth* c = find_cloth(h);
+  if (!c) return SILK_ERR_INVALID_HANDLE;
+  int nv = c->nv();
+  if (n != 3 * (int64_t)nv) return SILK_ERR_INVALID_POSITION;
+  if (!c->on_device) {
+    std::memcpy(out, c->x_host.data(), sizeof(float) * 3 * nv);
+    return SILK_OK;
+  }
+  std::vector<float4> xs(nv);
+  CUDA_CHECK(cudaMemcpyAsync(xs.data(), sx.p + c->voff, nv * sizeof(float4),
+                             cudaMemcpyDeviceToHost, stream));
+  sync();
+  const auto& perm = c->setup->perm;
+  for (int i = 0; i < nv; ++i) {
+    float4 q = xs[perm[i]];
+    out[3 * i] = q.x;
+    out[3 * i + 1] = q.y;
+    out[3 * i + 2] = q.z;
+  }
+  return SILK_OK;
+}
+
+silk_status World::set_cloth_config(uint32_t h, const silk_cloth_config& cfg) {
+  Cloth* c = find_cloth(h);
+  if (!c) return SILK_ERR_INVALID_HANDLE;
+  invalidate_layout();
+  c->cfg = cfg;
+  c->setup_valid = false;
+  return SILK_OK;
+}
+
+silk_status World::set_cloth_collision_config(uint32_t h,
+                                              const silk_collision_config& col) {
+  Cloth* c = find_cloth(h);
+  if (!c) return SILK_ERR_INVALID_HANDLE;
+  invalidate_layout();
+  c->coll = col;
+  return SILK_OK;
+}
+
+silk_status World::set_cloth_pin_index(uint32_t h, const int* pins, int64_t n) {
+  Cloth* c = find_cloth(h);
+  if (!c) return SILK_ERR_INVALID_HANDLE;
+  for (int64_t i = 0; i < n; ++i)
+    if (pins[i] < 0 || pins[i] >= c->nv()) return SILK_ERR_INVALID_PIN;
+  invalidate_layout();
+  c->pins.assign(pins, pins + n);
+  // PinPosition is rebuilt from the initial vertices (cloth_assembler.cu:79).
+  c->pin_pos.clear();
+  for (int p : c->pins)
+    for (int d = 0; d < 3; ++d) c->pin_pos.push_back(c->rest[3 * p + d]);
+  return SILK_OK;
+}
+
+silk_status World::set_cloth_pin_position(uint32_t h, const float* pos,
+                                          int64_t n) {
+  Cloth* c = find_cloth(h);
+  if (!c) return SILK_ERR_INVALID_HANDLE;
+  if (n != 3 * (int64_t)c->pins.size()) return SILK_ERR_INVALID_PIN;
+  c->pin_pos.assign(pos, pos + n);
+  pins_dirty_ = true;
+  return SILK_OK;
+}
+
+silk_status World::add_obstacle(const silk_collision_config& col,
+                                const float* v, int64_t nvf, const int* f,
+                                int64_t nfi, uint32_t* handle) {
+  if (handle) *handle = 0;
+  std::string why = check_obstacle_mesh(v, nvf, f, nfi);
+  if (!why.empty()) {
+    last_error = why;
+    return SILK_ERR_INVALID_MESH;
+  }
+  invalidate_layout();
+  auto o = std::make_unique<Obstacle>();
+  o->handle = next_handle_++;
+  o->coll = col;
+  o->cur.assign(v, v + nvf);
+  o->prev = o->cur;
+  if (nfi > 0) o->faces.assign(f, f + nfi);
+  *handle = o->handle;
+  obstacles.push_back(std::move(o));
+  return SILK_OK;
+}
+
+silk_status World::remove_obstacle(uint32_t h) {
+  if (!find_obstacle(h)) return SILK_ERR_INVALID_HANDLE;
+  invalidate_layout();
+  obstacles.erase(std::remove_if(obstacles.begin(), obstacles.end(),
+                                 [h](auto& p) { return p->handle == h; }),
+                  obstacles.end());
+  return SILK_OK;
+}
+
+silk_status World::set_obstacle_collision_config(uint32_t h,
+                                                 const silk_collision_config& c) {
+  Obstacle* o = find_obstacle(h);
+  if (!o) return SILK_ERR_INVALID_HANDLE;
+  invalidate_layout();
+  o->coll = c;
+  return SILK_OK;
+}
+
+silk_status World::set_obstacle_position(uint32_t h, const float* pos,
+                                         int64_t n) {
+  Obstacle* o = find_obstacle(h);
+  if (!o) return SILK_ERR_INVALID_HANDLE;
+  if (n != (int64_t)o->cur.size()) return SILK_ERR_INVALID_POSITION;
+  // cuda_backend.cu:323-344: the previous target becomes the start of the
+  // obstacle motion over the next step.
+  o->is_static = false;
+  o->is_static_twice = false;
+  std::swap(o->cur, o->prev);
+  o->cur.assign(pos, pos + n);
+  o->positions_dirty = true;
+  return SILK_OK;
+}
+
+SolverView World::view() {
+  SolverView s;
+  s.nv = nv_total;
+  s.nf = nf_total;
+  s.dt = g.dt;
+  s.acc = make_float4(g.acceleration_x, g.acceleration_y, g.acceleration_z, 0.f);
+  s.x = x.p;
+  s.prev = sx.p;
+  s.prev_v = prev_v.p;
+  s.mass = mass.p;
+  s.bending_rhs = bending_rhs.p;
+  s.faces = faces_d.p;
+  s.B0 = B0.p;
+  s.B1 = B1.p;
+  s.zu = zu.p;
+  s.zold = zold.p;
+  s.vf_off = vf_off.p;
+  s.vf_list = vf_list.p;
+  s.pin_flag = pin_flag.p;
+  s.pin_target = pin_target.p;
+  s.pin_lambda = pin_lambda.p;
+  s.contact_w = contact_w.p;
+  s.contact_p = contact_p.p;
+  s.contact_p_prev = contact_p_prev.p;
+  s.contact_eta = contact_eta.p;
+  s.lhs = lhs.p;
+  s.rhs = rhs.p;
+  s.inertia = inertia.p;
+  return s;
+}
+
+// Per-cloth static device data: sliced-ELL off-diagonal L, MAS plans.
+void World::build_cloth_device(Cloth& c) {
+  const ClothSetup& S = *c.setup;
+  ClothDev& d = c.dev;
+  cudaStream_t st = stream;
+  int nv = S.nv;
+  // Sliced ELL of the off-diagonal part, 32 rows per slice.
+  int nsl = div_up(nv, 32);
+  std::vector<int> sl_ptr(nsl + 1, 0), sl_w(nsl, 0);
+  std::vector<float> ldiag(nv, 0.f);
+  for (int s = 0; s < nsl; ++s) {
+    int w = 0;
+    for (int r = 32 * s; r < std::min(nv, 32 * s + 32); ++r) {
+      int cnt = 0;
+      for (int k = S.Lrows[r]; k < S.Lrows[r + 1]; ++k)
+        if (S.Lcols[k] != r) ++cnt;
+      w = std::max(w, cnt);
+    }
+    sl_w[s] = w;
+    sl_ptr[s + 1] = sl_ptr[s] + 32 * w;
+  }
+  std::vector<int2> ent(sl_ptr[nsl]);
+  for (int s = 0; s < nsl; ++s)
+    for (int lane = 0; lane < 32; ++lane) {
+      int r = 32 * s + lane;
+      int k = 0;
+      if (r < nv) {
+        for (int q = S.Lrows[r]; q < S.Lrows[r + 1]; ++q) {
+          if (S.Lcols[q] == r) {
+            ldiag[r] = (float)S.Lvals[q];
+            continue;
+          }
+          float val = (float)S.Lvals[q];
+          int bits;
+          std::memcpy(&bits, &val, 4);
+          ent[sl_ptr[s] + k * 32 + lane] = make_int2(S.Lcols[q], bits);
+          ++k;
+        }
+      }
+      for (; k < sl_w[s]; ++k)
+        ent[sl_ptr[s] + k * 32 + lane] = make_int2(r < nv ? r : 0, 0);
+    }
+  d.sl_ptr.upload(sl_ptr, st);
+  d.sl_w.upload(sl_w, st);
+  d.ent.upload(ent, st);
+  d.Ldiag.upload(ldiag, st);
+  d.Lvals.upload(S.Lvals, st);
+  d.part_off.upload(S.part_offsets, st);
+  std::vector<int4> cm(nv);
+  for (int v = 0; v < nv; ++v)
+    cm[v] = make_int4(S.cmap[4 * v], S.cmap[4 * v + 1], S.cmap[4 * v + 2],
+                      S.cmap[4 * v + 3]);
+  d.cmap.upload(cm, st);
+  auto upload_level = [&](const MasLevelPlan& P, ClothDev::Level& L, int nnode,
+                          int nrout) {
+    L.fill_src.upload(P.fill_src, st);
+    std::vector<signed char> sc(P.slot_cco.size());
+    for (size_t i = 0; i < sc.size(); ++i) sc[i] = (signed char)P.slot_cco[i];
+    L.slot_cco.upload(sc, st);
+    L.cco_base.upload(P.bank_cco_base, st);
+    L.ncco.upload(P.bank_ncco, st);
+    L.M.alloc((size_t)P.nbank * kPacked);
+    L.Mb.alloc((size_t)P.nbank * kPacked);
+    if (nnode > 0) {
+      L.zout.alloc(nnode);
+      L.zout.zero(st);
+    }
+    if (nrout > 0) {
+      L.rout.alloc(nrout);
+      L.rout.zero(st);
+    }
+  };
+  int n0 = S.levels > 0 ? S.galerkin[0].n : 0;
+  upload_level(S.fine, d.fine, 0, S.levels > 0 ? n0 : 0);
+  d.coarse.clear();
+  d.coarse.resize(S.levels);
+  for (int l = 1; l <= S.levels; ++l) {
+    int nnode = S.galerkin[l - 1].n;
+    int nnext = l < S.levels ? S.galerkin[l].n : 0;
+    upload_level(S.coarse[l - 1], d.coarse[l - 1], nnode, nnext);
+  }
+  d.gal.clear();
+  d.gal.resize(S.levels);
+  for (int k = 0; k < S.levels; ++k) {
+    const auto& G = S.galerkin[k];
+    d.gal[k].src_off.upload(G.src_off, st);
+    d.gal[k].src.upload(G.src, st);
+    if (k == 0) {
+      d.gal[k].diag_off.upload(G.diag_off, st);
+      d.gal[k].diag.upload(G.diag, st);
+    }
+    d.gal[k].vals.alloc(G.cols.size());
+  }
+  d.r.alloc(nv);
+  d.z0.alloc(nv);
+  d.p.alloc(nv);
+  d.Ap.alloc(nv);
+  d.p.zero(st);
+  int nbank0 = S.fine.nbank;
+  d.cg_grid = cg_grid_size(nsl, nbank0);
+  d.partials.alloc(4 * (size_t)d.cg_grid);
+  d.coarse_partial.alloc(1);
+  d.barrier.alloc(4);
+  d.barrier.zero(st);
+  d.result.alloc(2);
+  d.result_rr.alloc(1);
+  // CG argument template (vectors are bound per solve).
+  CgArgs& a = d.cg;
+  a = CgArgs{};
+  a.nv = nv;
+  a.nslices = nsl;
+  a.sl_ptr = d.sl_ptr.p;
+  a.sl_w = d.sl_w.p;
+  a.ent = d.ent.p;
+  a.Ldiag = d.Ldiag.p;
+  a.r = d.r.p;
+  a.z0 = d.z0.p;
+  a.p = d.p.p;
+  a.Ap = d.Ap.p;
+  a.cmap = d.cmap.p;
+  a.nbank0 = nbank0;
+  a.part_off = d.part_off.p;
+  auto lv_dev = [&](const MasLevelPlan& P, ClothDev::Level& L, int nnode,
+                    float4* rin) {
+    MasLevelDev m;
+    m.nbank = P.nbank;
+    m.nnode = nnode;
+    m.fill_src = L.fill_src.p;
+    m.slot_cco = L.slot_cco.p;
+    m.cco_base = L.cco_base.p;
+    m.ncco = L.ncco.p;
+    m.M = L.M.p;
+    m.Mb = L.Mb.p;
+    m.rin = rin;
+    m.zout = L.zout.p;
+    m.rout = L.rout.p;
+    return m;
+  };
+  a.fine = lv_dev(S.fine, d.fine, nv, nullptr);
+  a.levels = S.levels;
+  for (int l = 1; l <= S.levels; ++l) {
+    float4* rin = l == 1 ? d.fine.rout.p : d.coarse[l - 2].rout.p;
+    a.coarse[l - 1] = lv_dev(S.coarse[l - 1], d.coarse[l - 1],
+                             S.galerkin[l - 1].n, rin);
+  }
+  a.partials = d.partials.p;
+  a.coarse_partial = d.coarse_partial.p;
+  a.barrier = d.barrier.p;
+  a.result = d.result.p;
+  a.result_rr = d.result_rr.p;
+}
+
+void World::ensure_layout() {
+  ensure_stream();
+  if (layout_valid_ && layout_dt_ == g.dt) return;
+  if (layout_valid_) invalidate_layout();
+  cudaStream_t st = stream;
+  nv_total = nf_total = 0;
+  for (auto& c : cloths) {
+    if (!c->setup_valid) {
+      c->setup = std::make_unique<ClothSetup>();
+      ClothParams prm;
+      prm.elastic_stiffness = c->cfg.elastic_stiffness;
+      prm.bending_stiffness = c->cfg.bending_stiffness;
+      prm.density = c->cfg.density;
+      prm.damping = c->cfg.damping;
+      build_cloth_setup(c->rest.data(), c->nv(), c->faces.data(), c->nf(), prm,
+                        *c->setup);
+      build_cloth_device(*c);
+      c->setup_valid = true;
+    }
+    c->voff = nv_total;
+    c->foff = nf_total;
+    nv_total += c->nv();
+    nf_total += c->nf();
+  }
+  int nv = nv_total, nf = nf_total;
+  for (DevBuf<float4>* b : {&sx, &sv, &prev_v, &outer, &outer_v, &x, &bending_rhs,
+                            &rhs, &inertia, &pin_target, &pin_lambda, &contact_p,
+                            &contact_p_prev, &contact_eta})
+    b->alloc(nv);
+  for (DevBuf<float>* b : {&mass, &damp, &lhs, &contact_w, &contact_w_base}) b->alloc(nv);
+  pin_flag.alloc(nv);
+  faces_d.alloc(nf);
+  B0.alloc(nf);
+  B1.alloc(nf);
+  zu.alloc(3 * (size_t)nf);
+  zold.alloc(2 * (size_t)nf);
+  std::vector<float4> hx, hv, hbr;
+  std::vector<float> hm, hd, hcw;
+  std::vector<int4> hf;
+  std::vector<float4> hb0, hb1;
+  std::vector<int> hvo(1, 0), hvl;
+  for (auto& c : cloths) {
+    const ClothSetup& S = *c->setup;
+    auto xs = to_float4(c->x_host, S.perm);
+    auto vs = to_float4(c->v_host, S.perm);
+    hx.insert(hx.end(), xs.begin(), xs.end());
+    hv.insert(hv.end(), vs.begin(), vs.end());
+    std::vector<double> cw;
+    contact_weights(S, g.dt, cw);
+    for (int i = 0; i < S.nv; ++i) {
+      hbr.push_back(make_float4((float)S.bending_rhs[3 * i], (float)S.bending_rhs[3 * i + 1],
+                                (float)S.bending_rhs[3 * i + 2], 0.f));
+      hm.push_back((float)S.mass[i]);
+      hd.push_back(1.0f - c->cfg.damping);
+      hcw.push_back((float)cw[i]);
+    }
+    for (int t = 0; t < S.nf; ++t) {
+      hf.push_back(make_int4(c->voff + S.F[3 * t], c->voff + S.F[3 * t + 1],
+                             c->voff + S.F[3 * t + 2], 0));
+      hb0.push_back(make_float4(S.B[6 * t], S.B[6 * t + 1], S.B[6 * t + 2], S.area_sqrt[t]));
+      hb1.push_back(make_float4(S.B[6 * t + 3], S.B[6 * t + 4], S.B[6 * t + 5],
+                                c->cfg.elastic_stiffness));
+    }
+    for (int i = 0; i < S.nv; ++i) {
+      for (int k = S.vf_offsets[i]; k < S.vf_offsets[i + 1]; ++k) {
+        int code = S.vf_list[k];
+        hvl.push_back(((c->foff + (code >> 2)) << 2) | (code & 3));
+      }
+      hvo.push_back((int)hvl.size());
+    }
+  }
+  auto up4 = [&](DevBuf<float4>& b, const std::vector<float4>& h) {
+    if (!h.empty())
+      CUDA_CHECK(cudaMemcpyAsync(b.p, h.data(), h.size() * sizeof(float4),
+                                 cudaMemcpyHostToDevice, st));
+  };
+  up4(sx, hx);
+  up4(sv, hv);
+  up4(bending_rhs, hbr);
+  mass.upload(hm, st);
+  damp.upload(hd, st);
+  contact_w_base.upload(hcw, st);
+  faces_d.upload(hf, st);
+  B0.upload(hb0, st);
+  B1.upload(hb1, st);
+  vf_off.upload(hvo, st);
+  vf_list.upload(hvl, st);
+  zu.zero(st);
+  zold.zero(st);
+  pin_lambda.zero(st);
+  contact_w.zero(st);
+  contact_p.zero(st);
+  contact_p_prev.zero(st);
+  contact_eta.zero(st);
+  face_partials.alloc((size_t)face_step_blocks(nf) * kAdmmSlots);
+  vertex_partials.alloc((size_t)vertex_step_blocks(nv) * kAdmmSlots);
+  ctl.alloc(1);
+  cg_stats.alloc(2);
+  pinned_dof = 0;
+  for (auto& c : cloths) c->on_device = true;
+  pins_dirty_ = true;
+  if (coll_) coll_->rebuild();
+  layout_valid_ = true;
+  layout_dt_ = g.dt;
+}
+
+void World::upload_pins() {
+  if (!pins_dirty_) return;
+  std::vector<unsigned char> flag(nv_total, 0);
+  std::vector<float4> tgt(nv_total, make_float4(0, 0, 0, 0));
+  pinned_dof = 0;
+  for (auto& c : cloths) {
+    const auto& perm = c->setup->perm;
+    for (size_t k = 0; k < c->pins.size(); ++k) {
+      int v = c->voff + perm[c->pins[k]];
+      if (!flag[v]) pinned_dof += 3;
+      flag[v] = 1;
+      tgt[v] = make_float4(c->pin_pos[3 * k], c->pin_pos[3 * k + 1],
+                           c->pin_pos[3 * k + 2], 0.f);
+    }
+  }
+  if (nv_total) {
+    CUDA_CHECK(cudaMemcpyAsync(pin_flag.p, flag.data(), nv_total,
+                               cudaMemcpyHostToDevice, stream));
+    CUDA_CHECK(cudaMemcpyAsync(pin_target.p, tgt.data(), nv_total * sizeof(float4),
+                               cudaMemcpyHostToDevice, stream));
+    sync();  // host vectors go out of scope
+  }
+  pins_dirty_ = false;
+}
+
+// MASPreconditioner::factorize on A = L + diag(lhs) (mas_preconditioner.cu:903).
+void World::factorize(Cloth& c) {
+  ClothDev& d = c.dev;
+  const ClothSetup& S = *c.setup;
+  const float* dyn = lhs.p + c.voff;
+  for (int k = 0; k < S.levels; ++k) {
+    GalerkinDev gd;
+    gd.n_entries = (int)S.galerkin[k].cols.size();
+    gd.src_off = d.gal[k].src_off.p;
+    gd.src = d.gal[k].src.p;
+    gd.diag_off = k == 0 ? d.gal[k].diag_off.p : nullptr;
+    gd.diag = k == 0 ? d.gal[k].diag.p : nullptr;
+    gd.vals = d.gal[k].vals.p;
+    launch_galerkin_fill(gd, k == 0 ? d.Lvals.p : d.gal[k - 1].vals.p, dyn, stream);
+  }
+  launch_bank_invert(d.cg.fine, true, d.part_off.p, d.Lvals.p, dyn, stream);
+  for (int l = 1; l <= S.levels; ++l)
+    launch_bank_invert(d.cg.coarse[l - 1], false, nullptr, d.gal[l - 1].vals.p,
+                       nullptr, stream);
+}
+
+void World::cg_solve(Cloth& c, float rel_tol) {
+  CgArgs a = c.dev.cg;
+  a.dyn = lhs.p + c.voff;
+  a.b = rhs.p + c.voff;
+  a.x = x.p + c.voff;
+  a.bf16 = opt.mas_bf16 ? 1 : 0;
+  a.rel_tol = rel_tol;
+  a.abs_tol = g.linear_solver_abs_tol;
+  a.max_iter = opt.cg_max_iter > 0 ? opt.cg_max_iter : 1000;
+  a.stats = cg_stats.p;
+  launch_cg(a, c.dev.cg_grid, stream);
+}
+
+bool World::admm_solve() {
+  SolverView s = view();
+  cudaStream_t st = stream;
+  launch_compute_inertia(s, st);
+  pin_lambda.zero(st);
+  float rel = std::min(std::max(g.initial_linear_rel_tol, g.linear_solver_rel_tol_min),
+                       g.linear_solver_rel_tol_max);
+  if (opt.fixed_linear_rel_tol > 0) rel = opt.fixed_linear_rel_tol;
+  int fb = face_step_blocks(nf_total), vb = vertex_step_blocks(nv_total);
+  AdmmFinalizeArgs fa;
+  fa.face_partials = face_partials.p;
+  fa.face_blocks = fb;
+  fa.vertex_partials = vertex_partials.p;
+  fa.vertex_blocks = vb;
+  fa.dof_primal_static = 6 * nf_total + pinned_dof;
+  fa.contact_active_dof = coll_ ? coll_->active_dof_device() : nullptr;
+  fa.state_dof = 3 * nv_total;
+  fa.abs_tol = g.admm_abs_tol;
+  fa.rel_tol = g.admm_rel_tol;
+  fa.init_lin_rel = g.initial_linear_rel_tol;
+  fa.lin_rel_min = g.linear_solver_rel_tol_min;
+  fa.lin_rel_max = g.linear_solver_rel_tol_max;
+  fa.fixed_rel = opt.fixed_linear_rel_tol;
+  fa.ctl = ctl.p;
+  bool contacts = coll_ && coll_->contact_count() > 0;
+  for (int it = 0; it < g.max_inner_iteration; ++it) {
+    if (it != 0) {
+      for (auto& c : cloths) {
+        if (it == 1) factorize(*c);
+        cg_solve(*c, rel);
+      }
+    }
+    launch_face_step(s, face_partials.p, fb, st);
+    if (contacts) {
+      launch_contact_init(s, st);
+      coll_->contact_solve();
+    }
+    launch_vertex_step(s, vertex_partials.p, vb, st);
+    stats.admm_iterations += 1;
+    if (it == 0) continue;
+    fa.iteration = it;
+    launch_admm_finalize(fa, st);
+    AdmmControl h;
+    CUDA_CHECK(cudaMemcpyAsync(&h, ctl.p, sizeof(AdmmControl), cudaMemcpyDeviceToHost, st));
+    sync();
+    if (h.diverged) return false;
+    if (h.converged) break;
+    rel = h.next_rel_tol;
+  }
+  launch_enforce(s, st);
+  return true;
+}
+
+silk_status World::solver_step() {
+  if (!initialized) return SILK_ERR_NOT_INITIALIZED;
+  try {
+    long long launches0 = g_launch_count;
+    stats = silk_step_stats{};
+    if (cloths.empty()) {
+      last_error = "nothing to solve";
+      return SILK_ERR_UNKNOWN;
+    }
+    ensure_layout();
+    upload_pins();
+    cudaStream_t st = stream;
+    int nv = nv_total;
+    cg_stats.zero(st);
+    // init (main_loop.cu:24-76): damped velocity, fresh ADMM aux variables.
+    launch_damp(nv, damp.p, sv.p, prev_v.p, st);
+    zu.zero(st);
+    CUDA_CHECK(cudaMemcpyAsync(outer.p, sx.p, nv * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    CUDA_CHECK(cudaMemcpyAsync(outer_v.p, prev_v.p, nv * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    bool collide = coll_ && coll_->has_colliders();
+    float ms = 0.f, dact = 0.f;
+    if (coll_) {
+      coll_->refresh_obstacles();
+      coll_->begin_step();
+    }
+    if (collide) {
+      float pad = coll_->scene_padding();
+      ms = 0.2f * pad;
+      dact = 1.0f * pad;
+      coll_->refit(outer.p, outer.p);
+      coll_->append_active(0.0f, dact);
+    }
+    float remaining = 1.0f;
+    for (int oit = 0; oit < g.max_outer_iteration; ++oit) {
+      stats.outer_iterations += 1;
+      launch_predict(nv, g.dt, make_float4(g.acceleration_x, g.acceleration_y, g.acceleration_z, 0.f),
+                     outer.p, outer_v.p, x.p, st);
+      if (!admm_solve()) {
+        last_error = "solver diverged";
+        return SILK_ERR_ITERATIVE_SOLVE_FAIL;
+      }
+      float toi = remaining;
+      if (collide) {
+        coll_->refit(x.p, outer.p);
+        int nq = 0, nh = 0;
+        toi = coll_->min_toi(1.0f - remaining, remaining, ms, &nq, &nh);
+        stats.ccd_queries += nq;
+        stats.ccd_hits += nh;
+      }
+      stats.min_toi = toi;
+      launch_velocity(nv, g.dt, x.p, outer.p, outer_v.p, st);
+      if (toi >= remaining) {
+        CUDA_CHECK(cudaMemcpyAsync(outer.p, x.p, nv * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+        break;
+      }
+      float rollback = 0.8f * toi;
+      float frac = rollback / remaining;
+      launch_mix(nv, frac, x.p, outer.p, st);
+      remaining -= rollback;
+      coll_->refit(outer.p, outer.p);
+      coll_->append_active(1.0f - remaining, dact);
+    }
+    // Final velocity from the whole accepted displacement (main_loop.cu:248).
+    launch_velocity(nv, g.dt, outer.p, sx.p, sv.p, st);
+    CUDA_CHECK(cudaMemcpyAsync(sx.p, outer.p, nv * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    int cgs[2];
+    CUDA_CHECK(cudaMemcpyAsync(cgs, cg_stats.p, sizeof(cgs), cudaMemcpyDeviceToHost, st));
+    sync();
+    stats.cg_iterations = cgs[0];
+    stats.cg_solves = cgs[1];
+    if (coll_) {
+      stats.contacts = coll_->contact_count();
+      stats.colors = coll_->color_count();
+      stats.broadphase_candidates = coll_->last_candidates();
+    }
+    for (auto& o : obstacles) {
+      o->prev = o->cur;
+      if (o->is_static) o->is_static_twice = true;
+      else o->is_static = true;
+    }
+    stats.kernel_launches = g_launch_count - launches0;
+    return SILK_OK;
+  } catch (const std::exception& e) {
+    last_error = e.what();
+    return SILK_ERR_UNKNOWN;
+  }
+}
+
+silk_status World::debug_partition(uint32_t h, int* perm, int64_t perm_len,
+                                   int* offs, int64_t cap, int* nparts) {
+  Cloth* c = find_cloth(h);
+  if (!c) return SILK_ERR_INVALID_HANDLE;
+  ensure_layout();
+  const ClothSetup& S = *c->setup;
+  if (perm_len != S.nv) return SILK_ERR_INVALID_POSITION;
+  for (int i = 0; i < S.nv; ++i) perm[i] = S.perm[i];
+  int np = (int)S.part_offsets.size() - 1;
+  *nparts = np;
+  for (int i = 0; i <= np && i < cap; ++i) offs[i] = S.part_offsets[i];
+  return SILK_OK;
+}
+
+silk_status World::debug_matrix(uint32_t h, double* dense, int64_t n) {
+  Cloth* c = find_cloth(h);
+  if (!c) return SILK_ERR_INVALID_HANDLE;
+  ensure_layout();
+  const ClothSetup& S = *c->setup;
+  if (n != (int64_t)S.nv * S.nv) return SILK_ERR_INVALID_POSITION;
+  std::fill(dense, dense + n, 0.0);
+  for (int i = 0; i < S.nv; ++i)
+    for (int k = S.Lrows[i]; k < S.Lrows[i + 1]; ++k)
+      dense[(size_t)i * S.nv + S.Lcols[k]] = S.Lvals[k];
+  return SILK_OK;
+}
+
+silk_status World::debug_refit(const float* disp, int64_t n) {
+  if (!initialized) return SILK_ERR_NOT_INITIALIZED;
+  ensure_layout();
+  std::vector<float4> h(nv_total);
+  int64_t off = 0;
+  for (auto& c : cloths) {
+    for (int i = 0; i < c->nv(); ++i) {
+      float4 q = make_float4(0, 0, 0, 0);
+      if (disp && off + 3 * i + 2 < n)
+        q = make_float4(disp[off + 3 * i], disp[off + 3 * i + 1], disp[off + 3 * i + 2], 0.f);
+      h[c->voff + c->setup->perm[i]] = q;
+    }
+    off += 3 * c->nv();
+  }
+  // x = sx + disp.
+  std::vector<float4> xs(nv_total);
+  CUDA_CHECK(cudaMemcpy(xs.data(), sx.p, nv_total * sizeof(float4), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < nv_total; ++i) {
+    xs[i].x += h[i].x;
+    xs[i].y += h[i].y;
+    xs[i].z += h[i].z;
+  }
+  CUDA_CHECK(cudaMemcpy(x.p, xs.data(), nv_total * sizeof(float4), cudaMemcpyHostToDevice));
+  coll_->refresh_obstacles();
+  coll_->refit(x.p, sx.p);
+  sync();
+  return SILK_OK;
+}
+
+silk_status World::debug_candidates(int* out, int64_t cap, int* n) {
+  *n = coll_->debug_candidates(out, cap);
+  return SILK_OK;
+}
+
+silk_status World::debug_dcd(float t, float dact, int* keys, int64_t cap, int* n) {
+  *n = coll_->debug_dcd(t, dact, keys, cap);
+  return SILK_OK;
+}
+
+silk_status World::debug_min_toi(float ts, float mt, float ms, float* toi,
+                                 int* nq, int* nh) {
+  *toi = coll_->min_toi(ts, mt, ms, nq, nh);
+  return SILK_OK;
+}
+
+}  // namespace silkb

@@ -1,0 +1,213 @@
+// World: host orchestration of the per-step cloth pipeline on one GPU.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/silk_b200.h"
+#include "common.cuh"
+#include "host_setup.hpp"
+#include "mas_cg.cuh"
+#include "solver_kernels.cuh"
+
+namespace silkb {
+
+// Owning device allocation.
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) {
+    o.p = nullptr;
+    o.n = 0;
+  }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      reset();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    reset();
+    n = count;
+    if (count) CUDA_CHECK(cudaMalloc(&p, count * sizeof(T)));
+  }
+  void zero(cudaStream_t st) {
+    if (n) CUDA_CHECK(cudaMemsetAsync(p, 0, n * sizeof(T), st));
+  }
+  void upload(const std::vector<T>& h, cudaStream_t st) {
+    alloc(h.size());
+    if (n) CUDA_CHECK(cudaMemcpyAsync(p, h.data(), n * sizeof(T),
+                                      cudaMemcpyHostToDevice, st));
+  }
+};
+
+struct ClothDev {
+  DevBuf<int> sl_ptr, sl_w;
+  DevBuf<int2> ent;
+  DevBuf<float> Ldiag;
+  DevBuf<double> Lvals;
+  DevBuf<int> part_off;
+  DevBuf<int4> cmap;
+  struct Level {
+    DevBuf<int> fill_src, cco_base, ncco;
+    DevBuf<signed char> slot_cco;
+    DevBuf<float> M;
+    DevBuf<__nv_bfloat16> Mb;
+    DevBuf<float4> zout, rout;
+  };
+  Level fine;
+  std::vector<Level> coarse;
+  struct Gal {
+    DevBuf<int> src_off, src, diag_off, diag;
+    DevBuf<double> vals;
+  };
+  std::vector<Gal> gal;
+  DevBuf<float4> r, z0, p, Ap;
+  DevBuf<double> partials, coarse_partial;
+  DevBuf<unsigned> barrier;
+  DevBuf<int> result;
+  DevBuf<float> result_rr;
+  CgArgs cg;
+  int cg_grid = 1;
+};
+
+struct Cloth {
+  uint32_t handle = 0;
+  silk_cloth_config cfg{};
+  silk_collision_config coll{};
+  std::vector<float> rest;   // original order, 3 per vertex
+  std::vector<int> faces;    // original ids
+  std::vector<int> pins;     // original ids
+  std::vector<float> pin_pos;
+  std::vector<float> x_host, v_host;  // original order; valid if !on_device
+  bool on_device = false;
+  std::unique_ptr<ClothSetup> setup;
+  bool setup_valid = false;
+  ClothDev dev;
+  int voff = 0, foff = 0, eoff = 0;
+  int nv() const { return (int)rest.size() / 3; }
+  int nf() const { return (int)faces.size() / 3; }
+};
+
+struct Obstacle {
+  uint32_t handle = 0;
+  silk_collision_config coll{};
+  std::vector<float> cur, prev;  // 3 per vertex
+  std::vector<int> faces;
+  bool is_static = true, is_static_twice = true;
+  bool positions_dirty = true;
+  int nv() const { return (int)cur.size() / 3; }
+  int nf() const { return (int)faces.size() / 3; }
+};
+
+class CollisionSystem;
+
+class World {
+ public:
+  World();
+  ~World();
+
+  std::string last_error;
+  bool initialized = false;
+
+  silk_status init(int backend);
+  silk_status set_global_config(const silk_global_config& c);
+  void clear();
+  silk_status solver_step();
+  silk_status solver_reset();
+  silk_status add_cloth(const silk_cloth_config& cc,
+                        const silk_collision_config& col, const float* v,
+                        int64_t nvf, const int* f, int64_t nfi, const int* pins,
+                        int64_t npins, uint32_t* handle);
+  silk_status remove_cloth(uint32_t h);
+  silk_status get_cloth_position(uint32_t h, float* out, int64_t n);
+  silk_status set_cloth_config(uint32_t h, const silk_cloth_config& c);
+  silk_status set_cloth_collision_config(uint32_t h,
+                                         const silk_collision_config& c);
+  silk_status set_cloth_pin_index(uint32_t h, const int* pins, int64_t n);
+  silk_status set_cloth_pin_position(uint32_t h, const float* pos, int64_t n);
+  silk_status add_obstacle(const silk_collision_config& col, const float* v,
+                           int64_t nvf, const int* f, int64_t nfi,
+                           uint32_t* handle);
+  silk_status remove_obstacle(uint32_t h);
+  silk_status set_obstacle_collision_config(uint32_t h,
+                                            const silk_collision_config& c);
+  silk_status set_obstacle_position(uint32_t h, const float* pos, int64_t n);
+  silk_status set_solver_options(const silk_solver_options& o);
+  silk_status set_stream(void* s);
+
+  // Inspection.
+  silk_status debug_partition(uint32_t h, int* perm, int64_t perm_len,
+                              int* offs, int64_t cap, int* nparts);
+  silk_status debug_matrix(uint32_t h, double* dense, int64_t n);
+  silk_status debug_refit(const float* disp, int64_t n);
+  silk_status debug_candidates(int* out, int64_t cap, int* n);
+  silk_status debug_dcd(float t, float dact, int* keys, int64_t cap, int* n);
+  silk_status debug_min_toi(float ts, float mt, float ms, float* toi, int* nq,
+                            int* nh);
+
+  silk_step_stats stats{};
+
+  // ---- state shared with the collision system ----
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  silk_global_config g{};
+  silk_solver_options opt{};
+  std::vector<std::unique_ptr<Cloth>> cloths;
+  std::vector<std::unique_ptr<Obstacle>> obstacles;
+  int nv_total = 0, nf_total = 0;
+  // Global per-vertex arrays (solver order, cloths concatenated).
+  DevBuf<float4> sx, sv, prev_v, outer, outer_v, x;
+  DevBuf<float> mass, damp, lhs, contact_w, contact_w_base;
+  DevBuf<float4> bending_rhs, rhs, inertia, pin_target, pin_lambda;
+  DevBuf<float4> contact_p, contact_p_prev, contact_eta;
+  DevBuf<unsigned char> pin_flag;
+  DevBuf<int4> faces_d;
+  DevBuf<float4> B0, B1, zu, zold;
+  DevBuf<int> vf_off, vf_list;
+  DevBuf<double> face_partials, vertex_partials;
+  DevBuf<AdmmControl> ctl;
+  DevBuf<int> cg_stats;  // [iterations, solves]
+  int pinned_dof = 0;
+
+  Cloth* find_cloth(uint32_t h);
+  Obstacle* find_obstacle(uint32_t h);
+  SolverView view();
+
+ private:
+  uint32_t next_handle_ = 1;
+  bool layout_valid_ = false;
+  bool pins_dirty_ = true;
+  float layout_dt_ = -1.0f;
+  std::unique_ptr<CollisionSystem> coll_;
+
+  void ensure_stream();
+  void invalidate_layout();
+  void ensure_layout();
+  void build_cloth_device(Cloth& c);
+  void upload_pins();
+  void factorize(Cloth& c);
+  void cg_solve(Cloth& c, float rel_tol);
+  bool admm_solve();  // false on divergence
+  void sync();
+};
+
+}  // namespace silkb

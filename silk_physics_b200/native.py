@@ -1,0 +1,478 @@
+"""ctypes binding of libsilk_b200.so and the Python ``World`` mirror."""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+_LIB_PATH = Path(__file__).resolve().parent / "libsilk_b200.so"
+
+
+class ErrorCode(enum.IntEnum):
+    """silk::ErrorCode (silk/include/silk/result.hpp:22-35)."""
+
+    Unknown = 0
+    NotInitialized = 1
+    InvalidConfig = 2
+    TooManyBody = 3
+    InvalidHandle = 4
+    InvalidMesh = 5
+    InvalidPin = 6
+    InvalidPosition = 7
+    CholeskyDecompositionFail = 8
+    NeedInitSolverFirst = 9
+    IterativeSolveFail = 10
+    NoCudaSupport = 11
+
+
+class Backend(enum.IntEnum):
+    CPU = 0
+    GPU = 1
+
+
+@dataclass
+class Result:
+    """silk::Result: truthy on success; ``code`` and ``detail`` on error."""
+
+    success: bool = True
+    code: ErrorCode = ErrorCode.Unknown
+    detail: str = ""
+
+    def __bool__(self) -> bool:
+        return self.success
+
+    def to_string(self) -> str:
+        if self.success:
+            return "OK"
+        if not self.detail:
+            return self.code.name
+        return f"{self.code.name}. Reason: {self.detail}."
+
+
+class _GlobalConfigC(C.Structure):
+    _fields_ = [
+        ("acceleration_x", C.c_float), ("acceleration_y", C.c_float),
+        ("acceleration_z", C.c_float), ("max_outer_iteration", C.c_int32),
+        ("max_inner_iteration", C.c_int32), ("dt", C.c_float),
+        ("linear_solver_abs_tol", C.c_float), ("linear_solver_rel_tol_min", C.c_float),
+        ("linear_solver_rel_tol_max", C.c_float), ("initial_linear_rel_tol", C.c_float),
+        ("admm_abs_tol", C.c_float), ("admm_rel_tol", C.c_float),
+    ]
+
+
+class _ClothConfigC(C.Structure):
+    _fields_ = [("elastic_stiffness", C.c_float), ("bending_stiffness", C.c_float),
+                ("density", C.c_float), ("damping", C.c_float)]
+
+
+class _CollisionConfigC(C.Structure):
+    _fields_ = [("is_collision_on", C.c_int32), ("is_self_collision_on", C.c_int32),
+                ("group", C.c_int32), ("restitution", C.c_float), ("friction", C.c_float)]
+
+
+class _SolverOptionsC(C.Structure):
+    _fields_ = [("fixed_linear_rel_tol", C.c_float), ("cg_max_iter", C.c_int32),
+                ("mas_bf16", C.c_int32), ("reserved", C.c_int32 * 5)]
+
+
+class _StepStatsC(C.Structure):
+    _fields_ = [("outer_iterations", C.c_int32), ("admm_iterations", C.c_int32),
+                ("cg_iterations", C.c_int32), ("cg_solves", C.c_int32),
+                ("contacts", C.c_int32), ("colors", C.c_int32),
+                ("ccd_queries", C.c_int32), ("ccd_hits", C.c_int32),
+                ("min_toi", C.c_float), ("broadphase_candidates", C.c_int32),
+                ("kernel_launches", C.c_int64), ("reserved", C.c_int32 * 6)]
+
+
+@dataclass
+class GlobalConfig:
+    """silk::GlobalConfig (silk.hpp:47-77)."""
+
+    acceleration_x: float = 0.0
+    acceleration_y: float = 0.0
+    acceleration_z: float = -10.0
+    max_outer_iteration: int = 100
+    max_inner_iteration: int = 100
+    dt: float = 1.0 / 60.0
+    linear_solver_abs_tol: float = 1e-7
+    linear_solver_rel_tol_min: float = 1e-6
+    linear_solver_rel_tol_max: float = 1e-3
+    initial_linear_rel_tol: float = 1e-2
+    admm_abs_tol: float = 1e-5
+    admm_rel_tol: float = 1e-3
+
+    def to_c(self) -> _GlobalConfigC:
+        return _GlobalConfigC(*[getattr(self, n) for n, _ in _GlobalConfigC._fields_])
+
+
+@dataclass
+class ClothConfig:
+    """silk::ClothConfig (silk.hpp:35-45)."""
+
+    elastic_stiffness: float = 100.0
+    bending_stiffness: float = 0.0001
+    density: float = 0.1
+    damping: float = 0.01
+
+    def to_c(self) -> _ClothConfigC:
+        return _ClothConfigC(self.elastic_stiffness, self.bending_stiffness,
+                             self.density, self.damping)
+
+
+@dataclass
+class CollisionConfig:
+    """silk::CollisionConfig (silk.hpp:26-33)."""
+
+    is_collision_on: bool = True
+    is_self_collision_on: bool = True
+    group: int = 0
+    restitution: float = 0.3
+    friction: float = 0.3
+
+    def to_c(self) -> _CollisionConfigC:
+        return _CollisionConfigC(int(self.is_collision_on), int(self.is_self_collision_on),
+                                 self.group, self.restitution, self.friction)
+
+
+@dataclass
+class SolverOptions:
+    """Switches with no silk::GlobalConfig field (bench / precision modes)."""
+
+    fixed_linear_rel_tol: float = 0.0
+    cg_max_iter: int = 1000
+    mas_bf16: bool = False
+
+    def to_c(self) -> _SolverOptionsC:
+        o = _SolverOptionsC()
+        o.fixed_linear_rel_tol = self.fixed_linear_rel_tol
+        o.cg_max_iter = self.cg_max_iter
+        o.mas_bf16 = int(self.mas_bf16)
+        return o
+
+
+@dataclass
+class StepStats:
+    outer_iterations: int = 0
+    admm_iterations: int = 0
+    cg_iterations: int = 0
+    cg_solves: int = 0
+    contacts: int = 0
+    colors: int = 0
+    ccd_queries: int = 0
+    ccd_hits: int = 0
+    min_toi: float = 0.0
+    broadphase_candidates: int = 0
+    kernel_launches: int = 0
+
+
+_F32P = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_I32P = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_F64P = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_U64P = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+_W = C.c_void_p
+
+
+def _load() -> C.CDLL:
+    if not _LIB_PATH.exists():
+        raise ImportError(
+            f"{_LIB_PATH} is missing: build it with `python -m silk_physics_b200.build`")
+    L = C.CDLL(str(_LIB_PATH))
+    sig = {
+        "silk_world_create": ([], _W),
+        "silk_world_destroy": ([_W], None),
+        "silk_world_last_error": ([_W], C.c_char_p),
+        "silk_world_init": ([_W, C.c_int32], C.c_int),
+        "silk_set_global_config": ([_W, C.POINTER(_GlobalConfigC)], C.c_int),
+        "silk_global_config_default": ([C.POINTER(_GlobalConfigC)], None),
+        "silk_clear": ([_W], None),
+        "silk_solver_step": ([_W], C.c_int),
+        "silk_solver_reset": ([_W], C.c_int),
+        "silk_add_cloth": ([_W, C.POINTER(_ClothConfigC), C.POINTER(_CollisionConfigC),
+                            _F32P, C.c_int64, _I32P, C.c_int64, C.c_void_p, C.c_int64,
+                            C.POINTER(C.c_uint32)], C.c_int),
+        "silk_remove_cloth": ([_W, C.c_uint32], C.c_int),
+        "silk_get_cloth_position": ([_W, C.c_uint32, _F32P, C.c_int64], C.c_int),
+        "silk_set_cloth_config": ([_W, C.c_uint32, C.POINTER(_ClothConfigC)], C.c_int),
+        "silk_set_cloth_collision_config": ([_W, C.c_uint32, C.POINTER(_CollisionConfigC)],
+                                            C.c_int),
+        "silk_set_cloth_pin_index": ([_W, C.c_uint32, C.c_void_p, C.c_int64], C.c_int),
+        "silk_set_cloth_pin_position": ([_W, C.c_uint32, C.c_void_p, C.c_int64], C.c_int),
+        "silk_add_obstacle": ([_W, C.POINTER(_CollisionConfigC), _F32P, C.c_int64, C.c_void_p,
+                               C.c_int64, C.POINTER(C.c_uint32)], C.c_int),
+        "silk_remove_obstacle": ([_W, C.c_uint32], C.c_int),
+        "silk_set_obstacle_collision_config": ([_W, C.c_uint32,
+                                                C.POINTER(_CollisionConfigC)], C.c_int),
+        "silk_set_obstacle_position": ([_W, C.c_uint32, _F32P, C.c_int64], C.c_int),
+        "silk_solver_options_default": ([C.POINTER(_SolverOptionsC)], None),
+        "silk_set_solver_options": ([_W, C.POINTER(_SolverOptionsC)], C.c_int),
+        "silk_get_step_stats": ([_W, C.POINTER(_StepStatsC)], C.c_int),
+        "silk_set_stream": ([_W, C.c_void_p], C.c_int),
+        "silk_debug_cloth_partition": ([_W, C.c_uint32, _I32P, C.c_int64, _I32P, C.c_int64,
+                                        C.POINTER(C.c_int32)], C.c_int),
+        "silk_debug_cloth_matrix": ([_W, C.c_uint32, _F64P, C.c_int64], C.c_int),
+        "silk_debug_refit": ([_W, C.c_void_p, C.c_int64], C.c_int),
+        "silk_debug_candidates": ([_W, _I32P, C.c_int64, C.POINTER(C.c_int32)], C.c_int),
+        "silk_debug_dcd": ([_W, C.c_float, C.c_float, _I32P, C.c_int64,
+                            C.POINTER(C.c_int32)], C.c_int),
+        "silk_debug_min_toi": ([_W, C.c_float, C.c_float, C.c_float, C.POINTER(C.c_float),
+                                C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
+        "silk_ccd_batch": ([C.c_int32, _F32P, C.c_int64, _F32P, _F32P, C.c_float, C.c_int32,
+                            C.c_float, _I32P, _F32P, _F32P], C.c_int),
+        "silk_color_contacts": ([_I32P, _U64P, C.c_int64, _I32P, C.POINTER(C.c_int32)],
+                                C.c_int),
+        "silk_partition_mesh": ([_F32P, C.c_int64, _I32P, C.c_int64, _I32P, _I32P, C.c_int64,
+                                 C.POINTER(C.c_int32)], C.c_int),
+        "silk_assemble_cloth_host": ([C.POINTER(_ClothConfigC), _F32P, C.c_int64, _I32P,
+                                      C.c_int64, C.c_float, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    return L
+
+
+lib = _load()
+
+
+def _result(status: int, world=None) -> Result:
+    if status == 0:
+        return Result()
+    detail = ""
+    if world is not None:
+        detail = (lib.silk_world_last_error(world) or b"").decode()
+    return Result(False, ErrorCode(status - 1), detail)
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32).ravel())
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32).ravel())
+
+
+class World:
+    """Python mirror of silk::World (silk.hpp:83-239).
+
+    Methods return ``Result``; ``add_cloth`` / ``add_obstacle`` return a
+    ``(Result, handle)`` pair because Python has no out-references.
+    """
+
+    def __init__(self) -> None:
+        self._w = lib.silk_world_create()
+        if not self._w:
+            raise MemoryError("silk_world_create failed")
+
+    def __del__(self) -> None:
+        w = getattr(self, "_w", None)
+        if w:
+            lib.silk_world_destroy(w)
+            self._w = None
+
+    # --- global ---
+    def init(self, backend: Backend = Backend.GPU) -> Result:
+        return _result(lib.silk_world_init(self._w, int(backend)), self._w)
+
+    def set_global_config(self, config: GlobalConfig) -> Result:
+        c = config.to_c()
+        return _result(lib.silk_set_global_config(self._w, C.byref(c)), self._w)
+
+    def clear(self) -> None:
+        lib.silk_clear(self._w)
+
+    # --- solver ---
+    def solver_step(self) -> Result:
+        return _result(lib.silk_solver_step(self._w), self._w)
+
+    def solver_reset(self) -> Result:
+        return _result(lib.silk_solver_reset(self._w), self._w)
+
+    # --- cloth ---
+    def add_cloth(self, cloth_config: ClothConfig, collision_config: CollisionConfig,
+                  verts, faces, pin_index=()) -> tuple[Result, int]:
+        v, f, p = _f32(verts), _i32(faces), _i32(pin_index)
+        h = C.c_uint32(0)
+        cc, col = cloth_config.to_c(), collision_config.to_c()
+        st = lib.silk_add_cloth(self._w, C.byref(cc), C.byref(col), v, v.size, f, f.size,
+                                p.ctypes.data if p.size else None, p.size, C.byref(h))
+        return _result(st, self._w), int(h.value)
+
+    def remove_cloth(self, handle: int) -> Result:
+        return _result(lib.silk_remove_cloth(self._w, handle), self._w)
+
+    def get_cloth_position(self, handle: int, position: np.ndarray) -> Result:
+        """Fill ``position`` (float32, size 3 * vertex count) in mesh order."""
+        if position.dtype != np.float32 or not position.flags.c_contiguous:
+            raise TypeError("position must be a contiguous float32 array")
+        return _result(lib.silk_get_cloth_position(self._w, handle, position.reshape(-1),
+                                                   position.size), self._w)
+
+    def set_cloth_config(self, handle: int, config: ClothConfig) -> Result:
+        c = config.to_c()
+        return _result(lib.silk_set_cloth_config(self._w, handle, C.byref(c)), self._w)
+
+    def set_cloth_collision_config(self, handle: int, config: CollisionConfig) -> Result:
+        c = config.to_c()
+        return _result(lib.silk_set_cloth_collision_config(self._w, handle, C.byref(c)),
+                       self._w)
+
+    def set_cloth_pin_index(self, handle: int, pin_index) -> Result:
+        p = _i32(pin_index)
+        return _result(lib.silk_set_cloth_pin_index(self._w, handle,
+                                                    p.ctypes.data if p.size else None,
+                                                    p.size), self._w)
+
+    def set_cloth_pin_position(self, handle: int, position) -> Result:
+        p = _f32(position)
+        return _result(lib.silk_set_cloth_pin_position(self._w, handle,
+                                                       p.ctypes.data if p.size else None,
+                                                       p.size), self._w)
+
+    # --- obstacle ---
+    def add_obstacle(self, collision_config: CollisionConfig, verts,
+                     faces) -> tuple[Result, int]:
+        v, f = _f32(verts), _i32(faces)
+        h = C.c_uint32(0)
+        col = collision_config.to_c()
+        st = lib.silk_add_obstacle(self._w, C.byref(col), v, v.size,
+                                   f.ctypes.data if f.size else None, f.size, C.byref(h))
+        return _result(st, self._w), int(h.value)
+
+    def remove_obstacle(self, handle: int) -> Result:
+        return _result(lib.silk_remove_obstacle(self._w, handle), self._w)
+
+    def set_obstacle_collision_config(self, handle: int, config: CollisionConfig) -> Result:
+        c = config.to_c()
+        return _result(lib.silk_set_obstacle_collision_config(self._w, handle, C.byref(c)),
+                       self._w)
+
+    def set_obstacle_position(self, handle: int, position) -> Result:
+        p = _f32(position)
+        return _result(lib.silk_set_obstacle_position(self._w, handle, p, p.size), self._w)
+
+    # --- extensions ---
+    def set_solver_options(self, options: SolverOptions) -> Result:
+        o = options.to_c()
+        return _result(lib.silk_set_solver_options(self._w, C.byref(o)), self._w)
+
+    def step_stats(self) -> StepStats:
+        s = _StepStatsC()
+        lib.silk_get_step_stats(self._w, C.byref(s))
+        return StepStats(**{n: getattr(s, n) for n in StepStats.__dataclass_fields__})
+
+    def set_stream(self, cuda_stream: int | None) -> Result:
+        return _result(lib.silk_set_stream(self._w, cuda_stream or None), self._w)
+
+    # --- inspection ---
+    def cloth_partition(self, handle: int, nv: int) -> tuple[np.ndarray, np.ndarray]:
+        perm = np.zeros(nv, np.int32)
+        offs = np.zeros(nv + 1, np.int32)
+        n = C.c_int32(0)
+        st = lib.silk_debug_cloth_partition(self._w, handle, perm, nv, offs, nv + 1,
+                                            C.byref(n))
+        if st:
+            raise RuntimeError(_result(st, self._w).to_string())
+        return perm, offs[: n.value + 1].copy()
+
+    def cloth_matrix(self, handle: int, nv: int) -> np.ndarray:
+        d = np.zeros(nv * nv, np.float64)
+        st = lib.silk_debug_cloth_matrix(self._w, handle, d, d.size)
+        if st:
+            raise RuntimeError(_result(st, self._w).to_string())
+        return d.reshape(nv, nv)
+
+    def debug_refit(self, disp=None) -> None:
+        if disp is None:
+            st = lib.silk_debug_refit(self._w, None, 0)
+        else:
+            d = _f32(disp)
+            st = lib.silk_debug_refit(self._w, d.ctypes.data, d.size)
+        if st:
+            raise RuntimeError(_result(st, self._w).to_string())
+
+    def debug_candidates(self, cap: int = 1 << 22) -> np.ndarray:
+        out = np.zeros(5 * cap, np.int32)
+        n = C.c_int32(0)
+        st = lib.silk_debug_candidates(self._w, out, cap, C.byref(n))
+        if st:
+            raise RuntimeError(_result(st, self._w).to_string())
+        return out[: 5 * min(n.value, cap)].reshape(-1, 5)
+
+    def debug_dcd(self, t: float, activation: float, cap: int = 1 << 20) -> np.ndarray:
+        out = np.zeros(7 * cap, np.int32)
+        n = C.c_int32(0)
+        st = lib.silk_debug_dcd(self._w, t, activation, out, cap, C.byref(n))
+        if st:
+            raise RuntimeError(_result(st, self._w).to_string())
+        return out[: 7 * min(n.value, cap)].reshape(-1, 7)
+
+    def debug_min_toi(self, time_start: float, max_time: float,
+                      min_separation: float) -> tuple[float, int, int]:
+        toi = C.c_float(0)
+        nq, nh = C.c_int32(0), C.c_int32(0)
+        st = lib.silk_debug_min_toi(self._w, time_start, max_time, min_separation,
+                                    C.byref(toi), C.byref(nq), C.byref(nh))
+        if st:
+            raise RuntimeError(_result(st, self._w).to_string())
+        return toi.value, nq.value, nh.value
+
+
+def ccd_batch(is_vertex_face: bool, x: np.ndarray, err3, min_separation,
+              tolerance: float = 1e-6, max_iter: int = 4096, max_time: float = 1.0):
+    """GPU Tight-Inclusion CCD over n queries (x: n x 24 floats)."""
+    x = _f32(x)
+    n = x.size // 24
+    ms = _f32(np.broadcast_to(np.asarray(min_separation, np.float32), (n,)))
+    hit = np.zeros(n, np.int32)
+    toi = np.zeros(n, np.float32)
+    tup = np.zeros(n, np.float32)
+    st = lib.silk_ccd_batch(int(is_vertex_face), x, n, _f32(err3), ms, tolerance, max_iter,
+                            max_time, hit, toi, tup)
+    if st:
+        raise RuntimeError(_result(st).to_string())
+    return hit.astype(bool), toi, tup
+
+
+def partition_mesh(verts, faces) -> tuple[np.ndarray, np.ndarray]:
+    """(perm original->solver, part offsets) of the MAS vertex partition."""
+    v, f = _f32(verts), _i32(faces)
+    nv = v.size // 3
+    perm = np.zeros(nv, np.int32)
+    offs = np.zeros(nv + 1, np.int32)
+    n = C.c_int32(0)
+    st = lib.silk_partition_mesh(v, v.size, f, f.size, perm, offs, offs.size, C.byref(n))
+    if st:
+        raise RuntimeError(_result(st).to_string())
+    return perm, offs[: n.value + 1].copy()
+
+
+def assemble_cloth_host(cloth: ClothConfig, verts, faces, dt: float):
+    """Host assembly in solver order: (L dense, mass, contact weight, bending rhs)."""
+    v, f = _f32(verts), _i32(faces)
+    nv = v.size // 3
+    L = np.zeros(nv * nv, np.float64)
+    m = np.zeros(nv, np.float64)
+    w = np.zeros(nv, np.float64)
+    b = np.zeros(3 * nv, np.float64)
+    c = cloth.to_c()
+    st = lib.silk_assemble_cloth_host(C.byref(c), v, v.size, f, f.size, dt, L.ctypes.data,
+                                      m.ctypes.data, w.ctypes.data, b.ctypes.data)
+    if st:
+        raise RuntimeError(_result(st).to_string())
+    return L.reshape(nv, nv), m, w, b
+
+
+def color_contacts(verts4: np.ndarray, prio: np.ndarray) -> tuple[np.ndarray, int]:
+    v = _i32(verts4)
+    p = np.ascontiguousarray(np.asarray(prio, np.uint64).ravel())
+    colors = np.zeros(p.size, np.int32)
+    nc = C.c_int32(0)
+    st = lib.silk_color_contacts(v, p, p.size, colors, C.byref(nc))
+    if st:
+        raise RuntimeError(_result(st).to_string())
+    return colors, nc.value

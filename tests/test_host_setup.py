@@ -1,0 +1,98 @@
+"""Host-side setup checked against the oracle (no GPU needed)."""
+import numpy as np
+import pytest
+
+from silk_physics_b200 import native as N
+from silk_physics_b200 import scenes as S
+
+
+def _connected(verts_ids, adj):
+    seen = {verts_ids[0]}
+    todo = [verts_ids[0]]
+    members = set(verts_ids)
+    while todo:
+        u = todo.pop()
+        for w in adj[u]:
+            if w in members and w not in seen:
+                seen.add(w)
+                todo.append(w)
+    return len(seen) == len(members)
+
+
+@pytest.mark.parametrize("s", [5, 17, 32, 57])
+def test_partition_invariants(s):
+    """graph_partition_test.cpp: parts non-empty, ids in range, size <= 32;
+    ours are also connected (one coarse node per bank)."""
+    V, F = S.grid_sheet(s)
+    perm, offs = N.partition_mesh(V, F)
+    nv = len(V)
+    assert sorted(perm.tolist()) == list(range(nv))
+    sizes = np.diff(offs)
+    assert offs[0] == 0 and offs[-1] == nv
+    assert sizes.min() >= 1 and sizes.max() <= 32
+    adj = [set() for _ in range(nv)]
+    for a, b, c in F:
+        for x, y in ((a, b), (b, c), (c, a)):
+            adj[x].add(y)
+            adj[y].add(x)
+    inv = np.argsort(perm)
+    for p in range(len(sizes)):
+        assert _connected(inv[offs[p]:offs[p + 1]].tolist(), adj)
+
+
+@pytest.mark.parametrize("cloth", [N.ClothConfig(), N.ClothConfig(250.0, 0.01, 0.2, 0.05)])
+def test_assembly_matches_reference_assembly(oracle, cloth):
+    """The decoupled scalar L equals the 3x3-block system the reference
+    assembles from 6x9 Jacobians (cloth_assembly_l2_cache.cpp:71-136), and
+    the full matrix is exactly kron(L, I3)."""
+    V, F = S.grid_sheet(12, jitter=1e-3, seed=3)
+    perm, offs = N.partition_mesh(V, F)
+    L, m, w, b = N.assemble_cloth_host(cloth, V, F, 1.0 / 60.0)
+    ow = oracle.OracleWorld(fp64=True)
+    h = ow.add_cloth(V, F, [], perm, offs, cloth=(cloth.elastic_stiffness,
+                                                 cloth.bending_stiffness, cloth.density,
+                                                 cloth.damping))
+    Lo = ow.scalar_matrix(h)
+    full = ow.full_matrix(h)
+    assert np.abs(L - Lo).max() <= 1e-10 * np.abs(Lo).max()
+    assert np.abs(full - np.kron(Lo, np.eye(3))).max() <= 1e-14 * np.abs(Lo).max()
+    mo, cwo, bro = ow.vectors(h)
+    np.testing.assert_allclose(m, mo[0::3], rtol=1e-12)
+    np.testing.assert_allclose(w, cwo[0::3], rtol=1e-9)
+    np.testing.assert_allclose(b, bro, rtol=1e-9, atol=1e-14)
+    assert np.allclose(L, L.T)
+
+
+def test_mesh_validation_codes():
+    """mesh.cpp:231-276 rules through the host assembly entry point."""
+    V, F = S.grid_sheet(4)
+    cfg = N.ClothConfig()
+
+    def code(v, f):
+        try:
+            N.assemble_cloth_host(cfg, v, f, 1 / 60)
+            return "ok"
+        except RuntimeError as e:
+            return str(e)
+
+    assert code(V, F) == "ok"
+    bad = V.copy()
+    bad[3, 0] = np.nan
+    assert code(bad, F).startswith("InvalidMesh")
+    f2 = F.copy()
+    f2[0, 0] = len(V)
+    assert code(V, f2).startswith("InvalidMesh")
+    f3 = F.copy()
+    f3[0, 1] = f3[0, 0]
+    assert code(V, f3).startswith("InvalidMesh")
+    # Sliver triangle below 0.5 degrees.
+    sv = np.array([[0, 0, 0], [1, 0, 0], [0.5, 1e-3, 0]], np.float32)
+    assert code(sv, np.array([[0, 1, 2]], np.int32)).startswith("InvalidMesh")
+    # Two disconnected triangles.
+    tv = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [5, 0, 0], [6, 0, 0], [5, 1, 0]],
+                  np.float32)
+    assert code(tv, np.array([[0, 1, 2], [3, 4, 5]], np.int32)).startswith("InvalidMesh")
+    # Non-manifold edge: three triangles on one edge.
+    nv = np.array([[0, 0, 0], [1, 0, 0], [0.5, 1, 0], [0.5, -1, 0], [0.5, 0, 1]], np.float32)
+    nf = np.array([[0, 1, 2], [1, 0, 3], [0, 1, 4]], np.int32)
+    assert code(nv, nf).startswith("InvalidMesh")
