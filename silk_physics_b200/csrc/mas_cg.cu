@@ -16,13 +16,13 @@
 //    fixed order by every block).
 #include <cuda/atomic>
 
+#include "grid_barrier.cuh"
 #include "mas_cg.cuh"
 
 namespace silkb {
 
 namespace {
 
-constexpr long long kSpinLimit = 1ll << 25;  // ~2 s with the back-off below
 constexpr int kCgThreads = 256;
 constexpr int kCgWarps = kCgThreads / 32;
 
@@ -92,55 +92,6 @@ __global__ void __launch_bounds__(256) bank_invert_kernel(
     if (lv.Mb) lv.Mb[(size_t)bank * kPacked + idx] = __float2bfloat16_rn((float)v);
   }
 }
-
-// ------------------------------------------------------------------------
-// Grid barrier for a cooperative launch, with a bounded wait: when the
-// iteration limit runs out the kernel records an error and every block
-// leaves at its next barrier.
-// ------------------------------------------------------------------------
-struct GridBarrier {
-  unsigned* count;
-  unsigned* err;
-  unsigned* gen;
-  unsigned nblocks;
-
-  __device__ bool sync() {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      cuda::atomic_ref<unsigned, cuda::thread_scope_device> g(*gen), c(*count),
-          e(*err);
-      int ok = 1;
-      unsigned my = g.load(cuda::memory_order_relaxed);
-      if (e.load(cuda::memory_order_relaxed) != 0u) {
-        ok = 0;
-      } else {
-        unsigned arrived = c.fetch_add(1u, cuda::memory_order_acq_rel);
-        if (arrived == nblocks - 1u) {
-          c.store(0u, cuda::memory_order_relaxed);
-          g.fetch_add(1u, cuda::memory_order_release);
-        } else {
-          long long spins = 0;
-          while (g.load(cuda::memory_order_acquire) == my) {
-            if (e.load(cuda::memory_order_relaxed) != 0u) {
-              ok = 0;
-              break;
-            }
-            if (++spins > kSpinLimit) {
-              e.store(1u, cuda::memory_order_relaxed);
-              ok = 0;
-              break;
-            }
-            __nanosleep(32);
-          }
-        }
-      }
-      s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
-  }
-};
 
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
