@@ -85,8 +85,21 @@ typedef struct {
                                  admm_solver.cu:228-233 */
   int32_t cg_max_iter;        /* 1000 (mas_cg_solver.cuh:25) */
   int32_t mas_bf16;           /* 0: FP32 bank inverses; 1: BF16 storage */
-  int32_t reserved[5];
+  int32_t profile;            /* 1: time the CG kernel with CUDA events */
+  int32_t reserved[4];
 } silk_solver_options;
+
+/* CUDA-event timing of the persistent CG kernel over the steps since the
+ * last reset (silk_solver_options.profile = 1).  algorithmic_bytes counts
+ * compulsory DRAM traffic per CG iteration: matrix entries, MAS bank
+ * inverses and each vector read or written once. */
+typedef struct {
+  double cg_time_ms;
+  int64_t cg_launches;
+  int64_t cg_iterations;
+  double cg_algorithmic_bytes;
+  double reserved[4];
+} silk_profile;
 
 /* Statistics of the last solver_step. */
 typedef struct {
@@ -160,6 +173,11 @@ silk_status silk_get_step_stats(const silk_world* w, silk_step_stats* s);
 /* Launch all device work of this world on the given cudaStream_t (NULL =
  * the world's own stream).  Lets a caller time steps with its own events. */
 silk_status silk_set_stream(silk_world* w, void* cuda_stream);
+/* Kernel profile accumulated since the last reset; reset = 1 clears it. */
+silk_status silk_get_profile(silk_world* w, silk_profile* p, int32_t reset);
+/* Vertex velocities of a cloth in mesh order (3 * vertex count floats). */
+silk_status silk_get_cloth_velocity(const silk_world* w, uint32_t handle,
+                                    float* velocity, int64_t velocity_len);
 
 /* --- Inspection entry points used by the parity tests ------------------- */
 /* Solver-order permutation (original -> solver) and partition offsets. */

@@ -273,6 +273,9 @@ static int find_next_split(const float* w, const float* tol) {
   return best;
 }
 
+// Largest number of pending boxes seen by any search (sizes GPU storage).
+static thread_local size_t g_max_pending = 0;
+
 // interval_root_finder.cpp:390-510 (bucket DFS keyed by t.lower).
 template <bool VF>
 static std::optional<CCDResult> root_finder_bucket_dfs(
@@ -340,7 +343,12 @@ static std::optional<CCDResult> root_finder_bucket_dfs(
                        0.f, 0.f};
     }
     IBox tmp = cur;
-    auto push = [&](const IBox& b) { stacks[b[0].lower].push_back(b); };
+    auto push = [&](const IBox& b) {
+      stacks[b[0].lower].push_back(b);
+      size_t pending = 0;
+      for (auto& kv : stacks) pending += kv.second.size();
+      if (pending > g_max_pending) g_max_pending = pending;
+    };
     if (split == 0 || !VF) {
       tmp[split] = halves.second;
       push(tmp);
@@ -2279,6 +2287,25 @@ int oracle_solver_step(void* w) {
   return a->fp64 ? a->d->step() : a->f->step();
 }
 
+int oracle_set_cloth_state(void* w, uint32_t h, const float* x, const float* v,
+                           int n) {
+  AnyWorld* a = (AnyWorld*)w;
+  auto impl = [&](auto& W) {
+    for (auto& c : W.cloths)
+      if (c.id == h) {
+        if (n != 3 * c.nv) return 7;
+        for (int i = 0; i < c.nv; ++i)
+          for (int d = 0; d < 3; ++d) {
+            c.x[3 * c.perm[i] + d] = x[3 * i + d];
+            c.v[3 * c.perm[i] + d] = v[3 * i + d];
+          }
+        return 0;
+      }
+    return 4;
+  };
+  return a->fp64 ? impl(*a->d) : impl(*a->f);
+}
+
 int oracle_get_cloth_position(void* w, uint32_t h, float* out, int n) {
   AnyWorld* a = (AnyWorld*)w;
   auto impl = [&](auto& W) {
@@ -2432,6 +2459,12 @@ float oracle_debug_min_toi(void* w, float time_start, float max_time, float ms,
   AnyWorld* a = (AnyWorld*)w;
   return a->fp64 ? a->d->find_min_toi(time_start, max_time, ms, nq, nh)
                  : a->f->find_min_toi(time_start, max_time, ms, nq, nh);
+}
+
+long oracle_ccd_max_pending(int reset) {
+  long r = (long)g_max_pending;
+  if (reset) g_max_pending = 0;
+  return r;
 }
 
 int oracle_ccd(int is_vf, const float* x, const float* err, float ms, float tol,

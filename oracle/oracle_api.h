@@ -79,6 +79,9 @@ int oracle_add_obstacle(void* w, const oracle_collision_config* col,
 int oracle_set_obstacle_position(void* w, uint32_t h, const float* pos, int n);
 int oracle_set_cloth_pin_position(void* w, uint32_t h, const float* pos, int n);
 int oracle_solver_step(void* w);
+/* Overwrite a cloth's positions and velocities (original vertex order). */
+int oracle_set_cloth_state(void* w, uint32_t h, const float* x, const float* v,
+                           int n);
 int oracle_get_cloth_position(void* w, uint32_t h, float* out, int n);
 int oracle_get_cloth_position_f64(void* w, uint32_t h, double* out, int n);
 int oracle_get_stats(void* w, oracle_stats* s);

@@ -67,7 +67,7 @@ def lib() -> C.CDLL:
                      "oracle_get_cloth_position_f64", "oracle_get_stats",
                      "oracle_cloth_dense_scalar_matrix", "oracle_cloth_dense_full_matrix",
                      "oracle_cloth_vectors", "oracle_debug_candidates", "oracle_debug_refit",
-                     "oracle_debug_dcd"]:
+                     "oracle_debug_dcd", "oracle_set_cloth_state"]:
             getattr(_lib, name).restype = C.c_int
     return _lib
 
@@ -139,6 +139,12 @@ class OracleWorld:
 
     def step(self) -> int:
         return self.L.oracle_solver_step(self.w)
+
+    def set_state(self, h, x, v):
+        xs = np.ascontiguousarray(x, np.float32).ravel()
+        vs = np.ascontiguousarray(v, np.float32).ravel()
+        return self.L.oracle_set_cloth_state(self.w, h, _p(xs, C.c_float), _p(vs, C.c_float),
+                                             xs.size)
 
     def position(self, h) -> np.ndarray:
         out = np.zeros(3 * self.nv[h], np.float64)

@@ -200,6 +200,19 @@ silk_status silk_set_stream(silk_world* w, void* cuda_stream) {
   return guard_init(w, [&](World& W) { return W.set_stream(cuda_stream); });
 }
 
+silk_status silk_get_profile(silk_world* w, silk_profile* p, int32_t reset) {
+  if (!p) return SILK_ERR_INVALID_CONFIG;
+  return guard(w, [&](World& W) { return W.get_profile(p, reset != 0); });
+}
+
+silk_status silk_get_cloth_velocity(const silk_world* w, uint32_t handle,
+                                    float* velocity, int64_t velocity_len) {
+  if (!velocity && velocity_len != 0) return SILK_ERR_INVALID_POSITION;
+  return guard_init(const_cast<silk_world*>(w), [&](World& W) {
+    return W.get_cloth_velocity(handle, velocity, velocity_len);
+  });
+}
+
 silk_status silk_debug_cloth_partition(const silk_world* w, uint32_t handle,
                                        int32_t* perm, int64_t perm_len,
                                        int32_t* part_offsets,

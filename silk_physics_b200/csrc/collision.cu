@@ -44,7 +44,8 @@ constexpr float kDcdEps = 1e-6f;       // dcd.cu:18
 constexpr int kCcdMaxIter = 4096;      // main_loop.cuh:24
 constexpr float kCcdTolerance = 1e-6f; // main_loop.cuh:23
 constexpr int kGsSweeps = 10;          // contact_constraints.cuh:89
-constexpr int kCcdStack = 256;
+constexpr int kCcdStack = 96;
+constexpr int kCcdSpillChunk = 512;  // overflowed queries per second pass
 
 // std::min / std::max semantics.
 __device__ __forceinline__ float smin(float a, float b) { return (b < a) ? b : a; }
@@ -637,8 +638,14 @@ __device__ float clamp_div(float a, float b, float mx) {
   return smin(a / b, mx);
 }
 
+// Pending boxes of one search: a small per-thread array for the first pass;
+// queries that outgrow it are re-run with a global-memory array of
+// max_iter + 2 entries, the most a search can hold (each evaluation pops one
+// box and pushes at most two, and pushes stop after max_iter evaluations).
 struct DfsStack {
-  IBox e[kCcdStack];
+  IBox local[kCcdStack];
+  IBox* e;
+  int cap;
   int n;
 };
 
@@ -674,7 +681,7 @@ __device__ int root_finder(bool vf, const float3* Pt, const float* tol,
   // smallest t.lower first and, for equal t.lower, the most recently pushed
   // (the std::map of per-t.lower stacks of the reference).
   auto push = [&](const IBox& b) -> bool {
-    if (st.n >= kCcdStack) return false;
+    if (st.n >= st.cap) return false;
     int pos = st.n;
     while (pos > 0 && st.e[pos - 1].t0 < b.t0) --pos;
     for (int k = st.n; k > pos; --k) st.e[k] = st.e[k - 1];
@@ -823,13 +830,35 @@ __device__ void trajectory(const ObjDev& o, int v, float ts, float interval,
   }
 }
 
+// Storage of the pending boxes: with spill == nullptr the thread-local array
+// (first pass), else a global slice of spill_cap boxes per query (second
+// pass over the queries whose first pass overflowed).
+struct CcdSpill {
+  IBox* spill;
+  int spill_cap;
+  const int* list;    // second pass: query indices
+  int* overflow;      // first pass: queries to re-run
+  int* n_overflow;
+};
+
+__device__ __forceinline__ void bind_stack(DfsStack& st, const CcdSpill& sp, int i) {
+  if (sp.spill) {
+    st.e = sp.spill + (size_t)i * sp.spill_cap;
+    st.cap = sp.spill_cap;
+  } else {
+    st.e = st.local;
+    st.cap = kCcdStack;
+  }
+}
+
 __global__ void __launch_bounds__(kCollThreads) ccd_kernel(
     const ObjDev* objs, const int4* cand, int n, float ts, float interval,
     float ms, float3 vf_err, float3 ee_err, float local_tol, unsigned* min_bits,
-    int* counts) {
+    int* counts, CcdSpill sp) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  int4 c = cand[i];
+  int q = sp.list ? sp.list[i] : i;
+  int4 c = cand[q];
   int kind = c.z >> 16, sa = c.z & 0xffff, sb = c.w;
   const ObjDev& A = objs[sa];
   const ObjDev& B = objs[sb];
@@ -854,31 +883,44 @@ __global__ void __launch_bounds__(kCollThreads) ccd_kernel(
   err[1] = e.y;
   err[2] = e.z;
   DfsStack st;
+  bind_stack(st, sp, i);
   float toi = 1.0f, tup = 1.0f;
   float local_max = interval / interval;
   int s = ccd_query(vf, Pt, err, ms, local_tol, kCcdMaxIter, local_max, toi, tup, st);
+  if (s == 2) {
+    if (!sp.spill) sp.overflow[atomicAdd(sp.n_overflow, 1)] = q;
+    else atomicAdd(&counts[1], 1);
+    return;
+  }
   if (s == 0) return;
   atomicAdd(&counts[0], 1);
-  if (s == 2) atomicAdd(&counts[1], 1);
   if (toi == 0.0f) return;
   atomicMin(min_bits, __float_as_uint(toi));  // toi >= 0: bit order = value order
 }
 
 __global__ void ccd_batch_kernel(bool vf, const float* x, int n, float3 err,
                                  const float* ms, float tol, int max_iter,
-                                 float max_time, int* hit, float* toi, float* tup) {
+                                 float max_time, int* hit, float* toi, float* tup,
+                                 int* n_bad, CcdSpill sp) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  int q = sp.list ? sp.list[i] : i;
   float3 Pt[8];
   for (int k = 0; k < 8; ++k)
-    Pt[k] = make_float3(x[24 * i + 3 * k], x[24 * i + 3 * k + 1], x[24 * i + 3 * k + 2]);
+    Pt[k] = make_float3(x[24 * q + 3 * k], x[24 * q + 3 * k + 1], x[24 * q + 3 * k + 2]);
   float e[3] = {err.x, err.y, err.z};
   DfsStack st;
+  bind_stack(st, sp, i);
   float t = max_time, u = max_time;
-  int s = ccd_query(vf, Pt, e, ms[i], tol, max_iter, max_time, t, u, st);
-  hit[i] = s != 0 ? 1 : 0;
-  toi[i] = s != 0 ? t : max_time;
-  if (tup) tup[i] = s != 0 ? u : max_time;
+  int s = ccd_query(vf, Pt, e, ms[q], tol, max_iter, max_time, t, u, st);
+  if (s == 2) {
+    if (!sp.spill) sp.overflow[atomicAdd(sp.n_overflow, 1)] = q;
+    else atomicAdd(n_bad, 1);
+    return;
+  }
+  hit[q] = s != 0 ? 1 : 0;
+  toi[q] = s != 0 ? t : max_time;
+  if (tup) tup[q] = s != 0 ? u : max_time;
 }
 
 // ---------------------------------------------------------------------------
@@ -1148,7 +1190,9 @@ struct CollisionImpl {
   DevBuf<CollisionDev> cols;
   int cols_cap = 0;
   DevBuf<unsigned> min_bits;
-  DevBuf<int> ccd_counts;
+  DevBuf<int> ccd_counts;  // [hits, storage overflows, first-pass spills]
+  DevBuf<int> ccd_overflow;
+  DevBuf<IBox> ccd_spill;
   // Contacts.
   std::set<Key> keys;
   std::vector<Key> key_list;
@@ -1171,7 +1215,7 @@ CollisionSystem::CollisionSystem(World& w) : w_(w), impl_(new CollisionImpl) {
   CUDA_CHECK(cudaMemset(impl_->active_dof.p, 0, sizeof(int)));
   impl_->counter.alloc(4);
   impl_->min_bits.alloc(1);
-  impl_->ccd_counts.alloc(2);
+  impl_->ccd_counts.alloc(3);
   impl_->jp_flags.alloc(2);
   impl_->gs_barrier.alloc(4);
   CUDA_CHECK(cudaMemset(impl_->gs_barrier.p, 0, 4 * sizeof(unsigned)));
@@ -1740,17 +1784,32 @@ float CollisionSystem::min_toi(float ts, float max_time, float ms, int* nq, int*
   float one = max_time / max_time;
   std::memcpy(&one_bits, &one, 4);
   CUDA_CHECK(cudaMemcpyAsync(I.min_bits.p, &one_bits, 4, cudaMemcpyHostToDevice, st));
-  CUDA_CHECK(cudaMemsetAsync(I.ccd_counts.p, 0, 2 * sizeof(int), st));
+  CUDA_CHECK(cudaMemsetAsync(I.ccd_counts.p, 0, 3 * sizeof(int), st));
+  if ((int)I.ccd_overflow.n < n) I.ccd_overflow.alloc(n + n / 4);
+  CcdSpill first{nullptr, 0, nullptr, I.ccd_overflow.p, I.ccd_counts.p + 2};
   ccd_kernel<<<div_up(n, kCollThreads), kCollThreads, 0, st>>>(
       I.table_d.p, I.cand.p, n, ts, max_time, ms, vf, ee, local_tol, I.min_bits.p,
-      I.ccd_counts.p);
+      I.ccd_counts.p, first);
   SILK_LAUNCHED();
+  int counts[3];
+  CUDA_CHECK(cudaMemcpyAsync(counts, I.ccd_counts.p, sizeof(counts), cudaMemcpyDeviceToHost, st));
+  CUDA_CHECK(cudaStreamSynchronize(st));
+  // Second pass for the searches that outgrew the per-thread array.
+  const int cap = kCcdMaxIter + 2;
+  for (int start = 0; start < counts[2]; start += kCcdSpillChunk) {
+    int m = std::min(kCcdSpillChunk, counts[2] - start);
+    if (I.ccd_spill.n < (size_t)kCcdSpillChunk * cap) I.ccd_spill.alloc((size_t)kCcdSpillChunk * cap);
+    CcdSpill second{I.ccd_spill.p, cap, I.ccd_overflow.p + start, nullptr, nullptr};
+    ccd_kernel<<<div_up(m, kCollThreads), kCollThreads, 0, st>>>(
+        I.table_d.p, I.cand.p, m, ts, max_time, ms, vf, ee, local_tol, I.min_bits.p,
+        I.ccd_counts.p, second);
+    SILK_LAUNCHED();
+  }
   unsigned bits = 0;
-  int counts[2];
   CUDA_CHECK(cudaMemcpyAsync(&bits, I.min_bits.p, 4, cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaMemcpyAsync(counts, I.ccd_counts.p, sizeof(counts), cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaStreamSynchronize(st));
-  if (counts[1] > 0) throw CudaError("CCD search stack overflow");
+  if (counts[1] > 0) throw CudaError("CCD search storage overflow");
   *nh = counts[0];
   float local;
   std::memcpy(&local, &bits, 4);
@@ -1822,11 +1881,37 @@ void ccd_batch_host(bool vf, const float* x, int64_t n, const float* err3,
   hitd.alloc(n);
   CUDA_CHECK(cudaMemcpy(xd.p, x, 24 * n * sizeof(float), cudaMemcpyHostToDevice));
   CUDA_CHECK(cudaMemcpy(msd.p, ms, n * sizeof(float), cudaMemcpyHostToDevice));
+  DevBuf<int> over, counts;
+  over.alloc(n);
+  counts.alloc(2);
+  CUDA_CHECK(cudaMemset(counts.p, 0, 2 * sizeof(int)));
+  float3 e3 = make_float3(err3[0], err3[1], err3[2]);
+  CcdSpill first{nullptr, 0, nullptr, over.p, counts.p};
   ccd_batch_kernel<<<div_up((int)n, kCollThreads), kCollThreads>>>(
-      vf, xd.p, (int)n, make_float3(err3[0], err3[1], err3[2]), msd.p, tol, max_iter,
-      max_time, hitd.p, toid.p, tupd.p);
+      vf, xd.p, (int)n, e3, msd.p, tol, max_iter, max_time, hitd.p, toid.p, tupd.p,
+      counts.p + 1, first);
   SILK_LAUNCHED();
   CUDA_CHECK(cudaGetLastError());
+  int h[2];
+  CUDA_CHECK(cudaMemcpy(h, counts.p, sizeof(h), cudaMemcpyDeviceToHost));
+  if (h[0] > 0) {
+    // Second pass with max_iter + 2 pending boxes per search (unbounded
+    // searches, max_iter <= 0, get 65536).
+    int cap = max_iter > 0 ? max_iter + 2 : 65536;
+    int chunk = std::max(1, std::min(h[0], (int)((256ll << 20) / ((long long)cap * sizeof(IBox)))));
+    DevBuf<IBox> spill;
+    spill.alloc((size_t)chunk * cap);
+    for (int start = 0; start < h[0]; start += chunk) {
+      int m = std::min(chunk, h[0] - start);
+      CcdSpill second{spill.p, cap, over.p + start, nullptr, nullptr};
+      ccd_batch_kernel<<<div_up(m, kCollThreads), kCollThreads>>>(
+          vf, xd.p, m, e3, msd.p, tol, max_iter, max_time, hitd.p, toid.p, tupd.p,
+          counts.p + 1, second);
+      SILK_LAUNCHED();
+    }
+    CUDA_CHECK(cudaMemcpy(h, counts.p, sizeof(h), cudaMemcpyDeviceToHost));
+    if (h[1] > 0) throw CudaError("CCD search storage overflow");
+  }
   CUDA_CHECK(cudaMemcpy(hit, hitd.p, n * sizeof(int), cudaMemcpyDeviceToHost));
   CUDA_CHECK(cudaMemcpy(toi, toid.p, n * sizeof(float), cudaMemcpyDeviceToHost));
   if (t_upper) CUDA_CHECK(cudaMemcpy(t_upper, tupd.p, n * sizeof(float), cudaMemcpyDeviceToHost));

@@ -30,6 +30,10 @@ World::World() {
 
 World::~World() {
   coll_.reset();
+  for (auto& e : events) {
+    cudaEventDestroy(e.first);
+    cudaEventDestroy(e.second);
+  }
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -451,6 +455,20 @@ void World::build_cloth_device(Cloth& c) {
   d.barrier.zero(st);
   d.result.alloc(2);
   d.result_rr.alloc(1);
+  d.stats.alloc(2);
+  d.stats.zero(st);
+  // Compulsory DRAM bytes of one CG iteration: off-diagonal entries (8 B),
+  // per row Ldiag + dynamic diagonal + p read + Ap write (40 B) in the SpMV
+  // phase, r/p/Ap/x read + x/r/z0 write (112 B) in the fine MAS phase, z0/p/
+  // cmap read + p write (64 B) in the prolongation, plus every bank inverse.
+  {
+    long nnz_off = (long)S.Lcols.size() - nv;
+    long banks = S.fine.nbank;
+    for (auto& c : S.coarse) banks += c.nbank;
+    double base = 8.0 * nnz_off + 216.0 * nv;
+    d.bytes_per_iter_fp32 = base + (double)banks * kPacked * 4.0;
+    d.bytes_per_iter_bf16 = base + (double)banks * kPacked * 2.0;
+  }
   // CG argument template (vectors are bound per solve).
   CgArgs& a = d.cg;
   a = CgArgs{};
@@ -594,7 +612,6 @@ void World::ensure_layout() {
   face_partials.alloc((size_t)face_step_blocks(nf) * kAdmmSlots);
   vertex_partials.alloc((size_t)vertex_step_blocks(nv) * kAdmmSlots);
   ctl.alloc(1);
-  cg_stats.alloc(2);
   pinned_dof = 0;
   for (auto& c : cloths) c->on_device = true;
   pins_dirty_ = true;
@@ -658,8 +675,50 @@ void World::cg_solve(Cloth& c, float rel_tol) {
   a.rel_tol = rel_tol;
   a.abs_tol = g.linear_solver_abs_tol;
   a.max_iter = opt.cg_max_iter > 0 ? opt.cg_max_iter : 1000;
-  a.stats = cg_stats.p;
-  launch_cg(a, c.dev.cg_grid, stream);
+  a.stats = c.dev.stats.p;
+  if (opt.profile) {
+    if (events_used == events.size()) {
+      cudaEvent_t e0, e1;
+      CUDA_CHECK(cudaEventCreate(&e0));
+      CUDA_CHECK(cudaEventCreate(&e1));
+      events.emplace_back(e0, e1);
+    }
+    auto& ev = events[events_used++];
+    CUDA_CHECK(cudaEventRecord(ev.first, stream));
+    launch_cg(a, c.dev.cg_grid, stream);
+    CUDA_CHECK(cudaEventRecord(ev.second, stream));
+  } else {
+    launch_cg(a, c.dev.cg_grid, stream);
+  }
+}
+
+silk_status World::get_profile(silk_profile* p, bool reset) {
+  *p = prof;
+  if (reset) prof = silk_profile{};
+  return SILK_OK;
+}
+
+silk_status World::get_cloth_velocity(uint32_t h, float* out, int64_t n) {
+  Cloth* c = find_cloth(h);
+  if (!c) return SILK_ERR_INVALID_HANDLE;
+  int nv = c->nv();
+  if (n != 3 * (int64_t)nv) return SILK_ERR_INVALID_POSITION;
+  if (!c->on_device) {
+    std::memcpy(out, c->v_host.data(), sizeof(float) * 3 * nv);
+    return SILK_OK;
+  }
+  std::vector<float4> vs(nv);
+  CUDA_CHECK(cudaMemcpyAsync(vs.data(), sv.p + c->voff, nv * sizeof(float4),
+                             cudaMemcpyDeviceToHost, stream));
+  sync();
+  const auto& perm = c->setup->perm;
+  for (int i = 0; i < nv; ++i) {
+    float4 q = vs[perm[i]];
+    out[3 * i] = q.x;
+    out[3 * i + 1] = q.y;
+    out[3 * i + 2] = q.z;
+  }
+  return SILK_OK;
 }
 
 bool World::admm_solve() {
@@ -728,7 +787,8 @@ silk_status World::solver_step() {
     upload_pins();
     cudaStream_t st = stream;
     int nv = nv_total;
-    cg_stats.zero(st);
+    for (auto& c : cloths) c->dev.stats.zero(st);
+    events_used = 0;
     // init (main_loop.cu:24-76): damped velocity, fresh ADMM aux variables.
     launch_damp(nv, damp.p, sv.p, prev_v.p, st);
     zu.zero(st);
@@ -780,11 +840,29 @@ silk_status World::solver_step() {
     // Final velocity from the whole accepted displacement (main_loop.cu:248).
     launch_velocity(nv, g.dt, outer.p, sx.p, sv.p, st);
     CUDA_CHECK(cudaMemcpyAsync(sx.p, outer.p, nv * sizeof(float4), cudaMemcpyDeviceToDevice, st));
-    int cgs[2];
-    CUDA_CHECK(cudaMemcpyAsync(cgs, cg_stats.p, sizeof(cgs), cudaMemcpyDeviceToHost, st));
+    std::vector<int> cgs(2 * cloths.size());
+    for (size_t k = 0; k < cloths.size(); ++k)
+      CUDA_CHECK(cudaMemcpyAsync(&cgs[2 * k], cloths[k]->dev.stats.p, 2 * sizeof(int),
+                                 cudaMemcpyDeviceToHost, st));
     sync();
-    stats.cg_iterations = cgs[0];
-    stats.cg_solves = cgs[1];
+    for (size_t k = 0; k < cloths.size(); ++k) {
+      stats.cg_iterations += cgs[2 * k];
+      stats.cg_solves += cgs[2 * k + 1];
+      if (opt.profile) {
+        double bpi = opt.mas_bf16 ? cloths[k]->dev.bytes_per_iter_bf16
+                                  : cloths[k]->dev.bytes_per_iter_fp32;
+        prof.cg_algorithmic_bytes += bpi * (cgs[2 * k] + cgs[2 * k + 1]);
+        prof.cg_iterations += cgs[2 * k];
+      }
+    }
+    if (opt.profile) {
+      for (size_t e = 0; e < events_used; ++e) {
+        float ms = 0.f;
+        CUDA_CHECK(cudaEventElapsedTime(&ms, events[e].first, events[e].second));
+        prof.cg_time_ms += ms;
+      }
+      prof.cg_launches += (int64_t)events_used;
+    }
     if (coll_) {
       stats.contacts = coll_->contact_count();
       stats.colors = coll_->color_count();

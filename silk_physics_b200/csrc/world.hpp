@@ -85,8 +85,11 @@ struct ClothDev {
   DevBuf<unsigned> barrier;
   DevBuf<int> result;
   DevBuf<float> result_rr;
+  DevBuf<int> stats;  // accumulated [iterations, solves] of this cloth
   CgArgs cg;
   int cg_grid = 1;
+  double bytes_per_iter_fp32 = 0.0;  // algorithmic DRAM bytes per CG iteration
+  double bytes_per_iter_bf16 = 0.0;
 };
 
 struct Cloth {
@@ -153,6 +156,8 @@ class World {
   silk_status set_obstacle_position(uint32_t h, const float* pos, int64_t n);
   silk_status set_solver_options(const silk_solver_options& o);
   silk_status set_stream(void* s);
+  silk_status get_profile(silk_profile* p, bool reset);
+  silk_status get_cloth_velocity(uint32_t h, float* out, int64_t n);
 
   // Inspection.
   silk_status debug_partition(uint32_t h, int* perm, int64_t perm_len,
@@ -185,8 +190,10 @@ class World {
   DevBuf<int> vf_off, vf_list;
   DevBuf<double> face_partials, vertex_partials;
   DevBuf<AdmmControl> ctl;
-  DevBuf<int> cg_stats;  // [iterations, solves]
   int pinned_dof = 0;
+  silk_profile prof{};
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+  size_t events_used = 0;
 
   Cloth* find_cloth(uint32_t h);
   Obstacle* find_obstacle(uint32_t h);

@@ -75,7 +75,13 @@ class _CollisionConfigC(C.Structure):
 
 class _SolverOptionsC(C.Structure):
     _fields_ = [("fixed_linear_rel_tol", C.c_float), ("cg_max_iter", C.c_int32),
-                ("mas_bf16", C.c_int32), ("reserved", C.c_int32 * 5)]
+                ("mas_bf16", C.c_int32), ("profile", C.c_int32), ("reserved", C.c_int32 * 4)]
+
+
+class _ProfileC(C.Structure):
+    _fields_ = [("cg_time_ms", C.c_double), ("cg_launches", C.c_int64),
+                ("cg_iterations", C.c_int64), ("cg_algorithmic_bytes", C.c_double),
+                ("reserved", C.c_double * 4)]
 
 
 class _StepStatsC(C.Structure):
@@ -144,12 +150,14 @@ class SolverOptions:
     fixed_linear_rel_tol: float = 0.0
     cg_max_iter: int = 1000
     mas_bf16: bool = False
+    profile: bool = False
 
     def to_c(self) -> _SolverOptionsC:
         o = _SolverOptionsC()
         o.fixed_linear_rel_tol = self.fixed_linear_rel_tol
         o.cg_max_iter = self.cg_max_iter
         o.mas_bf16 = int(self.mas_bf16)
+        o.profile = int(self.profile)
         return o
 
 
@@ -210,6 +218,8 @@ def _load() -> C.CDLL:
         "silk_set_solver_options": ([_W, C.POINTER(_SolverOptionsC)], C.c_int),
         "silk_get_step_stats": ([_W, C.POINTER(_StepStatsC)], C.c_int),
         "silk_set_stream": ([_W, C.c_void_p], C.c_int),
+        "silk_get_profile": ([_W, C.POINTER(_ProfileC), C.c_int32], C.c_int),
+        "silk_get_cloth_velocity": ([_W, C.c_uint32, _F32P, C.c_int64], C.c_int),
         "silk_debug_cloth_partition": ([_W, C.c_uint32, _I32P, C.c_int64, _I32P, C.c_int64,
                                         C.POINTER(C.c_int32)], C.c_int),
         "silk_debug_cloth_matrix": ([_W, C.c_uint32, _F64P, C.c_int64], C.c_int),
@@ -367,6 +377,15 @@ class World:
 
     def set_stream(self, cuda_stream: int | None) -> Result:
         return _result(lib.silk_set_stream(self._w, cuda_stream or None), self._w)
+
+    def profile(self, reset: bool = False) -> dict:
+        p = _ProfileC()
+        lib.silk_get_profile(self._w, C.byref(p), int(reset))
+        return {n: getattr(p, n) for n, _ in _ProfileC._fields_ if n != "reserved"}
+
+    def get_cloth_velocity(self, handle: int, velocity: np.ndarray) -> Result:
+        return _result(lib.silk_get_cloth_velocity(self._w, handle, velocity.reshape(-1),
+                                                   velocity.size), self._w)
 
     # --- inspection ---
     def cloth_partition(self, handle: int, nv: int) -> tuple[np.ndarray, np.ndarray]:

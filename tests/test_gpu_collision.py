@@ -132,7 +132,7 @@ def test_coloring_valid_and_equal_to_oracle(oracle):
     np.testing.assert_array_equal(colors, ocolors)
     inc = {}
     for i, vs in enumerate(verts):
-        for v in vs:
+        for v in set(vs.tolist()):
             if v >= 0:
                 inc.setdefault(int(v), []).append(i)
     for lst in inc.values():
