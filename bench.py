@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""Benchmark of the per-step cloth pipeline (silk::World::solver_step).
+
+Workload (N = 1): the 6.4K-vertex sheet of the benchmark's second
+configuration -- an 80 x 80 grid (12,482 triangles, side 1 m, jitter
+N(0, 1e-4) m from a fixed seed) dropped from z = 1 onto a static icosphere
+(subdivision 4, radius 0.3 m), self-collision and obstacle CCD on, float32,
+dt = 1/60, gravity -9.81.  A step is one solver_step.  The sheet first falls
+freely for `--prelude` untimed steps so that the timed steps run with active
+contacts (the regime the reference's "6K cloth with active collision" claim
+describes); then `--warmup` untimed and `--steps` timed steps follow.
+
+Metric: steps/s (higher is better).  `value` is device time (CUDA events on
+the world's stream) with inputs resident; `e2e` drives the public API with
+host buffers each step (obstacle position upload + solver_step + position
+readback).  Between timed steps a 256 MiB buffer is written to flush L2.
+
+Multi-GPU: scenes are independent, so --gpus N runs N replicas (one process
+per GPU, no collective on the data path; barrier + max over ranks only).
+
+`--impl reference` times the CPU restatement of the reference algorithm
+(oracle/, the reference itself cannot be built here) on all host cores on the
+same scene and steps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = "c2_sheet80_on_icosphere_r0.3"
+METRIC = "steps/s (6.4K-vertex sheet on sphere, active contact)"
+
+
+def scene(seed=1236):
+    from silk_physics_b200 import scenes as S
+
+    V, F = S.grid_sheet(80, side=1.0, z=1.0, jitter=1e-4, seed=seed)
+    SV, SF = S.icosphere(4, radius=0.3)
+    return V, F, SV, SF
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = Path(f"/tmp/silk_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+            self.out.close()
+
+    def summary(self) -> dict:
+        try:
+            rows = [r.split(",") for r in self.path.read_text().strip().splitlines()]
+        except Exception:
+            rows = []
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for k, n in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(n)
+            except Exception:
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def traffic_per_launch():
+    """DRAM bytes per CG launch from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "cg_kernel_c2.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def make_world(stream_handle, opts, V, F, SV, SF):
+    from silk_physics_b200 import native as N
+
+    w = N.World()
+    r = w.init()
+    if not r:
+        raise RuntimeError(r.to_string())
+    w.set_global_config(N.GlobalConfig(acceleration_z=-9.81))
+    w.set_solver_options(opts)
+    if stream_handle:
+        w.set_stream(stream_handle)
+    r, h = w.add_cloth(N.ClothConfig(), N.CollisionConfig(), V, F, [])
+    assert r, r.to_string()
+    r, hs = w.add_obstacle(N.CollisionConfig(), SV, SF)
+    assert r, r.to_string()
+    return w, h, hs
+
+
+def cpu_oracle_sample(x0, v0, V, F, SV, SF, gpu_steps_per_admm, budget_s=20.0):
+    """Time the CPU restatement from the same state on all host cores.
+
+    Contact steps of this algorithm take minutes on a CPU, so the sample is
+    the steps that fit in ~budget_s (at least one); the result is steps/s."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+
+    ow = pyoracle.OracleWorld(config=dict(acceleration=(0.0, 0.0, -9.81)))
+    nv = len(V)
+    perm = np.arange(nv, dtype=np.int32)
+    offs = np.unique(np.append(np.arange(0, nv, 32), nv)).astype(np.int32)
+    h = ow.add_cloth(V, F, [], perm, offs)
+    ow.add_obstacle(SV, SF)
+    ow.set_state(h, x0, v0)
+    t0 = time.perf_counter()
+    steps = 0
+    admm = 0
+    while True:
+        ow.step()
+        steps += 1
+        admm += ow.stats()["admm_iterations"]
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return steps / el, steps, el, admm
+
+
+def run_ours(args) -> None:
+    import torch
+
+    rank, local_rank, world_size = dist_env()
+    torch.cuda.set_device(local_rank)
+    if world_size > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    from silk_physics_b200 import native as N
+
+    V, F, SV, SF = scene()
+    stream = torch.cuda.Stream()
+    opts = N.SolverOptions(fixed_linear_rel_tol=args.cg_rel_tol, profile=True,
+                           mas_bf16=args.bf16)
+    w, h, hs = make_world(stream.cuda_stream, opts, V, F, SV, SF)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    x = np.zeros(V.size, np.float32)
+    for _ in range(args.prelude):
+        r = w.solver_step()
+        assert r, r.to_string()
+    for _ in range(args.warmup):
+        r = w.solver_step()
+        assert r, r.to_string()
+    state_x = np.zeros(V.size, np.float32)
+    state_v = np.zeros(V.size, np.float32)
+    w.get_cloth_position(h, state_x)
+    w.get_cloth_velocity(h, state_v)
+    w.profile(reset=True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    launches = admm = cg = solves = contacts = 0
+    if world_size > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(k & 0xff)
+                ev[k][0].record(stream)
+            r = w.solver_step()
+            ev[k][1].record(stream)
+            assert r, r.to_string()
+            st = w.step_stats()
+            launches += st.kernel_launches
+            admm += st.admm_iterations
+            cg += st.cg_iterations
+            solves += st.cg_solves
+            contacts = st.contacts
+        torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(step_ms))
+    prof = w.profile(reset=True)
+    if world_size > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+        torch.distributed.barrier()
+    value = world_size * args.steps / (total_ms / 1e3)
+
+    # End to end through the public API with host buffers.
+    pin_obs = torch.from_numpy(SV.ravel().copy()).pin_memory().numpy()
+    pin_out = torch.empty(V.size, dtype=torch.float32).pin_memory().numpy()
+    e2e_ms = []
+    for _ in range(args.e2e_steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        w.set_obstacle_position(hs, pin_obs)
+        r = w.solver_step()
+        w.get_cloth_position(h, pin_out)
+        b.record(stream)
+        b.synchronize()
+        assert r, r.to_string()
+        e2e_ms.append(a.elapsed_time(b))
+    e2e_val = args.e2e_steps / (sum(e2e_ms) / 1e3) * world_size
+
+    if rank != 0:
+        if world_size > 1:
+            torch.distributed.destroy_process_group()
+        return
+    pk = peaks()
+    cg_launch_ms = prof["cg_time_ms"] / max(prof["cg_launches"], 1)
+    bytes_per_launch = prof["cg_algorithmic_bytes"] / max(prof["cg_launches"], 1)
+    achieved = bytes_per_launch / (cg_launch_ms / 1e3) / 1e9 if cg_launch_ms > 0 else 0.0
+    roofline = {"bound": "hbm", "kernel": "cg_kernel (persistent MAS-PCG)",
+                "achieved": round(achieved, 2), "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": round(achieved / pk["hbm_gbs"], 5), "peak_source": pk["source"],
+                "traffic": traffic_per_launch(),
+                "algorithmic_bytes_per_launch": round(bytes_per_launch),
+                "avg_launch_ms": round(cg_launch_ms, 5),
+                "cg_share_of_step": round(prof["cg_time_ms"] / total_ms, 4) if total_ms else None}
+    cpu = None
+    if world_size == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sps, n, el, cadmm = cpu_oracle_sample(state_x, state_v, V, F, SV, SF, None,
+                                               args.cpu_budget)
+        cpu = {"value": round(sps, 6), "unit": "steps/s", "cores": threads, "kind": "port",
+               "sample": f"{n} step(s) of the same scene from the GPU state after "
+                         f"{args.prelude + args.warmup} steps, {el:.1f} s wall, "
+                         f"{cadmm} ADMM iterations, OpenMP on all host threads"}
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": "steps/s", "n_gpus": world_size,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded grid sheet + icosphere)",
+        "config": {"workload": WORKLOAD, "vertices": int(len(V)), "faces": int(len(F)),
+                   "obstacle_vertices": int(len(SV)), "prelude_steps": args.prelude,
+                   "cg_rel_tol": args.cg_rel_tol if args.cg_rel_tol > 0 else "adaptive (reference)",
+                   "mas": "bf16" if args.bf16 else "fp32",
+                   "l2": "flushed between timed steps (256 MiB write)",
+                   "admm_iterations_per_step": admm / args.steps,
+                   "cg_iterations_per_solve": round(cg / max(solves, 1), 2),
+                   "contacts_last_step": contacts,
+                   "parallelism": f"replicas x{world_size}"},
+        "roofline": roofline, "cpu_baseline": cpu,
+        "e2e": {"value": round(e2e_val, 4), "unit": "steps/s",
+                "h2d_bytes_per_step": int(SV.nbytes), "d2h_bytes_per_step": int(V.nbytes)},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    if world_size > 1:
+        torch.distributed.destroy_process_group()
+
+
+def run_reference(args) -> None:
+    rank, _, world_size = dist_env()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+
+    V, F, SV, SF = scene()
+    ow = pyoracle.OracleWorld(config=dict(acceleration=(0.0, 0.0, -9.81)))
+    nv = len(V)
+    perm = np.arange(nv, dtype=np.int32)
+    offs = np.unique(np.append(np.arange(0, nv, 32), nv)).astype(np.int32)
+    h = ow.add_cloth(V, F, [], perm, offs)
+    ow.add_obstacle(SV, SF)
+    t_pre = time.perf_counter()
+    for _ in range(args.prelude + args.warmup):
+        ow.step()
+    pre = time.perf_counter() - t_pre
+    times = []
+    admm = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        a = time.perf_counter()
+        ow.step()
+        times.append(time.perf_counter() - a)
+        admm += ow.stats()["admm_iterations"]
+        if time.perf_counter() - t0 > args.cpu_budget and len(times) >= 1:
+            break
+    value = len(times) / sum(times)
+    sample = (f"{len(times)} timed step(s) after {args.prelude + args.warmup} untimed "
+              f"({pre:.1f} s), {admm} ADMM iterations, OpenMP on {threads} threads")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "steps/s",
+        "n_gpus": world_size, "steps": len(times), "warmup": args.warmup,
+        "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded grid sheet + icosphere)",
+        "config": {"workload": WORKLOAD, "vertices": int(nv), "prelude_steps": args.prelude,
+                   "implementation": "CPU restatement of the reference algorithm (oracle/); "
+                                     "the reference cannot be built offline"},
+        "cpu_baseline": {"value": round(value, 6), "unit": "steps/s", "cores": threads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": round(value, 6), "unit": "steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--prelude", type=int, default=24)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cg-rel-tol", type=float, default=0.0)
+    ap.add_argument("--bf16", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

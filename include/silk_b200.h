@@ -94,11 +94,16 @@ typedef struct {
  * compulsory DRAM traffic per CG iteration: matrix entries, MAS bank
  * inverses and each vector read or written once. */
 typedef struct {
-  double cg_time_ms;
+  double cg_time_ms;         /* CUDA events around the CG kernel */
   int64_t cg_launches;
   int64_t cg_iterations;
   double cg_algorithmic_bytes;
-  double reserved[4];
+  double admm_other_ms;      /* events: face/vertex/contact kernels */
+  double admm_host_ms;       /* host wall time of ADMM control (syncs) */
+  double ccd_host_ms;        /* host wall time of refit + CCD */
+  double dcd_host_ms;        /* host wall time of DCD + contact rebuild */
+  double step_host_ms;       /* host wall time of solver_step */
+  double reserved[3];
 } silk_profile;
 
 /* Statistics of the last solver_step. */

@@ -4,6 +4,7 @@
 // assembly/cloth_assembler.cu:64-172, pin_constraints.cu:50-107).
 #include <algorithm>
 #include <cmath>
+#include <chrono>
 #include <cstring>
 
 #include "collision.cuh"
@@ -677,19 +678,24 @@ void World::cg_solve(Cloth& c, float rel_tol) {
   a.max_iter = opt.cg_max_iter > 0 ? opt.cg_max_iter : 1000;
   a.stats = c.dev.stats.p;
   if (opt.profile) {
-    if (events_used == events.size()) {
-      cudaEvent_t e0, e1;
-      CUDA_CHECK(cudaEventCreate(&e0));
-      CUDA_CHECK(cudaEventCreate(&e1));
-      events.emplace_back(e0, e1);
-    }
-    auto& ev = events[events_used++];
-    CUDA_CHECK(cudaEventRecord(ev.first, stream));
+    auto* ev = next_event_pair(events, events_used);
+    CUDA_CHECK(cudaEventRecord(ev->first, stream));
     launch_cg(a, c.dev.cg_grid, stream);
-    CUDA_CHECK(cudaEventRecord(ev.second, stream));
+    CUDA_CHECK(cudaEventRecord(ev->second, stream));
   } else {
     launch_cg(a, c.dev.cg_grid, stream);
   }
+}
+
+std::pair<cudaEvent_t, cudaEvent_t>* World::next_event_pair(
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& pool, size_t& used) {
+  if (used == pool.size()) {
+    cudaEvent_t e0, e1;
+    CUDA_CHECK(cudaEventCreate(&e0));
+    CUDA_CHECK(cudaEventCreate(&e1));
+    pool.emplace_back(e0, e1);
+  }
+  return &pool[used++];
 }
 
 silk_status World::get_profile(silk_profile* p, bool reset) {
@@ -753,12 +759,15 @@ bool World::admm_solve() {
         cg_solve(*c, rel);
       }
     }
+    std::pair<cudaEvent_t, cudaEvent_t>* oe = opt.profile ? next_event_pair(events_other, events_other_used) : nullptr;
+    if (oe) CUDA_CHECK(cudaEventRecord(oe->first, st));
     launch_face_step(s, face_partials.p, fb, st);
     if (contacts) {
       launch_contact_init(s, st);
       coll_->contact_solve();
     }
     launch_vertex_step(s, vertex_partials.p, vb, st);
+    if (oe) CUDA_CHECK(cudaEventRecord(oe->second, st));
     stats.admm_iterations += 1;
     if (it == 0) continue;
     fa.iteration = it;
@@ -778,6 +787,11 @@ silk_status World::solver_step() {
   if (!initialized) return SILK_ERR_NOT_INITIALIZED;
   try {
     long long launches0 = g_launch_count;
+    using clk = std::chrono::steady_clock;
+    auto ms_since = [](clk::time_point t) {
+      return std::chrono::duration<double, std::milli>(clk::now() - t).count();
+    };
+    auto t_step = clk::now();
     stats = silk_step_stats{};
     if (cloths.empty()) {
       last_error = "nothing to solve";
@@ -789,6 +803,7 @@ silk_status World::solver_step() {
     int nv = nv_total;
     for (auto& c : cloths) c->dev.stats.zero(st);
     events_used = 0;
+    events_other_used = 0;
     // init (main_loop.cu:24-76): damped velocity, fresh ADMM aux variables.
     launch_damp(nv, damp.p, sv.p, prev_v.p, st);
     zu.zero(st);
@@ -804,25 +819,31 @@ silk_status World::solver_step() {
       float pad = coll_->scene_padding();
       ms = 0.2f * pad;
       dact = 1.0f * pad;
+      auto t0 = clk::now();
       coll_->refit(outer.p, outer.p);
       coll_->append_active(0.0f, dact);
+      prof.dcd_host_ms += ms_since(t0);
     }
     float remaining = 1.0f;
     for (int oit = 0; oit < g.max_outer_iteration; ++oit) {
       stats.outer_iterations += 1;
       launch_predict(nv, g.dt, make_float4(g.acceleration_x, g.acceleration_y, g.acceleration_z, 0.f),
                      outer.p, outer_v.p, x.p, st);
+      auto t_admm = clk::now();
       if (!admm_solve()) {
         last_error = "solver diverged";
         return SILK_ERR_ITERATIVE_SOLVE_FAIL;
       }
+      prof.admm_host_ms += ms_since(t_admm);
       float toi = remaining;
       if (collide) {
+        auto t0 = clk::now();
         coll_->refit(x.p, outer.p);
         int nq = 0, nh = 0;
         toi = coll_->min_toi(1.0f - remaining, remaining, ms, &nq, &nh);
         stats.ccd_queries += nq;
         stats.ccd_hits += nh;
+        prof.ccd_host_ms += ms_since(t0);
       }
       stats.min_toi = toi;
       launch_velocity(nv, g.dt, x.p, outer.p, outer_v.p, st);
@@ -834,8 +855,10 @@ silk_status World::solver_step() {
       float frac = rollback / remaining;
       launch_mix(nv, frac, x.p, outer.p, st);
       remaining -= rollback;
+      auto t0 = clk::now();
       coll_->refit(outer.p, outer.p);
       coll_->append_active(1.0f - remaining, dact);
+      prof.dcd_host_ms += ms_since(t0);
     }
     // Final velocity from the whole accepted displacement (main_loop.cu:248).
     launch_velocity(nv, g.dt, outer.p, sx.p, sv.p, st);
@@ -862,6 +885,11 @@ silk_status World::solver_step() {
         prof.cg_time_ms += ms;
       }
       prof.cg_launches += (int64_t)events_used;
+      for (size_t e = 0; e < events_other_used; ++e) {
+        float ms = 0.f;
+        CUDA_CHECK(cudaEventElapsedTime(&ms, events_other[e].first, events_other[e].second));
+        prof.admm_other_ms += ms;
+      }
     }
     if (coll_) {
       stats.contacts = coll_->contact_count();
@@ -874,6 +902,7 @@ silk_status World::solver_step() {
       else o->is_static = true;
     }
     stats.kernel_launches = g_launch_count - launches0;
+    prof.step_host_ms += ms_since(t_step);
     return SILK_OK;
   } catch (const std::exception& e) {
     last_error = e.what();

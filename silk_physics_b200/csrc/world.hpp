@@ -192,8 +192,10 @@ class World {
   DevBuf<AdmmControl> ctl;
   int pinned_dof = 0;
   silk_profile prof{};
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
-  size_t events_used = 0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events, events_other;
+  size_t events_used = 0, events_other_used = 0;
+  std::pair<cudaEvent_t, cudaEvent_t>* next_event_pair(
+      std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& pool, size_t& used);
 
   Cloth* find_cloth(uint32_t h);
   Obstacle* find_obstacle(uint32_t h);

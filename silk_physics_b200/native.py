@@ -81,7 +81,9 @@ class _SolverOptionsC(C.Structure):
 class _ProfileC(C.Structure):
     _fields_ = [("cg_time_ms", C.c_double), ("cg_launches", C.c_int64),
                 ("cg_iterations", C.c_int64), ("cg_algorithmic_bytes", C.c_double),
-                ("reserved", C.c_double * 4)]
+                ("admm_other_ms", C.c_double), ("admm_host_ms", C.c_double),
+                ("ccd_host_ms", C.c_double), ("dcd_host_ms", C.c_double),
+                ("step_host_ms", C.c_double), ("reserved", C.c_double * 3)]
 
 
 class _StepStatsC(C.Structure):

