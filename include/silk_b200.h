@@ -205,10 +205,12 @@ silk_status silk_debug_candidates(silk_world* w, int32_t* out, int64_t cap,
  * sorted; count in *n. */
 silk_status silk_debug_dcd(silk_world* w, float t, float activation,
                            int32_t* keys, int64_t cap, int32_t* n);
-/* Minimum time of impact over the current refit. */
+/* Minimum time of impact over the current refit.  prune = 1 lets searches
+ * stop once they cannot lower the minimum (the solver step's mode: same
+ * minimum, n_hits then counts completed searches only). */
 silk_status silk_debug_min_toi(silk_world* w, float time_start,
                                float max_time, float min_separation,
-                               float* toi, int32_t* n_queries,
+                               int32_t prune, float* toi, int32_t* n_queries,
                                int32_t* n_hits);
 
 /* --- Host-side setup (no GPU needed) ------------------------------------ */

@@ -247,11 +247,11 @@ silk_status silk_debug_dcd(silk_world* w, float t, float activation,
 }
 
 silk_status silk_debug_min_toi(silk_world* w, float time_start, float max_time,
-                               float min_separation, float* toi,
+                               float min_separation, int32_t prune, float* toi,
                                int32_t* n_queries, int32_t* n_hits) {
   return guard_init(w, [&](World& W) {
-    return W.debug_min_toi(time_start, max_time, min_separation, toi, n_queries,
-                           n_hits);
+    return W.debug_min_toi(time_start, max_time, min_separation, prune != 0, toi,
+                           n_queries, n_hits);
   });
 }
 

@@ -649,10 +649,18 @@ struct DfsStack {
   int n;
 };
 
-// Returns 0 = no root, 1 = root, 2 = stack overflow (conservative root).
+// Returns 0 = no root, 1 = root, 2 = storage overflow, 3 = pruned.
+//
+// Pruning (best != nullptr): boxes are processed in non-decreasing t.lower
+// (every child keeps or raises its parent's t.lower and the smallest pending
+// t.lower is always taken next), so once the current box starts at
+// t.lower > 0 with t.lower >= the smallest time of impact already found by
+// any query, no answer of this search can lower that minimum.  Stopping
+// there leaves the minimum over all queries bit-identical to the full search.
 __device__ int root_finder(bool vf, const float3* Pt, const float* tol,
                            float co_tol, const float* err, float ms, int max_iter,
-                           float max_time, IBox& result, DfsStack& st) {
+                           float max_time, IBox& result, DfsStack& st,
+                           const unsigned* best_bits = nullptr) {
   CcdCoeff co;
   for (int d = 0; d < 3; ++d) {
     auto comp = [&](const float3& p) { return d == 0 ? p.x : (d == 1 ? p.y : p.z); };
@@ -689,9 +697,14 @@ __device__ int root_finder(bool vf, const float3* Pt, const float* tol,
     ++st.n;
     return true;
   };
+  float best = __int_as_float(0x7f800000);
   while (has_cur || st.n > 0) {
     if (!has_cur) cur = st.e[--st.n];
     has_cur = false;
+    if (best_bits) {
+      if ((iter & 15) == 0) best = __uint_as_float(*(volatile const unsigned*)best_bits);
+      if (cur.t0 > 0.0f && cur.t0 >= best) return 3;
+    }
     ++iter;
     bool in_eps_all = true;
     float w_img[3];
@@ -765,7 +778,8 @@ __device__ int root_finder(bool vf, const float3* Pt, const float* tol,
 // search; toi follows narrowphase.cu's use of the answer.
 __device__ int ccd_query(bool vf, const float3* Pt, const float* err, float ms,
                          float tolerance, int max_iter, float max_time, float& toi,
-                         float& t_upper, DfsStack& st) {
+                         float& t_upper, DfsStack& st,
+                         const unsigned* best_bits = nullptr) {
   float3 p000, p001, p011, p010, p100, p101, p111, p110;
   if (vf) {
     p000 = sub3(Pt[0], Pt[1]);
@@ -796,13 +810,15 @@ __device__ int ccd_query(bool vf, const float3* Pt, const float* err, float ms,
   float tol[3] = {clamp_div(tolerance, dl, inf), clamp_div(tolerance, e0, inf),
                   clamp_div(tolerance, e1, inf)};
   IBox r;
-  int s = root_finder(vf, Pt, tol, tolerance, err, ms, max_iter, max_time, r, st);
-  if (s == 0) return 0;
+  int s = root_finder(vf, Pt, tol, tolerance, err, ms, max_iter, max_time, r, st, best_bits);
+  if (s == 0 || s == 3) return s;
   toi = r.t0;
   t_upper = r.t1;
   if (r.t0 > 0.0f) return s;
   IBox r2;
-  int s2 = root_finder(vf, Pt, tol, tolerance, err, 0.5f * ms, max_iter, max_time, r2, st);
+  int s2 = root_finder(vf, Pt, tol, tolerance, err, 0.5f * ms, max_iter, max_time, r2, st,
+                       best_bits);
+  if (s2 == 3) return 3;
   if (s2 == 0) {
     toi = max_time;
     t_upper = max_time;
@@ -851,12 +867,10 @@ __device__ __forceinline__ void bind_stack(DfsStack& st, const CcdSpill& sp, int
   }
 }
 
-__global__ void __launch_bounds__(kCollThreads) ccd_kernel(
-    const ObjDev* objs, const int4* cand, int n, float ts, float interval,
-    float ms, float3 vf_err, float3 ee_err, float local_tol, unsigned* min_bits,
-    int* counts, CcdSpill sp) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+__device__ __noinline__ void ccd_one(const ObjDev* objs, const int4* cand, int i, float ts,
+                                     float interval, float ms, float3 vf_err, float3 ee_err,
+                                     float local_tol, unsigned* min_bits, int* counts,
+                                     const CcdSpill& sp, int prune) {
   int q = sp.list ? sp.list[i] : i;
   int4 c = cand[q];
   int kind = c.z >> 16, sa = c.z & 0xffff, sb = c.w;
@@ -886,16 +900,33 @@ __global__ void __launch_bounds__(kCollThreads) ccd_kernel(
   bind_stack(st, sp, i);
   float toi = 1.0f, tup = 1.0f;
   float local_max = interval / interval;
-  int s = ccd_query(vf, Pt, err, ms, local_tol, kCcdMaxIter, local_max, toi, tup, st);
+  int s = ccd_query(vf, Pt, err, ms, local_tol, kCcdMaxIter, local_max, toi, tup, st,
+                    prune ? min_bits : nullptr);
   if (s == 2) {
     if (!sp.spill) sp.overflow[atomicAdd(sp.n_overflow, 1)] = q;
     else atomicAdd(&counts[1], 1);
     return;
   }
-  if (s == 0) return;
+  if (s == 0 || s == 3) return;
   atomicAdd(&counts[0], 1);
   if (toi == 0.0f) return;
   atomicMin(min_bits, __float_as_uint(toi));  // toi >= 0: bit order = value order
+}
+
+// Queries are taken from a shared counter so that threads whose searches end
+// early pick up new work instead of idling behind long searches.  With
+// prune != 0 a search stops once it cannot lower the running minimum
+// (root_finder); the hit count then covers completed searches only.
+__global__ void __launch_bounds__(kCollThreads) ccd_kernel(
+    const ObjDev* objs, const int4* cand, int n, float ts, float interval,
+    float ms, float3 vf_err, float3 ee_err, float local_tol, unsigned* min_bits,
+    int* counts, CcdSpill sp, int* next, int prune) {
+  for (;;) {
+    int i = atomicAdd(next, 1);
+    if (i >= n) return;
+    ccd_one(objs, cand, i, ts, interval, ms, vf_err, ee_err, local_tol, min_bits, counts,
+            sp, prune);
+  }
 }
 
 __global__ void ccd_batch_kernel(bool vf, const float* x, int n, float3 err,
@@ -1215,7 +1246,7 @@ CollisionSystem::CollisionSystem(World& w) : w_(w), impl_(new CollisionImpl) {
   CUDA_CHECK(cudaMemset(impl_->active_dof.p, 0, sizeof(int)));
   impl_->counter.alloc(4);
   impl_->min_bits.alloc(1);
-  impl_->ccd_counts.alloc(3);
+  impl_->ccd_counts.alloc(4 + 64);
   impl_->jp_flags.alloc(2);
   impl_->gs_barrier.alloc(4);
   CUDA_CHECK(cudaMemset(impl_->gs_barrier.p, 0, 4 * sizeof(unsigned)));
@@ -1757,7 +1788,8 @@ void CollisionSystem::contact_solve() {
   SILK_LAUNCHED();
 }
 
-float CollisionSystem::min_toi(float ts, float max_time, float ms, int* nq, int* nh) {
+float CollisionSystem::min_toi(float ts, float max_time, float ms, int* nq, int* nh,
+                               bool prune) {
   CollisionImpl& I = *impl_;
   cudaStream_t st = w_.stream;
   *nq = 0;
@@ -1784,25 +1816,37 @@ float CollisionSystem::min_toi(float ts, float max_time, float ms, int* nq, int*
   float one = max_time / max_time;
   std::memcpy(&one_bits, &one, 4);
   CUDA_CHECK(cudaMemcpyAsync(I.min_bits.p, &one_bits, 4, cudaMemcpyHostToDevice, st));
-  CUDA_CHECK(cudaMemsetAsync(I.ccd_counts.p, 0, 3 * sizeof(int), st));
+  // counts: [hits, storage overflows, first-pass spills, work counters...]
+  const int max_chunks = 64;
+  CUDA_CHECK(cudaMemsetAsync(I.ccd_counts.p, 0, (4 + max_chunks) * sizeof(int), st));
   if ((int)I.ccd_overflow.n < n) I.ccd_overflow.alloc(n + n / 4);
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    CUDA_CHECK(cudaGetDevice(&dev));
+    CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  auto grid_for = [&](int m) { return std::max(1, std::min(div_up(m, kCollThreads), 8 * sms)); };
   CcdSpill first{nullptr, 0, nullptr, I.ccd_overflow.p, I.ccd_counts.p + 2};
-  ccd_kernel<<<div_up(n, kCollThreads), kCollThreads, 0, st>>>(
+  ccd_kernel<<<grid_for(n), kCollThreads, 0, st>>>(
       I.table_d.p, I.cand.p, n, ts, max_time, ms, vf, ee, local_tol, I.min_bits.p,
-      I.ccd_counts.p, first);
+      I.ccd_counts.p, first, I.ccd_counts.p + 3, prune ? 1 : 0);
   SILK_LAUNCHED();
   int counts[3];
   CUDA_CHECK(cudaMemcpyAsync(counts, I.ccd_counts.p, sizeof(counts), cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaStreamSynchronize(st));
   // Second pass for the searches that outgrew the per-thread array.
   const int cap = kCcdMaxIter + 2;
-  for (int start = 0; start < counts[2]; start += kCcdSpillChunk) {
+  int chunk_id = 0;
+  for (int start = 0; start < counts[2]; start += kCcdSpillChunk, ++chunk_id) {
     int m = std::min(kCcdSpillChunk, counts[2] - start);
     if (I.ccd_spill.n < (size_t)kCcdSpillChunk * cap) I.ccd_spill.alloc((size_t)kCcdSpillChunk * cap);
+    int* next = I.ccd_counts.p + 4 + (chunk_id % max_chunks);
+    if (chunk_id >= max_chunks) CUDA_CHECK(cudaMemsetAsync(next, 0, sizeof(int), st));
     CcdSpill second{I.ccd_spill.p, cap, I.ccd_overflow.p + start, nullptr, nullptr};
-    ccd_kernel<<<div_up(m, kCollThreads), kCollThreads, 0, st>>>(
+    ccd_kernel<<<grid_for(m), kCollThreads, 0, st>>>(
         I.table_d.p, I.cand.p, m, ts, max_time, ms, vf, ee, local_tol, I.min_bits.p,
-        I.ccd_counts.p, second);
+        I.ccd_counts.p, second, next, prune ? 1 : 0);
     SILK_LAUNCHED();
   }
   unsigned bits = 0;

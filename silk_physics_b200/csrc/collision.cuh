@@ -31,9 +31,11 @@ class CollisionSystem {
   void begin_step();
   // DCD at collider time t; appends new contacts.  Returns the number added.
   int append_active(float time, float activation);
-  // Earliest time of impact over [time_start, time_start + max_time].
+  // Earliest time of impact over [time_start, time_start + max_time].  With
+  // prune, searches that cannot lower the minimum stop early (same minimum;
+  // n_hits then counts completed searches only).
   float min_toi(float time_start, float max_time, float min_separation,
-                int* n_queries, int* n_hits);
+                int* n_queries, int* n_hits, bool prune = true);
   // Contact projection of one ADMM iteration (after contact_init).
   void contact_solve();
   int contact_count() const;

@@ -14,6 +14,7 @@
 //    bounded spin (no host round trip, no graph rebuild per solve);
 //  * reductions are FP64 and deterministic (per-block partials summed in a
 //    fixed order by every block).
+#include <cooperative_groups.h>
 #include <cuda/atomic>
 
 #include "grid_barrier.cuh"
@@ -205,6 +206,7 @@ __device__ double spmv_phase(const CgArgs& a, const float4* v, float4* out,
       float4 vi = v[row];
       float d = a.Ldiag[row] + a.dyn[row];
       float yx = d * vi.x, yy = d * vi.y, yz = d * vi.z;
+#pragma unroll 4
       for (int k = 0; k < width; ++k) {
         int2 e = a.ent[base + k * 32 + lane];
         float val = __int_as_float(e.y);
@@ -317,9 +319,18 @@ __device__ void prolong_phase(const CgArgs& a, float beta) {
   }
 }
 
-__global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs a) {
-  extern __shared__ float sm_all[];
-  GridBarrier bar{a.barrier, a.barrier + 1, a.barrier + 2, gridDim.x};
+// Hardware barrier of a thread-block cluster: used when the whole solve runs
+// in one cluster (small and medium systems), where it replaces the global
+// memory barrier that dominates the CG iteration time of such systems.
+struct ClusterBarrier {
+  __device__ bool sync() {
+    cooperative_groups::this_cluster().sync();
+    return true;
+  }
+};
+
+template <class Barrier>
+__device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm_all) {
   double* part = a.partials + 4 * blockIdx.x;
   // r = b - A x.
   spmv_phase(a, a.x, a.r, 1);
@@ -401,6 +412,47 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs a) {
   }
 }
 
+__global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs a) {
+  extern __shared__ float sm_all[];
+  GridBarrier bar{a.barrier, a.barrier + 1, a.barrier + 2, gridDim.x};
+  cg_body(a, bar, sm_all);
+}
+
+__global__ void __launch_bounds__(kCgThreads) cg_kernel_cluster(CgArgs a) {
+  extern __shared__ float sm_all[];
+  ClusterBarrier bar;
+  cg_body(a, bar, sm_all);
+}
+
+int max_cluster_size() {
+  static int size = -1;
+  if (size < 0) {
+    size_t smem = kCgWarps * kPacked * sizeof(float);
+    if (cudaFuncSetAttribute(cg_kernel_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed,
+                             1) != cudaSuccess) {
+      cudaGetLastError();
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(16);
+    cfg.blockDim = dim3(kCgThreads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = 16;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxPotentialClusterSize(&n, cg_kernel_cluster, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      n = 8;
+    }
+    size = n >= 16 ? 16 : (n >= 8 ? 8 : 0);
+  }
+  return size;
+}
+
 }  // namespace
 
 void launch_galerkin_fill(const GalerkinDev& g, const double* src_vals,
@@ -420,6 +472,10 @@ void launch_bank_invert(const MasLevelDev& lv, bool fine, const int* part_off,
 }
 
 int cg_grid_size(int nslices, int nbank0) {
+  int want_blocks = div_up(nslices > nbank0 ? nslices : nbank0, kCgWarps);
+  int cl = max_cluster_size();
+  // One cluster while each warp has at most ~3 slices / banks to process.
+  if (cl > 0 && want_blocks <= 3 * cl) return -cl;
   static int max_coop = 0;
   if (max_coop == 0) {
     int dev = 0, sms = 0, per_sm = 0;
@@ -436,8 +492,25 @@ int cg_grid_size(int nslices, int nbank0) {
 }
 
 void launch_cg(const CgArgs& a, int grid, cudaStream_t st) {
-  CUDA_CHECK(cudaMemsetAsync(a.barrier, 0, 2 * sizeof(unsigned), st));
   size_t smem = kCgWarps * kPacked * sizeof(float);
+  if (grid < 0) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(-grid);
+    cfg.blockDim = dim3(kCgThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = -grid;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    CUDA_CHECK(cudaLaunchKernelEx(&cfg, cg_kernel_cluster, a));
+    SILK_LAUNCHED();
+    return;
+  }
+  CUDA_CHECK(cudaMemsetAsync(a.barrier, 0, 2 * sizeof(unsigned), st));
   void* args[] = {(void*)&a};
   CUDA_CHECK(cudaLaunchCooperativeKernel((const void*)cg_kernel, dim3(grid),
                                          dim3(kCgThreads), args, smem, st));

@@ -449,8 +449,9 @@ void World::build_cloth_device(Cloth& c) {
   d.Ap.alloc(nv);
   d.p.zero(st);
   int nbank0 = S.fine.nbank;
+  // Negative: one thread-block cluster of that many CTAs.
   d.cg_grid = cg_grid_size(nsl, nbank0);
-  d.partials.alloc(4 * (size_t)d.cg_grid);
+  d.partials.alloc(4 * (size_t)std::abs(d.cg_grid));
   d.coarse_partial.alloc(1);
   d.barrier.alloc(4);
   d.barrier.zero(st);
@@ -976,9 +977,9 @@ silk_status World::debug_dcd(float t, float dact, int* keys, int64_t cap, int* n
   return SILK_OK;
 }
 
-silk_status World::debug_min_toi(float ts, float mt, float ms, float* toi,
-                                 int* nq, int* nh) {
-  *toi = coll_->min_toi(ts, mt, ms, nq, nh);
+silk_status World::debug_min_toi(float ts, float mt, float ms, bool prune,
+                                 float* toi, int* nq, int* nh) {
+  *toi = coll_->min_toi(ts, mt, ms, nq, nh, prune);
   return SILK_OK;
 }
 

@@ -166,8 +166,8 @@ class World {
   silk_status debug_refit(const float* disp, int64_t n);
   silk_status debug_candidates(int* out, int64_t cap, int* n);
   silk_status debug_dcd(float t, float dact, int* keys, int64_t cap, int* n);
-  silk_status debug_min_toi(float ts, float mt, float ms, float* toi, int* nq,
-                            int* nh);
+  silk_status debug_min_toi(float ts, float mt, float ms, bool prune, float* toi,
+                            int* nq, int* nh);
 
   silk_step_stats stats{};
 

@@ -229,8 +229,9 @@ def _load() -> C.CDLL:
         "silk_debug_candidates": ([_W, _I32P, C.c_int64, C.POINTER(C.c_int32)], C.c_int),
         "silk_debug_dcd": ([_W, C.c_float, C.c_float, _I32P, C.c_int64,
                             C.POINTER(C.c_int32)], C.c_int),
-        "silk_debug_min_toi": ([_W, C.c_float, C.c_float, C.c_float, C.POINTER(C.c_float),
-                                C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
+        "silk_debug_min_toi": ([_W, C.c_float, C.c_float, C.c_float, C.c_int32,
+                                C.POINTER(C.c_float), C.POINTER(C.c_int32),
+                                C.POINTER(C.c_int32)], C.c_int),
         "silk_ccd_batch": ([C.c_int32, _F32P, C.c_int64, _F32P, _F32P, C.c_float, C.c_int32,
                             C.c_float, _I32P, _F32P, _F32P], C.c_int),
         "silk_color_contacts": ([_I32P, _U64P, C.c_int64, _I32P, C.POINTER(C.c_int32)],
@@ -432,12 +433,12 @@ class World:
             raise RuntimeError(_result(st, self._w).to_string())
         return out[: 7 * min(n.value, cap)].reshape(-1, 7)
 
-    def debug_min_toi(self, time_start: float, max_time: float,
-                      min_separation: float) -> tuple[float, int, int]:
+    def debug_min_toi(self, time_start: float, max_time: float, min_separation: float,
+                      prune: bool = False) -> tuple[float, int, int]:
         toi = C.c_float(0)
         nq, nh = C.c_int32(0), C.c_int32(0)
         st = lib.silk_debug_min_toi(self._w, time_start, max_time, min_separation,
-                                    C.byref(toi), C.byref(nq), C.byref(nh))
+                                    int(prune), C.byref(toi), C.byref(nq), C.byref(nh))
         if st:
             raise RuntimeError(_result(st, self._w).to_string())
         return toi.value, nq.value, nh.value

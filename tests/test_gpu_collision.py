@@ -86,6 +86,9 @@ def test_min_toi_identical(oracle):
         assert nqg == nqo and nhg == nho
         assert np.float32(tg) == np.float32(to)
         assert nhg > 0 and tg < mt
+        # Pruned searches (the step's mode) give the same minimum.
+        tp, nqp, _ = w.debug_min_toi(ts, mt, ms, prune=True)
+        assert nqp == nqg and np.float32(tp) == np.float32(tg)
 
 
 def _random_queries(rng, n, vf):
