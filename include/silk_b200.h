@@ -246,6 +246,47 @@ silk_status silk_ccd_batch(int32_t is_vertex_face, const float* x, int64_t n,
 silk_status silk_color_contacts(const int32_t* verts4, const uint64_t* prio,
                                 int64_t n, int32_t* colors, int32_t* ncolors);
 
+/* --- CCD batch that allocates nothing ----------------------------------- */
+/* No counterpart in the reference (its narrowphase, narrowphase.cu and
+ * ccd.cpp, runs on host cores).  Same queries and results as
+ * silk_ccd_batch, for callers that must not allocate device memory: hosts
+ * whose device memory is owned by a pool or arena with a fixed budget (an
+ * allocation outside it can fail or evict), and real-time loops in which
+ * cudaMalloc / cudaFree would synchronise the device and stall other
+ * streams.  The call performs no cudaMalloc, cudaFree or other allocating
+ * routine; its working memory is one static device array of 10,489,088
+ * bytes created with the library on each device that loads it.
+ *
+ * Buffers x (n x 24 floats), min_separation (n), hit (n), toi (n) and
+ * t_upper (n, may be NULL) are device (or managed) memory of the CURRENT
+ * device, 4-byte aligned; err3 (3 floats) and n_spilled (may be NULL; the
+ * number of queries that needed the large second-pass storage) are host
+ * memory.  Work is issued on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream) and the call returns after it has finished.
+ *
+ * Limits: n <= SILK_CCD_NOALLOC_MAX_QUERIES and
+ * 1 <= max_iter <= SILK_CCD_NOALLOC_MAX_ITER; outside them the call returns
+ * SILK_ERR_INVALID_CONFIG before touching the device.  Host (non-device)
+ * or misaligned buffers, NULL pointers and n < 0 also give
+ * SILK_ERR_INVALID_CONFIG; a CUDA error gives SILK_ERR_UNKNOWN.
+ *
+ * The first call on each device (any n, 0 included) looks up the scratch
+ * array's address, which loads the library's kernels onto that device; make
+ * that first call before any stream capture begins.  Each call zeroes the
+ * scratch counters itself, so nothing has to be cleared between calls.  All
+ * calls on one device share the one scratch array: overlapping calls would
+ * race on it, so calls on the same device from several host threads are
+ * serialised by a lock inside the library and each holds it until its work
+ * on the device has finished. */
+#define SILK_CCD_NOALLOC_MAX_QUERIES (1 << 20)
+#define SILK_CCD_NOALLOC_MAX_ITER 4096
+silk_status silk_ccd_batch_noalloc(int32_t is_vertex_face, const float* x,
+                                   int64_t n, const float* err3,
+                                   const float* min_separation, float tolerance,
+                                   int32_t max_iter, float max_time,
+                                   int32_t* hit, float* toi, float* t_upper,
+                                   void* stream, int32_t* n_spilled);
+
 #ifdef __cplusplus
 }
 #endif

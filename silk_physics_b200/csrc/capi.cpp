@@ -342,4 +342,31 @@ silk_status silk_color_contacts(const int32_t* verts4, const uint64_t* prio,
   }
 }
 
+static_assert(SILK_CCD_NOALLOC_MAX_QUERIES == silkb::kNoAllocMaxQueries &&
+                  SILK_CCD_NOALLOC_MAX_ITER == silkb::kNoAllocMaxIter,
+              "header limits match the scratch layout");
+
+silk_status silk_ccd_batch_noalloc(int32_t is_vertex_face, const float* x,
+                                   int64_t n, const float* err3,
+                                   const float* min_separation, float tolerance,
+                                   int32_t max_iter, float max_time,
+                                   int32_t* hit, float* toi, float* t_upper,
+                                   void* stream, int32_t* n_spilled) {
+  using S = silkb::NoAllocStatus;
+  S s = S::kCudaError;
+  try {
+    s = silkb::ccd_batch_noalloc(is_vertex_face != 0, x, n, err3, min_separation,
+                                 tolerance, max_iter, max_time, hit, toi, t_upper,
+                                 static_cast<cudaStream_t>(stream), n_spilled);
+  } catch (...) {
+    return SILK_ERR_UNKNOWN;
+  }
+  switch (s) {
+    case S::kOk: return SILK_OK;
+    case S::kBadArgument:
+    case S::kBeyondLimits: return SILK_ERR_INVALID_CONFIG;
+    default: return SILK_ERR_UNKNOWN;
+  }
+}
+
 }  // extern "C"

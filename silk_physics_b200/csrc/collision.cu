@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <set>
 #include <tuple>
 
@@ -2041,6 +2042,135 @@ int color_contacts_host(const int* verts4, const uint64_t* prio, int64_t n, int*
   int nc = 0;
   for (int64_t i = 0; i < n; ++i) nc = std::max(nc, colors[i]);
   return nc;
+}
+
+// ---------------------------------------------------------------------------
+// CCD batch over caller-owned device buffers that allocates nothing.
+//
+// Its only working memory is one statically sized device array, created
+// with this module on every device that loads the library:
+//   [0, 256)                 counters, which must be zero when the first pass
+//                            starts (each call zeroes them on its stream):
+//                            [0] queries whose search overflowed the
+//                            96-box per-thread storage, [1] second-pass
+//                            searches that exhausted their storage, [2] next
+//                            overflowed query for the second pass to take
+//   [256, 256 + 4 MiB)       indices of the overflowed queries (written by
+//                            the first pass before they are read; no
+//                            initial value needed)
+//   [.., + 6,294,528 B)      pending-box storage of the second pass:
+//                            kNoAllocSpillSlots regions of max_iter + 2 boxes
+//                            (the most a search of max_iter steps can hold)
+// The first pass is ccd_batch_kernel itself; the second pass runs the
+// overflowed queries on kNoAllocSpillSlots threads that each reuse one
+// storage region, so the scratch size does not grow with the batch.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t kNoAllocListOffset = 256;
+constexpr size_t kNoAllocSpillOffset =
+    kNoAllocListOffset + sizeof(int) * (size_t)kNoAllocMaxQueries;
+constexpr size_t kNoAllocScratchBytes =
+    kNoAllocSpillOffset + sizeof(IBox) * (size_t)kNoAllocSpillSlots * (kNoAllocMaxIter + 2);
+static_assert(kNoAllocSpillOffset % 256 == 0, "spill region alignment");
+
+static __device__ __align__(256) unsigned char g_ccd_noalloc_scratch[kNoAllocScratchBytes];
+
+__global__ void __launch_bounds__(kNoAllocSpillSlots) ccd_batch_spill_kernel(
+    bool vf, const float* x, float3 err, const float* ms, float tol, int max_iter,
+    float max_time, int* hit, float* toi, float* tup, int* counters, const int* list,
+    IBox* spill) {
+  const int n_over = counters[0];
+  DfsStack st;
+  st.cap = max_iter + 2;
+  st.e = spill + (size_t)threadIdx.x * st.cap;
+  const float e[3] = {err.x, err.y, err.z};
+  for (;;) {
+    int j = atomicAdd(&counters[2], 1);
+    if (j >= n_over) return;
+    int q = list[j];
+    float3 Pt[8];
+    for (int k = 0; k < 8; ++k)
+      Pt[k] = make_float3(x[24 * q + 3 * k], x[24 * q + 3 * k + 1], x[24 * q + 3 * k + 2]);
+    float t = max_time, u = max_time;
+    int s = ccd_query(vf, Pt, e, ms[q], tol, max_iter, max_time, t, u, st);
+    if (s == 2) {
+      atomicAdd(&counters[1], 1);
+      continue;
+    }
+    hit[q] = s != 0 ? 1 : 0;
+    toi[q] = s != 0 ? t : max_time;
+    if (tup) tup[q] = s != 0 ? u : max_time;
+  }
+}
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex[kNoAllocMaxDevices];
+unsigned char* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+bool device_buffer(const void* p, int dev) {
+  if (!p || (reinterpret_cast<uintptr_t>(p) & 3u)) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
+}
+}  // namespace
+
+NoAllocStatus ccd_batch_noalloc(bool vf, const float* x, int64_t n, const float* err3,
+                                const float* ms, float tol, int max_iter, float max_time,
+                                int* hit, float* toi, float* t_upper, cudaStream_t stream,
+                                int* n_spilled) {
+  if (n < 0 || !err3) return NoAllocStatus::kBadArgument;
+  if (n > kNoAllocMaxQueries || max_iter < 1 || max_iter > kNoAllocMaxIter)
+    return NoAllocStatus::kBeyondLimits;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+    cudaGetLastError();
+    return NoAllocStatus::kCudaError;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex[dev]);
+  if (!g_noalloc_addr[dev]) {
+    // One-time setup on this device (the device is current): resolving the
+    // symbol loads this module's kernels and its scratch array.
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_ccd_noalloc_scratch) != cudaSuccess || !p) {
+      cudaGetLastError();
+      return NoAllocStatus::kCudaError;
+    }
+    g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+  }
+  if (n_spilled) *n_spilled = 0;
+  if (n == 0) return NoAllocStatus::kOk;
+  if (!device_buffer(x, dev) || !device_buffer(ms, dev) || !device_buffer(hit, dev) ||
+      !device_buffer(toi, dev) || (t_upper && !device_buffer(t_upper, dev)))
+    return NoAllocStatus::kBadArgument;
+
+  unsigned char* base = g_noalloc_addr[dev];
+  int* counters = reinterpret_cast<int*>(base);
+  int* list = reinterpret_cast<int*>(base + kNoAllocListOffset);
+  IBox* spill = reinterpret_cast<IBox*>(base + kNoAllocSpillOffset);
+  const float3 e3 = make_float3(err3[0], err3[1], err3[2]);
+  if (cudaMemsetAsync(counters, 0, 4 * sizeof(int), stream) != cudaSuccess)
+    return NoAllocStatus::kCudaError;
+  CcdSpill first{nullptr, 0, nullptr, list, counters};
+  ccd_batch_kernel<<<div_up((int)n, kCollThreads), kCollThreads, 0, stream>>>(
+      vf, x, (int)n, e3, ms, tol, max_iter, max_time, hit, toi, t_upper, counters + 1, first);
+  SILK_LAUNCHED();
+  ccd_batch_spill_kernel<<<1, kNoAllocSpillSlots, 0, stream>>>(
+      vf, x, e3, ms, tol, max_iter, max_time, hit, toi, t_upper, counters, list, spill);
+  SILK_LAUNCHED();
+  if (cudaGetLastError() != cudaSuccess) return NoAllocStatus::kCudaError;
+  int h[4] = {0, 0, 0, 0};
+  if (cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess) {
+    cudaGetLastError();
+    return NoAllocStatus::kCudaError;
+  }
+  if (n_spilled) *n_spilled = h[0];
+  return h[1] > 0 ? NoAllocStatus::kStorageExhausted : NoAllocStatus::kOk;
 }
 
 }  // namespace silkb

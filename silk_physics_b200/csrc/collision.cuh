@@ -59,4 +59,15 @@ void ccd_batch_host(bool vf, const float* x, int64_t n, const float* err3,
 int color_contacts_host(const int* verts4, const uint64_t* prio, int64_t n,
                         int* colors);
 
+// CCD batch on caller-owned device buffers of the current device that
+// allocates no memory: all working memory is a static device array.
+constexpr int kNoAllocMaxQueries = 1 << 20;
+constexpr int kNoAllocMaxIter = 4096;
+constexpr int kNoAllocSpillSlots = 64;
+enum class NoAllocStatus { kOk, kBadArgument, kBeyondLimits, kCudaError, kStorageExhausted };
+NoAllocStatus ccd_batch_noalloc(bool vf, const float* x, int64_t n, const float* err3,
+                                const float* ms, float tol, int max_iter, float max_time,
+                                int* hit, float* toi, float* t_upper, cudaStream_t stream,
+                                int* n_spilled);
+
 }  // namespace silkb

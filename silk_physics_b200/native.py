@@ -236,6 +236,9 @@ def _load() -> C.CDLL:
                             C.c_float, _I32P, _F32P, _F32P], C.c_int),
         "silk_color_contacts": ([_I32P, _U64P, C.c_int64, _I32P, C.POINTER(C.c_int32)],
                                 C.c_int),
+        "silk_ccd_batch_noalloc": ([C.c_int32, C.c_void_p, C.c_int64, _F32P, C.c_void_p,
+                                    C.c_float, C.c_int32, C.c_float, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)], C.c_int),
         "silk_partition_mesh": ([_F32P, C.c_int64, _I32P, C.c_int64, _I32P, _I32P, C.c_int64,
                                  C.POINTER(C.c_int32)], C.c_int),
         "silk_assemble_cloth_host": ([C.POINTER(_ClothConfigC), _F32P, C.c_int64, _I32P,
@@ -458,6 +461,24 @@ def ccd_batch(is_vertex_face: bool, x: np.ndarray, err3, min_separation,
     if st:
         raise RuntimeError(_result(st).to_string())
     return hit.astype(bool), toi, tup
+
+
+# Mirrors SILK_CCD_NOALLOC_MAX_QUERIES / SILK_CCD_NOALLOC_MAX_ITER.
+CCD_NOALLOC_MAX_QUERIES = 1 << 20
+CCD_NOALLOC_MAX_ITER = 4096
+
+
+def ccd_batch_noalloc(is_vertex_face: bool, x_ptr: int, n: int, err3, ms_ptr: int,
+                      hit_ptr: int, toi_ptr: int, tup_ptr: int | None = None,
+                      tolerance: float = 1e-6, max_iter: int = 4096,
+                      max_time: float = 1.0, stream: int = 0) -> tuple[Result, int]:
+    """CCD batch on caller-owned device buffers (addresses on the current
+    device) that allocates nothing; returns (status, spilled query count)."""
+    spilled = C.c_int32(0)
+    st = lib.silk_ccd_batch_noalloc(int(is_vertex_face), x_ptr, n, _f32(err3), ms_ptr,
+                                    tolerance, max_iter, max_time, hit_ptr, toi_ptr,
+                                    tup_ptr, stream or None, C.byref(spilled))
+    return _result(st), spilled.value
 
 
 def partition_mesh(verts, faces) -> tuple[np.ndarray, np.ndarray]:
