@@ -147,7 +147,7 @@ def make_world(stream_handle, opts, V, F, SV, SF):
     return w, h, hs
 
 
-def cpu_oracle_sample(x0, v0, V, F, SV, SF, gpu_steps_per_admm, budget_s=20.0):
+def cpu_oracle_sample(x0, v0, V, F, SV, SF, cg_rel_tol, budget_s=20.0):
     """Time the CPU restatement from the same state on all host cores.
 
     Contact steps of this algorithm take minutes on a CPU, so the sample is
@@ -155,7 +155,8 @@ def cpu_oracle_sample(x0, v0, V, F, SV, SF, gpu_steps_per_admm, budget_s=20.0):
     sys.path.insert(0, str(ROOT / "oracle"))
     import pyoracle
 
-    ow = pyoracle.OracleWorld(config=dict(acceleration=(0.0, 0.0, -9.81)))
+    ow = pyoracle.OracleWorld(config=dict(acceleration=(0.0, 0.0, -9.81),
+                                          fixed_linear_rel_tol=cg_rel_tol))
     nv = len(V)
     perm = np.arange(nv, dtype=np.int32)
     offs = np.unique(np.append(np.arange(0, nv, 32), nv)).astype(np.int32)
@@ -270,8 +271,8 @@ def run_ours(args) -> None:
     cpu = None
     if world_size == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        sps, n, el, cadmm = cpu_oracle_sample(state_x, state_v, V, F, SV, SF, None,
-                                               args.cpu_budget)
+        sps, n, el, cadmm = cpu_oracle_sample(state_x, state_v, V, F, SV, SF,
+                                               args.cg_rel_tol, args.cpu_budget)
         cpu = {"value": round(sps, 6), "unit": "steps/s", "cores": threads, "kind": "port",
                "sample": f"{n} step(s) of the same scene from the GPU state after "
                          f"{args.prelude + args.warmup} steps, {el:.1f} s wall, "
@@ -312,7 +313,8 @@ def run_reference(args) -> None:
     import pyoracle
 
     V, F, SV, SF = scene()
-    ow = pyoracle.OracleWorld(config=dict(acceleration=(0.0, 0.0, -9.81)))
+    ow = pyoracle.OracleWorld(config=dict(acceleration=(0.0, 0.0, -9.81),
+                                          fixed_linear_rel_tol=args.cg_rel_tol))
     nv = len(V)
     perm = np.arange(nv, dtype=np.int32)
     offs = np.unique(np.append(np.arange(0, nv, 32), nv)).astype(np.int32)
@@ -359,7 +361,8 @@ def main() -> None:
     ap.add_argument("--prelude", type=int, default=24)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--cg-rel-tol", type=float, default=0.0)
+    ap.add_argument("--cg-rel-tol", type=float, default=1e-5,
+                    help="fixed CG relative tolerance (0 = the reference's adaptive rule)")
     ap.add_argument("--bf16", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -85,8 +85,11 @@ typedef struct {
                                  admm_solver.cu:228-233 */
   int32_t cg_max_iter;        /* 1000 (mas_cg_solver.cuh:25) */
   int32_t mas_bf16;           /* 0: FP32 bank inverses; 1: BF16 storage */
-  int32_t profile;            /* 1: time the CG kernel with CUDA events */
-  int32_t reserved[4];
+  int32_t profile;            /* 1: time the CG kernel with CUDA events;
+                                 2: also record the CG phase trace */
+  int32_t cg_form;            /* 0: resident CG kernel where the system fits
+                                 it, else streaming; 1: streaming always */
+  int32_t reserved[3];
 } silk_solver_options;
 
 /* CUDA-event timing of the persistent CG kernel over the steps since the
@@ -119,7 +122,8 @@ typedef struct {
   float min_toi;
   int32_t broadphase_candidates;
   int64_t kernel_launches;
-  int32_t reserved[6];
+  int32_t cg_resident_solves;  /* CG solves that ran in the resident form */
+  int32_t reserved[5];
 } silk_step_stats;
 
 /* --- World lifetime (silk.hpp:92-100) ---------------------------------- */
@@ -183,6 +187,14 @@ silk_status silk_get_profile(silk_world* w, silk_profile* p, int32_t reset);
 /* Vertex velocities of a cloth in mesh order (3 * vertex count floats). */
 silk_status silk_get_cloth_velocity(const silk_world* w, uint32_t handle,
                                     float* velocity, int64_t velocity_len);
+
+/* Phase trace of the last CG solve of a cloth, recorded when the solver
+ * option profile is 2: [0],[1] globaltimer (ns) and clock64 at kernel entry,
+ * [2],[3] at exit, [4] traced iterations k (at most 64), [5] kernel form
+ * (0 streaming, 1 resident), then 16 clock64 phase stamps per iteration
+ * (block 0, thread 0).  cap >= 1032; *n = 0 when nothing was traced. */
+silk_status silk_debug_cg_trace(const silk_world* w, uint32_t handle, int64_t* trace,
+                               int64_t cap, int32_t* n);
 
 /* --- Inspection entry points used by the parity tests ------------------- */
 /* Solver-order permutation (original -> solver) and partition offsets. */

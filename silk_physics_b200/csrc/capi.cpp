@@ -223,6 +223,14 @@ silk_status silk_debug_cloth_partition(const silk_world* w, uint32_t handle,
   });
 }
 
+silk_status silk_debug_cg_trace(const silk_world* w, uint32_t handle, int64_t* trace,
+                               int64_t cap, int32_t* n) {
+  if (!trace || !n) return SILK_ERR_INVALID_CONFIG;
+  return guard_init(const_cast<silk_world*>(w), [&](World& W) {
+    return W.debug_cg_trace(handle, trace, cap, n);
+  });
+}
+
 silk_status silk_debug_cloth_matrix(const silk_world* w, uint32_t handle,
                                     double* dense, int64_t n_len) {
   return guard_init(const_cast<silk_world*>(w), [&](World& W) {

@@ -1137,6 +1137,94 @@ __global__ void contact_gs_kernel(const ContactDev* contacts, const int* groups,
     }
 }
 
+// Single-block form of contact_gs_kernel for contact sets whose largest
+// colour fits one block (at most one contact per thread and colour) and whose
+// cloth vertices fit in shared memory.  The positions stay in shared memory
+// for the whole solve, colour phases are separated by __syncthreads, and the
+// contact of the next colour is loaded while the current one is processed.
+// Each contact goes through the same operations in the same order as in
+// contact_gs_kernel (contacts of one colour touch disjoint vertices), so both
+// forms give identical results.
+constexpr int kGsBlockThreads = 1024;
+constexpr size_t kGsBlockSmemMax = 200 * 1024;
+__global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
+    const ContactDev* __restrict__ contacts, const int* __restrict__ groups,
+    const int* __restrict__ group_off, int ncolors, float4* corr, float4* p, int nv) {
+  extern __shared__ float4 sp[];
+  for (int v = threadIdx.x; v < nv; v += blockDim.x) sp[v] = p[v];
+  const int t = threadIdx.x;
+  // A thread always takes the same contact of a colour, so the correction it
+  // prefetches was last written by itself.
+  auto fetch = [&](int col, int& ci, ContactDev& k, float4& o) {
+    int q = group_off[col] + t;
+    ci = q < group_off[col + 1] ? groups[q] : -1;
+    if (ci >= 0) {
+      k = contacts[ci];
+      o = corr[ci];
+    }
+  };
+  __syncthreads();
+  // Warm start with the saved corrections.
+  for (int col = 0; col < ncolors; ++col) {
+    int q = group_off[col] + t;
+    if (q < group_off[col + 1]) {
+      int ci = groups[q];
+      const ContactDev& k = contacts[ci];
+      float4 r = corr[ci];
+      for (int s = 0; s < 4; ++s) {
+        if (k.gamma[s] == 0.0f) continue;
+        float4 x = sp[k.v[s]];
+        float g = k.gamma[s];
+        sp[k.v[s]] = make_float4(x.x + g * r.x, x.y + g * r.y, x.z + g * r.z, 0.f);
+      }
+    }
+    __syncthreads();
+  }
+  const int phases = kGsSweeps * ncolors;
+  int ci = -1;
+  ContactDev k;
+  float4 on = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (phases > 0) fetch(0, ci, k, on);
+  for (int ph = 0; ph < phases; ++ph) {
+    const int cur = ci;
+    const ContactDev kc = k;
+    const float4 o = on;
+    if (ph + 1 < phases) fetch((ph + 1) % ncolors, ci, k, on);
+    if (cur >= 0) {
+      float3 u = kc.affine;
+      for (int s = 0; s < 4; ++s)
+        if (kc.v[s] >= 0) {
+          float4 x = sp[kc.v[s]];
+          u = add3(u, sc3(kc.coef[s], make_float3(x.x, x.y, x.z)));
+        }
+      float3 old = make_float3(o.x, o.y, o.z);
+      float3 us = sub3(u, old);
+      float un = dot3(us, kc.normal);
+      float3 unew;
+      if (un >= 0.0f) {
+        unew = us;
+      } else {
+        float3 ut = sub3(us, sc3(un, kc.normal));
+        float utn = sqrtf(dot3(ut, ut));
+        float radius = -kc.friction * un;
+        unew = utn <= radius ? make_float3(0.f, 0.f, 0.f) : sc3(1.0f - radius / utn, ut);
+      }
+      float3 du = sub3(unew, u);
+      float3 nc = add3(old, du);
+      corr[cur] = make_float4(nc.x, nc.y, nc.z, 0.f);
+      if (ci == cur) on = make_float4(nc.x, nc.y, nc.z, 0.f);  // one colour
+      for (int s = 0; s < 4; ++s) {
+        if (kc.gamma[s] == 0.0f) continue;
+        float4 x = sp[kc.v[s]];
+        float g = kc.gamma[s];
+        sp[kc.v[s]] = make_float4(x.x + g * du.x, x.y + g * du.y, x.z + g * du.z, 0.f);
+      }
+    }
+    __syncthreads();
+  }
+  for (int v = threadIdx.x; v < nv; v += blockDim.x) p[v] = sp[v];
+}
+
 // Canonical contact key (contact_constraints.cu:24-47).
 struct Key {
   int type;
@@ -1766,6 +1854,21 @@ void CollisionSystem::contact_solve() {
   CollisionImpl& I = *impl_;
   if (I.n_contacts == 0) return;
   cudaStream_t st = w_.stream;
+  const int nv = (int)w_.contact_p.n;
+  const size_t smem = (size_t)nv * sizeof(float4);
+  if (I.max_group <= kGsBlockThreads && smem <= kGsBlockSmemMax) {
+    static bool attr = false;
+    if (!attr) {
+      CUDA_CHECK(cudaFuncSetAttribute(contact_gs_block_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kGsBlockSmemMax));
+      attr = true;
+    }
+    contact_gs_block_kernel<<<1, kGsBlockThreads, smem, st>>>(
+        I.contacts.p, I.groups.p, I.group_off.p, I.n_colors, I.corr.p, w_.contact_p.p, nv);
+    SILK_LAUNCHED();
+    return;
+  }
   static int max_coop = 0;
   if (max_coop == 0) {
     int dev = 0, sms = 0, per = 0;

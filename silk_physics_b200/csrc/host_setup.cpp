@@ -218,11 +218,14 @@ void partition_mesh(const float* verts, int nv, const int* faces, int nf,
     y = (y | y << 2) & 0x1249249249249249ULL;
     return y;
   };
+  // One scale for all axes (a cube around the mesh): a nearly flat axis must
+  // not have its noise stretched over the full code range.
+  double ext = 0.0;
+  for (int d = 0; d < 3; ++d) ext = std::max(ext, (double)hi[d] - lo[d]);
   std::vector<uint64_t> code(nv);
   for (int i = 0; i < nv; ++i) {
     uint64_t c = 0;
     for (int d = 0; d < 3; ++d) {
-      double ext = (double)hi[d] - lo[d];
       double u = ext > 0 ? ((double)verts[3 * i + d] - lo[d]) / ext : 0.0;
       uint32_t q = (uint32_t)std::min(2097151.0, std::max(0.0, u * 2097151.0));
       c |= spread(q) << d;

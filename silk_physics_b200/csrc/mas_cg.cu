@@ -13,7 +13,12 @@
 //    cooperative kernel whose phases are separated by a grid barrier with a
 //    bounded spin (no host round trip, no graph rebuild per solve);
 //  * reductions are FP64 and deterministic (per-block partials summed in a
-//    fixed order by every block).
+//    fixed order by every block);
+//  * where the hierarchy allows it (every fine bank one coarse node, small
+//    upper levels) the solve runs in the resident form: one block per
+//    first-level coarse bank keeps its vertices' CG vectors in registers and
+//    its bank inverses in shared memory, three barriers per iteration, and
+//    BF16-stored inverses are applied with mma.sync (FP32 accumulation).
 #include <cooperative_groups.h>
 #include <cuda/atomic>
 
@@ -329,23 +334,61 @@ struct ClusterBarrier {
   }
 };
 
+__device__ __forceinline__ long long global_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Phase stamps of block 0 (slots: 0 prolongation done, 1 its barrier passed,
+// 2 SpMV done, 3 barrier, 4 fine level done, 5 barrier, 6 coarse levels
+// done, 7 barrier).
+struct CgTrace {
+  long long* t;
+  __device__ CgTrace(long long* p, int form)
+      : t(blockIdx.x == 0 && threadIdx.x == 0 ? p : nullptr) {
+    if (t) {
+      t[0] = global_ns();
+      t[1] = clock64();
+      t[5] = form;
+    }
+  }
+  __device__ __forceinline__ void stamp(int iter, int slot) {
+    if (t && iter >= 0 && iter < kCgTraceIters) {
+      long long c = clock64();
+      for (int k = slot; k < kCgTraceSlots; ++k) t[8 + iter * kCgTraceSlots + k] = c;
+    }
+  }
+  __device__ void finish(int iters) {
+    if (!t) return;
+    t[2] = global_ns();
+    t[3] = clock64();
+    t[4] = iters < kCgTraceIters ? iters : kCgTraceIters;
+  }
+};
+
+__device__ __forceinline__ void mark_fail(const CgArgs& a) {
+  if (threadIdx.x == 0 && a.fail) atomicExch(a.fail, 1);
+}
+
 template <class Barrier>
 __device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm_all) {
   double* part = a.partials + 4 * blockIdx.x;
+  CgTrace tr(a.trace, 0);
   // r = b - A x.
   spmv_phase(a, a.x, a.r, 1);
-  if (!bar.sync()) return;
+  if (!bar.sync()) return mark_fail(a);
   {
     double v[2] = {0.0, 0.0};
     fine_phase(a, 0.f, false, sm_all, v[0], v[1]);
     block_sum<2>(v, part);
   }
-  if (!bar.sync()) return;
+  if (!bar.sync()) return mark_fail(a);
   if (blockIdx.x == 0) {
     double v[1] = {coarse_phase(a, sm_all)};
     block_sum<1>(v, a.coarse_partial);
   }
-  if (!bar.sync()) return;
+  if (!bar.sync()) return mark_fail(a);
   double rz = grid_total(a.partials, 0, gridDim.x) + *a.coarse_partial;
   double rr = grid_total(a.partials, 1, gridDim.x);
   if (!isfinite(rz)) {
@@ -364,12 +407,16 @@ __device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm
   int status = kCgMaxIter;
   while (true) {
     prolong_phase(a, (float)beta);
-    if (!bar.sync()) return;
+    tr.stamp(iter, 0);
+    if (!bar.sync()) return mark_fail(a);
+    tr.stamp(iter, 1);
     {
       double v[1] = {spmv_phase(a, a.p, a.Ap, 0)};
       block_sum<1>(v, part + 2);
     }
-    if (!bar.sync()) return;
+    tr.stamp(iter, 2);
+    if (!bar.sync()) return mark_fail(a);
+    tr.stamp(iter, 3);
     double pAp = grid_total(a.partials, 2, gridDim.x);
     double alpha = fabs(pAp) < 1e-20 ? 0.0 : rz / pAp;
     {
@@ -377,12 +424,16 @@ __device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm
       fine_phase(a, (float)alpha, true, sm_all, v[0], v[1]);
       block_sum<2>(v, part);
     }
-    if (!bar.sync()) return;
+    tr.stamp(iter, 4);
+    if (!bar.sync()) return mark_fail(a);
+    tr.stamp(iter, 5);
     if (blockIdx.x == 0) {
       double v[1] = {coarse_phase(a, sm_all)};
       block_sum<1>(v, a.coarse_partial);
     }
-    if (!bar.sync()) return;
+    tr.stamp(iter, 6);
+    if (!bar.sync()) return mark_fail(a);
+    tr.stamp(iter, 7);
     double rz_old = rz;
     rz = grid_total(a.partials, 0, gridDim.x) + *a.coarse_partial;
     rr = grid_total(a.partials, 1, gridDim.x);
@@ -401,6 +452,7 @@ __device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm
     beta = fabs(rz_old) < 1e-20 ? 0.0 : rz / rz_old;
     if (stop) break;
   }
+  tr.finish(iter);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.result[0] = iter;
     a.result[1] = status;
@@ -422,6 +474,482 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel_cluster(CgArgs a) {
   extern __shared__ float sm_all[];
   ClusterBarrier bar;
   cg_body(a, bar, sm_all);
+}
+
+// ---------------------------------------------------------------------------
+// Resident PCG: block k owns first-level coarse bank k, i.e. the fine banks
+// 32k .. 32k+31, with one thread per fine-bank slot (warp w = fine bank
+// 32k+w, lane = slot).  Every vertex's x, r, p, Ap and its MAS output stay
+// in registers for the whole solve; the block's fine and first-level bank
+// inverses and the (few) banks of all higher levels are staged in shared
+// memory once per solve.  Only p crosses blocks (through a global exchange
+// buffer; neighbours inside the block are read from shared memory), plus the
+// per-block partial sums and the residual restricted to the second coarse
+// level, which every block then solves redundantly.  That leaves three
+// barriers per iteration:
+//   A  totals, coarse levels >= 2, p = z + beta p, publish p      | barrier
+//   B  Ap = A p (sliced ELL, bank-aligned slices), p.Ap partial    | barrier
+//   C  alpha, x/r update, fine and first-level MAS, restriction,   | barrier
+//      r.z and r.r partials
+// The arithmetic of each vector entry is that of cg_kernel; only the order
+// of the FP64 block sums (and of the off-diagonal terms of a row: entries
+// from other blocks first) differs.
+// ---------------------------------------------------------------------------
+constexpr int kResWarps = kResThreads / 32;
+
+// A bank slot of shared memory holds either the packed FP32 inverse (528
+// floats) or, for BF16 storage, the inverse as mma.m16n8k16 A fragments:
+// 4 tiles (2 row x 2 column halves) x 32 lanes x 8 bf16 = 2048 bytes.
+struct ResShared {
+  float Mf[kResWarps][kPacked];
+  float M1[kPacked];
+  float Mc[kResCoarseBanks][kPacked];
+  float4 pl[kResThreads];
+  float4 r1[32];
+  float4 z1[32];
+  float4 rc[kResCoarseBanks * BANK];
+  float4 zc[kResCoarseBanks * BANK];
+  __nv_bfloat16 rb[kResWarps][8][BANK];  // BF16 apply: residual as B operand (rows 3..7 zero)
+  float4 zs[kResWarps][BANK];             // BF16 apply: accumulator rows back to slots
+  double red[kResWarps][3];
+  double tot[3];
+};
+static_assert(offsetof(ResShared, M1) % 16 == 0 && offsetof(ResShared, Mc) % 16 == 0 &&
+                  (kPacked * sizeof(float)) % 16 == 0,
+              "bank slots hold 16-byte fragments");
+
+// Stage a bank inverse stored as packed BF16 into A-fragment order: lane
+// (g = lane / 4, t = lane % 4) of tile (mt, kt) holds rows 16 mt + g (+8) and
+// columns 16 kt + 2t (+1, +8, +9), the m16n8k16 row-major A layout.
+__device__ __forceinline__ void stage_bank_frag(const MasLevelDev& lv, int bank, float* slot,
+                                                int lane) {
+  const __nv_bfloat16* src = lv.Mb + (size_t)bank * kPacked;
+  uint4* dst = reinterpret_cast<uint4*>(slot);
+  const int g = lane >> 2, t = lane & 3;
+  auto pair = [&](int i, int j) -> unsigned {
+    unsigned lo = __bfloat16_as_ushort(src[upper_index(BANK, i, j)]);
+    unsigned hi = __bfloat16_as_ushort(src[upper_index(BANK, i, j + 1)]);
+    return lo | (hi << 16);
+  };
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int kt = 0; kt < 2; ++kt) {
+      const int r0 = 16 * mt + g, c0 = 16 * kt + 2 * t;
+      uint4 q;
+      q.x = pair(r0, c0);
+      q.y = pair(r0 + 8, c0);
+      q.z = pair(r0, c0 + 8);
+      q.w = pair(r0 + 8, c0 + 8);
+      dst[(mt * 2 + kt) * 32 + lane] = q;
+    }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint4& a, unsigned b0,
+                                         unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, "
+      "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a.x), "r"(a.y), "r"(a.z), "r"(a.w), "r"(b0), "r"(b1));
+}
+
+// z (lane slot) = M r on the tensor cores: Z (32 x 8) = M (32 x 32) R (32 x 8),
+// R holding the three channels of r in BF16 and zero columns 3..7, FP32
+// accumulation; four m16n8k16 products per bank.
+__device__ __forceinline__ float3 bank_apply_mma(const float* slot, float3 r, int lane,
+                                                 __nv_bfloat16 (*rb)[BANK], float4* zs) {
+  rb[0][lane] = __float2bfloat16_rn(r.x);
+  rb[1][lane] = __float2bfloat16_rn(r.y);
+  rb[2][lane] = __float2bfloat16_rn(r.z);
+  __syncwarp();
+  const int g = lane >> 2, t = lane & 3;
+  const unsigned* rw = reinterpret_cast<const unsigned*>(&rb[g][0]);
+  unsigned b[2][2];
+#pragma unroll
+  for (int kt = 0; kt < 2; ++kt) {
+    b[kt][0] = rw[kt * 8 + t];
+    b[kt][1] = rw[kt * 8 + 4 + t];
+  }
+  const uint4* frag = reinterpret_cast<const uint4*>(slot);
+  float c[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int kt = 0; kt < 2; ++kt) mma_bf16(c[mt], frag[(mt * 2 + kt) * 32 + lane], b[kt][0], b[kt][1]);
+  if (t < 2) {
+    float* z = reinterpret_cast<float*>(zs);
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+      const int row = 16 * mt + g;
+      *reinterpret_cast<float2*>(z + 4 * row + 2 * t) = make_float2(c[mt][0], c[mt][1]);
+      *reinterpret_cast<float2*>(z + 4 * (row + 8) + 2 * t) = make_float2(c[mt][2], c[mt][3]);
+    }
+  }
+  __syncwarp();
+  float4 q = zs[lane];
+  __syncwarp();
+  return make_float3(q.x, q.y, q.z);
+}
+
+// Block sums of up to three doubles per thread, in a fixed order; thread 0
+// of the block stores them to out (global) when out is not null.  The sums
+// are left in s.tot.
+template <int N>
+__device__ void res_block_sum(const double (&v)[N], ResShared& s, double* out) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    double a = warp_sum_d(v[k]);
+    if (lane == 0) s.red[warp][k] = a;
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      double a = warp_sum_d(s.red[lane][k]);
+      if (lane == 0) {
+        s.tot[k] = a;
+        if (out) out[k] = a;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Sum of slot `slot` of every block's partials, the same in every block.
+__device__ double res_total(const double* partials, int slot, int nblocks, ResShared& s) {
+  if (threadIdx.x < 32) {
+    double a = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += 32) a += __ldcg(partials + 4 * b + slot);
+    a = warp_sum_d(a);
+    if (threadIdx.x == 0) s.tot[slot] = a;
+  }
+  __syncthreads();
+  double t = s.tot[slot];
+  __syncthreads();
+  return t;
+}
+
+__device__ __forceinline__ float4 ldcg4(const float4* p) { return __ldcg(p); }
+
+// Off-diagonal row sum of this thread's vertex plus the diagonal term.
+__device__ __forceinline__ float3 res_row(const CgArgs& a, const ResShared& s,
+                                          const float4* ex, int rptr, int rw,
+                                          int lane, float d, float3 pv) {
+  float yx = d * pv.x, yy = d * pv.y, yz = d * pv.z;
+  const int2* e = a.rent + rptr + lane;
+#pragma unroll 4
+  for (int j = 0; j < rw; ++j) {
+    int2 q = e[j * BANK];
+    float val = __int_as_float(q.y);
+    float4 pj = q.x < 0 ? s.pl[-1 - q.x] : ldcg4(ex + q.x);
+    yx += val * pj.x;
+    yy += val * pj.y;
+    yz += val * pj.z;
+  }
+  return make_float3(yx, yy, yz);
+}
+
+template <class Barrier>
+__device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int k = blockIdx.x;
+  const int nblocks = gridDim.x;
+  const int fb = k * BANK + warp;
+  const bool bank_ok = fb < a.nbank0;
+  const bool has1 = a.levels > 0;
+  CgTrace tr(a.trace, 1);
+  int iter = -1;  // -1 while setting up (not traced)
+  double* part = a.partials + 4 * k;
+  auto fail = [&]() {
+    if (tid == 0 && a.fail) atomicExch(a.fail, 1);
+  };
+
+  // ---- one-time staging ----------------------------------------------------
+  // BF16 storage: inverses staged as tensor-core fragments and applied with
+  // mma.sync; FP32 storage: packed FP32 and the SIMT apply.
+  const bool tc = a.bf16 != 0;
+  auto stage = [&](const MasLevelDev& lv, int bank, float* slot) {
+    if (tc)
+      stage_bank_frag(lv, bank, slot, lane);
+    else
+      stage_bank(lv, 0, bank, slot, lane);
+  };
+  auto apply = [&](const float* slot, float3 r) {
+    return tc ? bank_apply_mma(slot, r, lane, s.rb[warp], s.zs[warp]) : bank_apply(slot, r, lane);
+  };
+  for (int i = lane; i < 5 * BANK; i += 32) s.rb[warp][3 + i / BANK][i % BANK] = __float2bfloat16_rn(0.f);
+  int vbase = 0, vsize = 0, rptr = 0, rw = 0;
+  if (bank_ok) {
+    vbase = a.part_off[fb];
+    vsize = a.part_off[fb + 1] - vbase;
+    rptr = a.rb_ptr[fb];
+    rw = a.rb_w[fb];
+    stage(a.fine, fb, s.Mf[warp]);
+  }
+  const bool own = lane < vsize;
+  const int v = vbase + lane;
+  if (has1 && warp == 0) stage(a.coarse[0], k, s.M1);
+  // First-level restriction plan of this block's coarse bank (warp 0).
+  int l1_ncco = 0, l1_base = 0, l1_mine = -1;
+  if (has1 && warp == 0 && a.levels > 1) {
+    l1_ncco = a.coarse[0].ncco[k];
+    l1_base = a.coarse[0].cco_base[k];
+    l1_mine = a.coarse[0].slot_cco[(size_t)k * BANK + lane];
+  }
+  {
+    int cb = 0;
+    for (int l = 1; l < a.levels; ++l) {
+      for (int j = warp; j < a.coarse[l].nbank; j += kResWarps)
+        stage(a.coarse[l], j, s.Mc[cb + j]);
+      cb += a.coarse[l].nbank;
+    }
+    for (int i = tid; i < kResCoarseBanks * BANK; i += kResThreads)
+      s.rc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  float d = 0.f;
+  float3 x = make_float3(0.f, 0.f, 0.f), b = x;
+  int cm[4] = {-1, -1, -1, -1};
+  if (own) {
+    d = a.Ldiag[v] + a.dyn[v];
+    float4 x4 = a.x[v], b4 = a.b[v];
+    x = make_float3(x4.x, x4.y, x4.z);
+    b = make_float3(b4.x, b4.y, b4.z);
+    if (has1) {
+      int4 c = a.cmap[v];
+      cm[0] = c.x;
+      cm[1] = c.y;
+      cm[2] = c.z;
+      cm[3] = c.w;
+    }
+  }
+  // Publish x for r = b - A x.
+  s.pl[tid] = make_float4(x.x, x.y, x.z, 0.f);
+  if (own) a.p[v] = make_float4(x.x, x.y, x.z, 0.f);
+  if (!bar.sync()) return fail();
+  float3 r;
+  {
+    float3 y = res_row(a, s, a.p, rptr, rw, lane, d, x);
+    r = own ? make_float3(b.x - y.x, b.y - y.y, b.z - y.z) : make_float3(0.f, 0.f, 0.f);
+  }
+
+  // Phase C body: fine and first-level MAS of r, restriction to level 2,
+  // partials (r.z, r.r) of this block.
+  float3 z0, p = make_float3(0.f, 0.f, 0.f), Ap = p;
+  auto mas_fine = [&]() {
+    double rr = own ? (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z : 0.0;
+    z0 = bank_ok ? apply(s.Mf[warp], r) : make_float3(0.f, 0.f, 0.f);
+    if (!own) z0 = make_float3(0.f, 0.f, 0.f);
+    double rz = own ? (double)r.x * z0.x + (double)r.y * z0.y + (double)r.z * z0.z : 0.0;
+    if (has1) {
+      float sx = warp_sum(r.x), sy = warp_sum(r.y), sz = warp_sum(r.z);
+      if (lane == 0) s.r1[warp] = make_float4(sx, sy, sz, 0.f);
+      tr.stamp(iter, 6);
+      __syncthreads();
+      if (warp == 0) {
+        bool valid = k * BANK + lane < a.coarse[0].nnode;
+        float4 q = s.r1[lane];
+        float3 r1 = valid ? make_float3(q.x, q.y, q.z) : make_float3(0.f, 0.f, 0.f);
+        float3 z1 = apply(s.M1, r1);
+        if (!valid) z1 = make_float3(0.f, 0.f, 0.f);
+        s.z1[lane] = make_float4(z1.x, z1.y, z1.z, 0.f);
+        rz += (double)r1.x * z1.x + (double)r1.y * z1.y + (double)r1.z * z1.z;
+        for (int c = 0; c < l1_ncco; ++c) {
+          float qx = warp_sum(l1_mine == c ? r1.x : 0.f);
+          float qy = warp_sum(l1_mine == c ? r1.y : 0.f);
+          float qz = warp_sum(l1_mine == c ? r1.z : 0.f);
+          if (lane == 0) a.coarse[0].rout[l1_base + c] = make_float4(qx, qy, qz, 0.f);
+        }
+      }
+    }
+    tr.stamp(iter, 7);
+    const double v2[2] = {rz, rr};
+    res_block_sum<2>(v2, s, part);
+    tr.stamp(iter, 8);
+  };
+  // Phase A head: totals and the redundant coarse levels >= 2.
+  auto totals = [&](double& rz, double& rr) {
+    // One round trip: warp 0 sums the partials while the other warps load the
+    // residual restricted to the second coarse level.
+    if (warp == 0) {
+      double s0 = 0.0, s1 = 0.0;
+      for (int q = lane; q < nblocks; q += 32) {
+        s0 += __ldcg(a.partials + 4 * q);
+        s1 += __ldcg(a.partials + 4 * q + 1);
+      }
+      s0 = warp_sum_d(s0);
+      s1 = warp_sum_d(s1);
+      if (lane == 0) {
+        s.tot[0] = s0;
+        s.tot[1] = s1;
+      }
+    } else if (a.levels > 1) {
+      for (int i = tid - 32; i < a.coarse[1].nnode; i += kResThreads - 32)
+        s.rc[i] = ldcg4(a.coarse[0].rout + i);
+    }
+    __syncthreads();
+    tr.stamp(iter, 10);
+    rz = s.tot[0];
+    rr = s.tot[1];
+    if (a.levels > 1) {
+      double rzc = 0.0;
+      int cb = 0;
+      for (int l = 1; l < a.levels; ++l) {
+        const MasLevelDev& lv = a.coarse[l];
+        const bool last = l + 1 >= a.levels;
+        if (warp < lv.nbank) {
+          int slot = (cb + warp) * BANK + lane;
+          bool valid = warp * BANK + lane < lv.nnode;
+          float4 q = s.rc[slot];
+          float3 rl = valid ? make_float3(q.x, q.y, q.z) : make_float3(0.f, 0.f, 0.f);
+          float3 zl = apply(s.Mc[cb + warp], rl);
+          if (!valid) zl = make_float3(0.f, 0.f, 0.f);
+          s.zc[slot] = make_float4(zl.x, zl.y, zl.z, 0.f);
+          rzc += (double)rl.x * zl.x + (double)rl.y * zl.y + (double)rl.z * zl.z;
+          if (!last) {
+            int n = lv.ncco[warp], base = lv.cco_base[warp];
+            int mine = lv.slot_cco[(size_t)warp * BANK + lane];
+            int next = (cb + lv.nbank) * BANK;
+            for (int c = 0; c < n; ++c) {
+              float qx = warp_sum(mine == c ? rl.x : 0.f);
+              float qy = warp_sum(mine == c ? rl.y : 0.f);
+              float qz = warp_sum(mine == c ? rl.z : 0.f);
+              if (lane == 0) s.rc[next + base + c] = make_float4(qx, qy, qz, 0.f);
+            }
+          }
+        }
+        cb += lv.nbank;
+        __syncthreads();
+      }
+      tr.stamp(iter, 11);
+      const double v1[1] = {rzc};
+      res_block_sum<1>(v1, s, nullptr);
+      rz += s.tot[0];
+    }
+  };
+  // Phase A tail: full preconditioned residual of this vertex.
+  auto mas_total = [&]() {
+    float3 z = z0;
+    if (own && has1) {
+      float4 q = s.z1[warp];
+      z.x += q.x;
+      z.y += q.y;
+      z.z += q.z;
+      int cb = 0;
+#pragma unroll
+      for (int l = 1; l < 4; ++l) {
+        if (l >= a.levels) break;
+        float4 c = s.zc[cb * BANK + cm[l]];
+        z.x += c.x;
+        z.y += c.y;
+        z.z += c.z;
+        cb += a.coarse[l].nbank;
+      }
+    }
+    return z;
+  };
+
+  mas_fine();
+  if (!bar.sync()) return fail();
+  double rz, rr;
+  totals(rz, rr);
+  iter = 0;
+  if (!isfinite(rz)) {
+    if (k == 0 && tid == 0) {
+      a.result[0] = 0;
+      a.result[1] = kCgInvalidInitialResidual;
+      *a.result_rr = (float)rr;
+    }
+    return;
+  }
+  const double rr0 = rr;
+  const double abs2 = (double)a.abs_tol * a.abs_tol;
+  const double rel2 = (double)a.rel_tol * a.rel_tol;
+  double beta = 0.0;
+  int status = kCgMaxIter;
+  while (true) {
+    // A tail: p = z + beta p, published.
+    {
+      float3 z = mas_total();
+      const float bt = (float)beta;
+      p = bt == 0.0f ? z : make_float3(z.x + bt * p.x, z.y + bt * p.y, z.z + bt * p.z);
+      if (!own) p = make_float3(0.f, 0.f, 0.f);
+      s.pl[tid] = make_float4(p.x, p.y, p.z, 0.f);
+      if (own) a.p[v] = make_float4(p.x, p.y, p.z, 0.f);
+    }
+    tr.stamp(iter, 0);
+    if (!bar.sync()) return fail();
+    tr.stamp(iter, 1);
+    // B: Ap and p.Ap.
+    {
+      Ap = res_row(a, s, a.p, rptr, rw, lane, d, p);
+      if (!own) Ap = make_float3(0.f, 0.f, 0.f);
+      tr.stamp(iter, 2);
+      const double v1[1] = {own ? (double)p.x * Ap.x + (double)p.y * Ap.y + (double)p.z * Ap.z
+                                : 0.0};
+      res_block_sum<1>(v1, s, part + 2);
+    }
+    tr.stamp(iter, 3);
+    if (!bar.sync()) return fail();
+    tr.stamp(iter, 4);
+    // C: alpha, x/r update, fine + first-level MAS.
+    {
+      double pAp = res_total(a.partials, 2, nblocks, s);
+      tr.stamp(iter, 5);
+      const float alpha = (float)(fabs(pAp) < 1e-20 ? 0.0 : rz / pAp);
+      x = make_float3(alpha * p.x + x.x, alpha * p.y + x.y, alpha * p.z + x.z);
+      r = make_float3(-alpha * Ap.x + r.x, -alpha * Ap.y + r.y, -alpha * Ap.z + r.z);
+      if (!own) r = make_float3(0.f, 0.f, 0.f);
+      mas_fine();
+    }
+    if (!bar.sync()) return fail();
+    tr.stamp(iter, 9);
+    // A head: totals, coarse levels, stopping rules.
+    double rz_old = rz;
+    totals(rz, rr);
+    tr.stamp(iter, 12);
+    ++iter;
+    bool stop = false;
+    if (iter >= a.max_iter) {
+      status = kCgMaxIter;
+      stop = true;
+    } else if (rr <= abs2) {
+      status = kCgAbsTol;
+      stop = true;
+    } else if (rr <= rel2 * rr0) {
+      status = kCgRelTol;
+      stop = true;
+    }
+    beta = fabs(rz_old) < 1e-20 ? 0.0 : rz / rz_old;
+    if (stop) break;
+  }
+  if (own) a.x[v] = make_float4(x.x, x.y, x.z, 0.f);
+  tr.finish(iter);
+  if (k == 0 && tid == 0) {
+    a.result[0] = iter;
+    a.result[1] = status;
+    *a.result_rr = (float)rr;
+    if (a.stats) {
+      atomicAdd(a.stats, iter);
+      atomicAdd(a.stats + 1, 1);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kResThreads, 1) cg_resident_kernel(CgArgs a) {
+  extern __shared__ __align__(16) unsigned char res_smem[];
+  ResShared& s = *reinterpret_cast<ResShared*>(res_smem);
+  GridBarrier bar{a.barrier, a.barrier + 1, a.barrier + 2, gridDim.x};
+  res_body(a, bar, s);
+}
+
+__global__ void __launch_bounds__(kResThreads, 1) cg_resident_cluster_kernel(CgArgs a) {
+  extern __shared__ __align__(16) unsigned char res_smem[];
+  ResShared& s = *reinterpret_cast<ResShared*>(res_smem);
+  ClusterBarrier bar;
+  res_body(a, bar, s);
 }
 
 int max_cluster_size() {
@@ -514,6 +1042,77 @@ void launch_cg(const CgArgs& a, int grid, cudaStream_t st) {
   void* args[] = {(void*)&a};
   CUDA_CHECK(cudaLaunchCooperativeKernel((const void*)cg_kernel, dim3(grid),
                                          dim3(kCgThreads), args, smem, st));
+  SILK_LAUNCHED();
+}
+
+int cg_resident_grid(int res_blocks) {
+  static int max_coop = -1, max_cluster = 0;
+  const size_t smem = sizeof(ResShared);
+  if (max_coop < 0) {
+    max_coop = 0;
+    int dev = 0, sms = 0, per_sm = 0;
+    CUDA_CHECK(cudaGetDevice(&dev));
+    CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CUDA_CHECK(cudaFuncSetAttribute(cg_resident_kernel,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_CHECK(cudaFuncSetAttribute(cg_resident_cluster_kernel,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_resident_kernel, kResThreads,
+                                                      smem) != cudaSuccess) {
+      cudaGetLastError();
+      per_sm = 0;
+    }
+    max_coop = sms * per_sm;
+    if (cudaFuncSetAttribute(cg_resident_cluster_kernel,
+                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+      cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(16);
+    cfg.blockDim = dim3(kResThreads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = 16;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxPotentialClusterSize(&n, cg_resident_cluster_kernel, &cfg) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      n = 0;
+    }
+    max_cluster = n >= 16 ? 16 : (n >= 8 ? 8 : 0);
+  }
+  if (res_blocks <= 0 || max_coop == 0) return 0;
+  if (res_blocks > 1 && res_blocks <= max_cluster) return -res_blocks;
+  return res_blocks <= max_coop ? res_blocks : 0;
+}
+
+void launch_cg_resident(const CgArgs& a, int grid, cudaStream_t st) {
+  const size_t smem = sizeof(ResShared);
+  if (grid < 0) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(-grid);
+    cfg.blockDim = dim3(kResThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = -grid;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    CUDA_CHECK(cudaLaunchKernelEx(&cfg, cg_resident_cluster_kernel, a));
+    SILK_LAUNCHED();
+    return;
+  }
+  CUDA_CHECK(cudaMemsetAsync(a.barrier, 0, 2 * sizeof(unsigned), st));
+  void* args[] = {(void*)&a};
+  CUDA_CHECK(cudaLaunchCooperativeKernel((const void*)cg_resident_kernel, dim3(grid),
+                                         dim3(kResThreads), args, smem, st));
   SILK_LAUNCHED();
 }
 

@@ -66,7 +66,23 @@ struct CgArgs {
   int* result = nullptr;  // [iterations, status]
   int* stats = nullptr;   // accumulated [iterations, solves]
   float* result_rr = nullptr;
+  // Resident form: one block of kResThreads per first-level coarse bank (32
+  // fine banks), see cg_resident_kernel.  res_blocks == 0: not available.
+  int res_blocks = 0;
+  const int* rb_ptr = nullptr;  // per fine bank: first entry of its ELL slice
+  const int* rb_w = nullptr;    // per fine bank: slice width
+  const int2* rent = nullptr;   // (column, value bits); column < 0: slot -1-c of the block
+  int* fail = nullptr;          // set to 1 when a barrier wait gives up
+  // Optional phase trace of block 0 (null = off): [0] globaltimer and [1]
+  // clock64 at entry, [2] and [3] at exit, [4] traced iterations, [5] kernel
+  // form (0 streaming, 1 resident), then for each of the first kCgTraceIters
+  // iterations kCgTraceSlots clock64 stamps (unused slots repeat the last).
+  long long* trace = nullptr;
 };
+
+constexpr int kCgTraceIters = 64;
+constexpr int kCgTraceSlots = 16;
+constexpr int kCgTraceLen = 8 + kCgTraceIters * kCgTraceSlots;
 
 enum CgStatus {
   kCgAbsTol = 0,
@@ -76,6 +92,13 @@ enum CgStatus {
   kCgBarrierTimeout = 4
 };
 
+constexpr int kResThreads = 1024;     // one thread per fine-bank slot
+constexpr int kResCoarseBanks = 16;   // banks of the coarse levels held by every block
+// Resident launch form for a system with res_blocks blocks: 0 = not possible
+// on this device, > 0 = cooperative grid of that many blocks, < 0 = one
+// thread-block cluster of -value blocks.
+int cg_resident_grid(int res_blocks);
+
 void launch_galerkin_fill(const GalerkinDev& g, const double* src_vals,
                           const float* dyn, cudaStream_t st);
 // mode 0: fine level (fill from L, add dynamic diagonal via part offsets).
@@ -84,5 +107,6 @@ void launch_bank_invert(const MasLevelDev& lv, bool fine, const int* part_off,
                         cudaStream_t st);
 int cg_grid_size(int nslices, int nbank0);
 void launch_cg(const CgArgs& a, int grid, cudaStream_t st);
+void launch_cg_resident(const CgArgs& a, int grid, cudaStream_t st);
 
 }  // namespace silkb

@@ -316,7 +316,7 @@ __global__ void admm_finalize_kernel(AdmmFinalizeArgs a) {
          pa2 = sh[kPrimalScaleAux2][0];
   double d2 = sh[kDualNorm2][0], c2 = sh[kDualCur2][0], q2 = sh[kDualPrev2][0];
   c->iteration = a.iteration;
-  if (sh[kNonFinite][0] > 0.0) {
+  if (sh[kNonFinite][0] > 0.0 || (a.cg_fail && *a.cg_fail)) {
     c->diverged = 1;
     c->converged = 0;
     return;

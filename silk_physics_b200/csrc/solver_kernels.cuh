@@ -89,6 +89,7 @@ struct AdmmFinalizeArgs {
   float init_lin_rel, lin_rel_min, lin_rel_max, fixed_rel;
   int iteration;
   AdmmControl* ctl;
+  const int* cg_fail = nullptr;  // set when a CG barrier wait gave up
 };
 void launch_admm_finalize(const AdmmFinalizeArgs& a, cudaStream_t st);
 void launch_enforce(const SolverView& s, cudaStream_t st);

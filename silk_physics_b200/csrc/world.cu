@@ -351,6 +351,79 @@ SolverView World::view() {
 }
 
 // Per-cloth static device data: sliced-ELL off-diagonal L, MAS plans.
+// Resident CG layout (cg_resident_kernel): block k owns fine banks
+// 32k .. 32k+31 with thread 32 w + lane on slot `lane` of fine bank 32k + w.
+// Possible when every fine bank is one coarse node (parts are connected), so
+// that first-level coarse bank k is exactly this group, and the coarse levels
+// above fit the shared memory of a block.  The off-diagonal part of L is
+// re-sliced per fine bank; a column inside the block is stored as -1 - slot,
+// and the entries from other blocks come first in each row.
+void World::build_resident_layout(Cloth& c) {
+  const ClothSetup& S = *c.setup;
+  ClothDev& d = c.dev;
+  d.res_blocks = 0;
+  d.res_grid = 0;
+  const int nbank0 = S.fine.nbank;
+  const int nblocks = div_up(nbank0, BANK);
+  if (S.levels > 0) {
+    for (int b = 0; b < nbank0; ++b)
+      if (S.fine.bank_ncco[b] != 1 || S.fine.bank_cco_base[b] != b) return;
+    if (S.coarse[0].nbank != nblocks) return;
+    int upper = 0;
+    for (int l = 2; l <= S.levels; ++l) upper += S.coarse[l - 1].nbank;
+    if (upper > kResCoarseBanks) return;
+  }
+  int grid = cg_resident_grid(nblocks);
+  if (grid == 0) return;
+  const int nv = S.nv;
+  std::vector<int> part_of(nv), lane_of(nv);
+  for (int b = 0; b < nbank0; ++b)
+    for (int v = S.part_offsets[b]; v < S.part_offsets[b + 1]; ++v) {
+      part_of[v] = b;
+      lane_of[v] = v - S.part_offsets[b];
+    }
+  std::vector<int> ptr(nbank0 + 1, 0), width(nbank0, 0);
+  for (int b = 0; b < nbank0; ++b) {
+    int w = 0;
+    for (int v = S.part_offsets[b]; v < S.part_offsets[b + 1]; ++v)
+      w = std::max(w, S.Lrows[v + 1] - S.Lrows[v] - 1);
+    width[b] = w;
+    ptr[b + 1] = ptr[b] + BANK * w;
+  }
+  std::vector<int2> ent(std::max(ptr[nbank0], 1));
+  for (int b = 0; b < nbank0; ++b) {
+    const int k = b / BANK;
+    for (int lane = 0; lane < BANK; ++lane) {
+      const int own_slot = (b - k * BANK) * BANK + lane;
+      const int v = S.part_offsets[b] + lane;
+      std::vector<int2> far, near;
+      if (v < S.part_offsets[b + 1])
+        for (int q = S.Lrows[v]; q < S.Lrows[v + 1]; ++q) {
+          int col = S.Lcols[q];
+          if (col == v) continue;
+          float val = (float)S.Lvals[q];
+          int bits;
+          std::memcpy(&bits, &val, 4);
+          int cb = part_of[col];
+          if (cb / BANK == k)
+            near.push_back(make_int2(-1 - ((cb - k * BANK) * BANK + lane_of[col]), bits));
+          else
+            far.push_back(make_int2(col, bits));
+        }
+      int j = 0;
+      for (auto& e : far) ent[ptr[b] + BANK * j++ + lane] = e;
+      for (auto& e : near) ent[ptr[b] + BANK * j++ + lane] = e;
+      for (; j < width[b]; ++j) ent[ptr[b] + BANK * j + lane] = make_int2(-1 - own_slot, 0);
+    }
+  }
+  cudaStream_t st = stream;
+  d.rb_ptr.upload(ptr, st);
+  d.rb_w.upload(width, st);
+  d.rent.upload(ent, st);
+  d.res_blocks = nblocks;
+  d.res_grid = grid;
+}
+
 void World::build_cloth_device(Cloth& c) {
   const ClothSetup& S = *c.setup;
   ClothDev& d = c.dev;
@@ -395,6 +468,7 @@ void World::build_cloth_device(Cloth& c) {
   d.sl_ptr.upload(sl_ptr, st);
   d.sl_w.upload(sl_w, st);
   d.ent.upload(ent, st);
+  build_resident_layout(c);
   d.Ldiag.upload(ldiag, st);
   d.Lvals.upload(S.Lvals, st);
   d.part_off.upload(S.part_offsets, st);
@@ -451,7 +525,7 @@ void World::build_cloth_device(Cloth& c) {
   int nbank0 = S.fine.nbank;
   // Negative: one thread-block cluster of that many CTAs.
   d.cg_grid = cg_grid_size(nsl, nbank0);
-  d.partials.alloc(4 * (size_t)std::abs(d.cg_grid));
+  d.partials.alloc(4 * (size_t)std::max(std::abs(d.cg_grid), d.res_blocks));
   d.coarse_partial.alloc(1);
   d.barrier.alloc(4);
   d.barrier.zero(st);
@@ -509,6 +583,12 @@ void World::build_cloth_device(Cloth& c) {
     float4* rin = l == 1 ? d.fine.rout.p : d.coarse[l - 2].rout.p;
     a.coarse[l - 1] = lv_dev(S.coarse[l - 1], d.coarse[l - 1],
                              S.galerkin[l - 1].n, rin);
+  }
+  if (d.res_grid != 0) {
+    a.res_blocks = d.res_blocks;
+    a.rb_ptr = d.rb_ptr.p;
+    a.rb_w = d.rb_w.p;
+    a.rent = d.rent.p;
   }
   a.partials = d.partials.p;
   a.coarse_partial = d.coarse_partial.p;
@@ -614,6 +694,8 @@ void World::ensure_layout() {
   face_partials.alloc((size_t)face_step_blocks(nf) * kAdmmSlots);
   vertex_partials.alloc((size_t)vertex_step_blocks(nv) * kAdmmSlots);
   ctl.alloc(1);
+  cg_fail.alloc(1);
+  cg_fail.zero(st);
   pinned_dof = 0;
   for (auto& c : cloths) c->on_device = true;
   pins_dirty_ = true;
@@ -678,13 +760,26 @@ void World::cg_solve(Cloth& c, float rel_tol) {
   a.abs_tol = g.linear_solver_abs_tol;
   a.max_iter = opt.cg_max_iter > 0 ? opt.cg_max_iter : 1000;
   a.stats = c.dev.stats.p;
+  if (opt.profile >= 2) {
+    if (c.dev.cg_trace.n < (size_t)kCgTraceLen) c.dev.cg_trace.alloc(kCgTraceLen);
+    a.trace = c.dev.cg_trace.p;
+  }
+  a.fail = cg_fail.p;
+  const bool resident = c.dev.res_grid != 0 && opt.cg_form != 1;
+  if (resident) stats.cg_resident_solves += 1;
+  auto launch = [&]() {
+    if (resident)
+      launch_cg_resident(a, c.dev.res_grid, stream);
+    else
+      launch_cg(a, c.dev.cg_grid, stream);
+  };
   if (opt.profile) {
     auto* ev = next_event_pair(events, events_used);
     CUDA_CHECK(cudaEventRecord(ev->first, stream));
-    launch_cg(a, c.dev.cg_grid, stream);
+    launch();
     CUDA_CHECK(cudaEventRecord(ev->second, stream));
   } else {
-    launch_cg(a, c.dev.cg_grid, stream);
+    launch();
   }
 }
 
@@ -697,6 +792,19 @@ std::pair<cudaEvent_t, cudaEvent_t>* World::next_event_pair(
     pool.emplace_back(e0, e1);
   }
   return &pool[used++];
+}
+
+silk_status World::debug_cg_trace(uint32_t h, int64_t* out, int64_t cap, int32_t* n) {
+  Cloth* c = find_cloth(h);
+  if (!c) return SILK_ERR_INVALID_HANDLE;
+  *n = 0;
+  if (!c->dev.cg_trace.p) return SILK_OK;
+  if (cap < kCgTraceLen) return SILK_ERR_INVALID_CONFIG;
+  sync();
+  CUDA_CHECK(cudaMemcpy(out, c->dev.cg_trace.p, kCgTraceLen * sizeof(long long),
+                        cudaMemcpyDeviceToHost));
+  *n = kCgTraceLen;
+  return SILK_OK;
 }
 
 silk_status World::get_profile(silk_profile* p, bool reset) {
@@ -752,6 +860,7 @@ bool World::admm_solve() {
   fa.lin_rel_max = g.linear_solver_rel_tol_max;
   fa.fixed_rel = opt.fixed_linear_rel_tol;
   fa.ctl = ctl.p;
+  fa.cg_fail = cg_fail.p;
   bool contacts = coll_ && coll_->contact_count() > 0;
   for (int it = 0; it < g.max_inner_iteration; ++it) {
     if (it != 0) {
@@ -832,7 +941,10 @@ silk_status World::solver_step() {
                      outer.p, outer_v.p, x.p, st);
       auto t_admm = clk::now();
       if (!admm_solve()) {
-        last_error = "solver diverged";
+        int f = 0;
+        CUDA_CHECK(cudaMemcpy(&f, cg_fail.p, sizeof(int), cudaMemcpyDeviceToHost));
+        last_error = f ? "CG barrier wait gave up" : "solver diverged";
+        if (f) cg_fail.zero(st);
         return SILK_ERR_ITERATIVE_SOLVE_FAIL;
       }
       prof.admm_host_ms += ms_since(t_admm);

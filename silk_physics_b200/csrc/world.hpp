@@ -86,6 +86,11 @@ struct ClothDev {
   DevBuf<int> result;
   DevBuf<float> result_rr;
   DevBuf<int> stats;  // accumulated [iterations, solves] of this cloth
+  DevBuf<long long> cg_trace;  // phase trace of the last CG solve (profile >= 2)
+  DevBuf<int> rb_ptr, rb_w;   // resident form: ELL slices per fine bank
+  DevBuf<int2> rent;
+  int res_blocks = 0;         // resident form: blocks (0 = streaming form only)
+  int res_grid = 0;           // cg_resident_grid(res_blocks)
   CgArgs cg;
   int cg_grid = 1;
   double bytes_per_iter_fp32 = 0.0;  // algorithmic DRAM bytes per CG iteration
@@ -157,6 +162,7 @@ class World {
   silk_status set_solver_options(const silk_solver_options& o);
   silk_status set_stream(void* s);
   silk_status get_profile(silk_profile* p, bool reset);
+  silk_status debug_cg_trace(uint32_t h, int64_t* out, int64_t cap, int32_t* n);
   silk_status get_cloth_velocity(uint32_t h, float* out, int64_t n);
 
   // Inspection.
@@ -190,6 +196,7 @@ class World {
   DevBuf<int> vf_off, vf_list;
   DevBuf<double> face_partials, vertex_partials;
   DevBuf<AdmmControl> ctl;
+  DevBuf<int> cg_fail;  // set by a CG kernel whose barrier wait gave up
   int pinned_dof = 0;
   silk_profile prof{};
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events, events_other;
@@ -212,6 +219,7 @@ class World {
   void invalidate_layout();
   void ensure_layout();
   void build_cloth_device(Cloth& c);
+  void build_resident_layout(Cloth& c);
   void upload_pins();
   void factorize(Cloth& c);
   void cg_solve(Cloth& c, float rel_tol);

@@ -75,7 +75,8 @@ class _CollisionConfigC(C.Structure):
 
 class _SolverOptionsC(C.Structure):
     _fields_ = [("fixed_linear_rel_tol", C.c_float), ("cg_max_iter", C.c_int32),
-                ("mas_bf16", C.c_int32), ("profile", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("mas_bf16", C.c_int32), ("profile", C.c_int32), ("cg_form", C.c_int32),
+                ("reserved", C.c_int32 * 3)]
 
 
 class _ProfileC(C.Structure):
@@ -92,7 +93,8 @@ class _StepStatsC(C.Structure):
                 ("contacts", C.c_int32), ("colors", C.c_int32),
                 ("ccd_queries", C.c_int32), ("ccd_hits", C.c_int32),
                 ("min_toi", C.c_float), ("broadphase_candidates", C.c_int32),
-                ("kernel_launches", C.c_int64), ("reserved", C.c_int32 * 6)]
+                ("kernel_launches", C.c_int64), ("cg_resident_solves", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
 
 
 @dataclass
@@ -152,7 +154,8 @@ class SolverOptions:
     fixed_linear_rel_tol: float = 0.0
     cg_max_iter: int = 1000
     mas_bf16: bool = False
-    profile: bool = False
+    profile: int = 0  # 1: CUDA-event kernel timing; 2: also the CG phase trace
+    cg_form: int = 0  # 0: resident CG kernel where possible; 1: streaming form
 
     def to_c(self) -> _SolverOptionsC:
         o = _SolverOptionsC()
@@ -160,6 +163,7 @@ class SolverOptions:
         o.cg_max_iter = self.cg_max_iter
         o.mas_bf16 = int(self.mas_bf16)
         o.profile = int(self.profile)
+        o.cg_form = int(self.cg_form)
         return o
 
 
@@ -176,6 +180,7 @@ class StepStats:
     min_toi: float = 0.0
     broadphase_candidates: int = 0
     kernel_launches: int = 0
+    cg_resident_solves: int = 0
 
 
 _F32P = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -229,6 +234,8 @@ def _load() -> C.CDLL:
         "silk_debug_candidates": ([_W, _I32P, C.c_int64, C.POINTER(C.c_int32)], C.c_int),
         "silk_debug_dcd": ([_W, C.c_float, C.c_float, _I32P, C.c_int64,
                             C.POINTER(C.c_int32)], C.c_int),
+        "silk_debug_cg_trace": ([_W, C.c_uint32, C.c_void_p, C.c_int64, C.POINTER(C.c_int32)],
+                                C.c_int),
         "silk_debug_min_toi": ([_W, C.c_float, C.c_float, C.c_float, C.c_int32,
                                 C.POINTER(C.c_float), C.POINTER(C.c_int32),
                                 C.POINTER(C.c_int32)], C.c_int),
@@ -445,6 +452,27 @@ class World:
         if st:
             raise RuntimeError(_result(st, self._w).to_string())
         return toi.value, nq.value, nh.value
+
+    def debug_cg_trace(self, handle: int) -> dict | None:
+        """Phase trace of the last CG solve (solver option profile = 2):
+        kernel ns and cycles, the kernel form (0 streaming, 1 resident) and,
+        per traced iteration, the cycles between consecutive phase stamps
+        (16 slots; slot 0 is measured from the previous iteration's last)."""
+        buf = np.zeros(8 + 64 * 16, np.int64)
+        n = C.c_int32(0)
+        st = lib.silk_debug_cg_trace(self._w, handle, buf.ctypes.data, buf.size, C.byref(n))
+        if st:
+            raise RuntimeError(_result(st, self._w).to_string())
+        if n.value == 0:
+            return None
+        k = int(buf[4])
+        stamps = buf[8: 8 + 16 * k].reshape(k, 16)
+        phases = None
+        if k > 1:
+            prev = np.concatenate([[stamps[0, 0]], stamps[:-1, 15]])
+            phases = np.diff(np.concatenate([prev[:, None], stamps], axis=1), axis=1)[1:]
+        return {"ns": int(buf[2] - buf[0]), "cycles": int(buf[3] - buf[1]), "iters": k,
+                "form": int(buf[5]), "phase_cycles": phases}
 
 
 def ccd_batch(is_vertex_face: bool, x: np.ndarray, err3, min_separation,
