@@ -117,7 +117,7 @@ def peaks() -> dict:
 
 def traffic_per_launch():
     """DRAM bytes per CG launch from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / "cg_kernel_c2.md"
+    p = ROOT / "profiles" / "cg_resident_c2.md"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
@@ -261,7 +261,7 @@ def run_ours(args) -> None:
     cg_launch_ms = prof["cg_time_ms"] / max(prof["cg_launches"], 1)
     bytes_per_launch = prof["cg_algorithmic_bytes"] / max(prof["cg_launches"], 1)
     achieved = bytes_per_launch / (cg_launch_ms / 1e3) / 1e9 if cg_launch_ms > 0 else 0.0
-    roofline = {"bound": "hbm", "kernel": "cg_kernel (persistent MAS-PCG)",
+    roofline = {"bound": "hbm", "kernel": "cg_resident_cluster_kernel (persistent MAS-PCG)",
                 "achieved": round(achieved, 2), "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved / pk["hbm_gbs"], 5), "peak_source": pk["source"],
                 "traffic": traffic_per_launch(),
@@ -301,6 +301,40 @@ def run_ours(args) -> None:
     print(json.dumps(line), flush=True)
     if world_size > 1:
         torch.distributed.destroy_process_group()
+
+
+RESIDENT_PHASES = ["A: p update + publish", "barrier 1", "B: SpMV rows", "B: p.Ap block sum",
+                   "barrier 2", "C: pAp total", "C: fine MAS + restriction",
+                   "C: first coarse level", "C: r.z/r.r block sum", "barrier 3",
+                   "A: partial + coarse loads", "A: upper coarse levels", "A: rz sum"]
+STREAMING_PHASES = ["prolongation", "barrier 1", "SpMV", "barrier 2", "fine MAS", "barrier 3",
+                    "coarse levels", "barrier 4"]
+
+
+def run_trace(args) -> None:
+    """Median per-phase time of one CG iteration (block 0, clock64 stamps)."""
+    import torch
+
+    from silk_physics_b200 import native as N
+
+    V, F, SV, SF = scene()
+    stream = torch.cuda.Stream()
+    opts = N.SolverOptions(fixed_linear_rel_tol=args.cg_rel_tol, profile=1, mas_bf16=args.bf16)
+    w, h, _ = make_world(stream.cuda_stream, opts, V, F, SV, SF)
+    for _ in range(args.prelude + args.warmup):
+        assert w.solver_step()
+    opts.profile = 2
+    assert w.set_solver_options(opts)
+    assert w.solver_step()
+    t = w.debug_cg_trace(h)
+    ghz = t["cycles"] / max(t["ns"], 1)
+    names = RESIDENT_PHASES if t["form"] == 1 else STREAMING_PHASES
+    med = np.median(t["phase_cycles"], axis=0)[:len(names)] / ghz / 1e3
+    print(json.dumps({"cg_trace": {
+        "workload": WORKLOAD, "form": "resident" if t["form"] == 1 else "streaming",
+        "mas": "bf16" if args.bf16 else "fp32", "traced_iterations": t["iters"],
+        "sm_ghz": round(ghz, 3), "phase_us": {n: round(float(m), 2) for n, m in zip(names, med)},
+        "iteration_us": round(float(med.sum()), 2)}}), flush=True)
 
 
 def run_reference(args) -> None:
@@ -366,11 +400,16 @@ def main() -> None:
     ap.add_argument("--bf16", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cg-trace", action="store_true",
+                    help="print the CG phase breakdown of one step (after prelude and warm-up) "
+                         "instead of the bench line")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         run_reference(args)
+    elif args.cg_trace:
+        run_trace(args)
     else:
         run_ours(args)
 

@@ -89,7 +89,10 @@ typedef struct {
                                  2: also record the CG phase trace */
   int32_t cg_form;            /* 0: resident CG kernel where the system fits
                                  it, else streaming; 1: streaming always */
-  int32_t reserved[3];
+  int32_t learned_warm_start; /* 1: offer the loaded model's prediction as the
+                                 start of each outer iteration's first CG solve */
+  int32_t capture_samples;    /* 1: record warm-start training samples */
+  int32_t reserved[1];
 } silk_solver_options;
 
 /* CUDA-event timing of the persistent CG kernel over the steps since the
@@ -123,7 +126,10 @@ typedef struct {
   int32_t broadphase_candidates;
   int64_t kernel_launches;
   int32_t cg_resident_solves;  /* CG solves that ran in the resident form */
-  int32_t reserved[5];
+  int32_t cg_first_solve_iterations; /* iterations of each outer iteration's
+                                        first CG solve, summed */
+  int32_t learned_starts;      /* first solves that started from the model */
+  int32_t reserved[3];
 } silk_step_stats;
 
 /* --- World lifetime (silk.hpp:92-100) ---------------------------------- */
@@ -257,6 +263,44 @@ silk_status silk_ccd_batch(int32_t is_vertex_face, const float* x, int64_t n,
  * and 64-bit priorities: greedy colouring in decreasing priority order. */
 silk_status silk_color_contacts(const int32_t* verts4, const uint64_t* prio,
                                 int64_t n, int32_t* colors, int32_t* ncolors);
+
+/* --- Learned CG warm start (no counterpart in the reference) ------------ */
+/* Per-vertex MLP 13 -> 64 -> 64 -> 64 -> 3 (GELU, BF16 weights and layer
+ * inputs on the tensor cores, FP32 accumulation) that predicts the solution
+ * of the first CG solve of every outer iteration from the vertex's inertial
+ * offset, last two step displacements, 1-ring mean displacement and pin
+ * flag.  The prediction is only offered: the CG kernel starts from it when its
+ * residual is smaller than the plain start's, and always stops at
+ * rel_tol^2 x the plain start's residual norm.  Parameters are one FP32
+ * vector of SILK_MLP_PARAMS floats: W1 (16x64), b1, W2 (64x64), b2, W3, b3,
+ * W4 (64x8), b4 (8), feature mean (16), feature std (16), output scale (8);
+ * weights row-major (input, output). */
+#define SILK_MLP_PARAMS 9968
+/* Load a trained model into the world (NULL disables it); used when the
+ * solver option learned_warm_start is 1. */
+silk_status silk_set_warm_start_model(silk_world* w, const float* params, int64_t n);
+/* Training samples of the last step (solver option capture_samples = 1):
+ * per vertex 16 features (13 used) and 4 targets (3 used: first CG solution
+ * minus the inertial prediction, over the step scale dt^2 |g|), in the
+ * solver's vertex order; *valid = 0 when the last step recorded none. */
+silk_status silk_get_warm_start_samples(const silk_world* w, uint32_t handle,
+                                        float* features, float* targets,
+                                        int64_t nverts, int32_t* valid);
+/* Model outputs (n x 3, normalised units) of n feature rows (n x 16). */
+silk_status silk_mlp_forward(const float* params, const float* features, int64_t n,
+                             float* out);
+/* Mean squared error against targets (n x 4, 3 used, already divided by
+ * the step scale and the output scale) and its gradient (SILK_MLP_PARAMS
+ * floats, statistics entries zero). */
+silk_status silk_mlp_loss_grad(const float* params, const float* features,
+                               const float* targets, int64_t n, float* grad,
+                               double* loss);
+/* Adam training on the GPU: `steps` updates on batches of `batch` samples
+ * drawn with replacement (batch <= 0 or >= n: full batch); params updated in
+ * place; loss_history (steps floats, may be NULL) gets each step's loss. */
+silk_status silk_mlp_train(float* params, const float* features, const float* targets,
+                           int64_t n, int32_t steps, int32_t batch, float lr,
+                           uint64_t seed, float* loss_history);
 
 /* --- CCD batch that allocates nothing ----------------------------------- */
 /* No counterpart in the reference (its narrowphase, narrowphase.cu and

@@ -5,6 +5,7 @@
 
 #include "../../include/silk_b200.h"
 #include "collision.cuh"
+#include "learned.cuh"
 #include "world.hpp"
 
 using silkb::World;
@@ -345,6 +346,58 @@ silk_status silk_color_contacts(const int32_t* verts4, const uint64_t* prio,
   try {
     *ncolors = silkb::color_contacts_host(verts4, prio, n, colors);
     return *ncolors >= 0 ? SILK_OK : SILK_ERR_UNKNOWN;
+  } catch (...) {
+    return SILK_ERR_UNKNOWN;
+  }
+}
+
+static_assert(SILK_MLP_PARAMS == silkb::kMlpParams, "MLP parameter count");
+
+silk_status silk_set_warm_start_model(silk_world* w, const float* params, int64_t n) {
+  return guard_init(w, [&](World& W) { return W.set_warm_start_model(params, n); });
+}
+
+silk_status silk_get_warm_start_samples(const silk_world* w, uint32_t handle,
+                                        float* features, float* targets,
+                                        int64_t nverts, int32_t* valid) {
+  if (!features || !targets || !valid) return SILK_ERR_INVALID_CONFIG;
+  return guard_init(const_cast<silk_world*>(w), [&](World& W) {
+    return W.get_warm_start_samples(handle, features, targets, nverts, valid);
+  });
+}
+
+silk_status silk_mlp_forward(const float* params, const float* features, int64_t n,
+                             float* out) {
+  if (!params || n < 0 || (n > 0 && (!features || !out))) return SILK_ERR_INVALID_CONFIG;
+  if (n == 0) return SILK_OK;
+  try {
+    silkb::mlp_forward_host(params, features, n, out);
+    return SILK_OK;
+  } catch (...) {
+    return SILK_ERR_UNKNOWN;
+  }
+}
+
+silk_status silk_mlp_loss_grad(const float* params, const float* features,
+                               const float* targets, int64_t n, float* grad,
+                               double* loss) {
+  if (!params || n <= 0 || !features || !targets || !grad || !loss)
+    return SILK_ERR_INVALID_CONFIG;
+  try {
+    silkb::mlp_loss_grad_host(params, features, targets, n, grad, loss);
+    return SILK_OK;
+  } catch (...) {
+    return SILK_ERR_UNKNOWN;
+  }
+}
+
+silk_status silk_mlp_train(float* params, const float* features, const float* targets,
+                           int64_t n, int32_t steps, int32_t batch, float lr,
+                           uint64_t seed, float* loss_history) {
+  if (!params || n <= 0 || !features || !targets || steps < 0) return SILK_ERR_INVALID_CONFIG;
+  try {
+    silkb::mlp_train_host(params, features, targets, n, steps, batch, lr, seed, loss_history);
+    return SILK_OK;
   } catch (...) {
     return SILK_ERR_UNKNOWN;
   }

@@ -1,0 +1,547 @@
+// Learned CG warm start: feature extraction, the MLP forward on the tensor
+// cores (mma.sync m16n8k16, BF16 operands, FP32 accumulation; the whole MLP
+// of 16 samples stays in one warp's registers, each layer's accumulators
+// becoming the next layer's A fragments), the backward pass (FP32, straight
+// through the BF16 rounding) with deterministic per-block gradient partials,
+// and the Adam update.  No counterpart in the reference.
+#include <cuda_bf16.h>
+
+#include "learned.cuh"
+
+namespace silkb {
+
+namespace {
+
+constexpr int kFwdWarps = 4;
+constexpr int kFwdThreads = 32 * kFwdWarps;
+constexpr int kBwdThreads = 256;
+constexpr int kBwdTile = 32;  // samples per backward tile
+constexpr int kBwdBlocks = 296;
+
+__device__ __forceinline__ float gelu(float x) {
+  return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f));
+}
+__device__ __forceinline__ float gelu_grad(float x) {
+  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) +
+         x * expf(-0.5f * x * x) * 0.39894228040143268f;
+}
+__device__ __forceinline__ float bf16r(float x) {
+  return __bfloat162float(__float2bfloat16_rn(x));
+}
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(lo)) |
+         ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(hi)) << 16);
+}
+
+__device__ __forceinline__ void mma(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                    uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, "
+      "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Layer table: weight offset, K, N, first fragment tile.
+struct LayerDesc {
+  int w, k, n, tile;
+};
+__host__ __device__ constexpr LayerDesc layer(int l) {
+  return l == 0   ? LayerDesc{kOffW1, kMlpK, kMlpH, 0}
+         : l == 1 ? LayerDesc{kOffW2, kMlpH, kMlpH, kTilesL1}
+         : l == 2 ? LayerDesc{kOffW3, kMlpH, kMlpH, kTilesL1 + kTilesL2}
+                  : LayerDesc{kOffW4, kMlpH, kMlpKOut, kTilesL1 + kTilesL2 + kTilesL3};
+}
+
+// B fragment of tile (kt, nt) for lane (g, t): W[16kt + 2t (+1)][8nt + g] and
+// W[16kt + 2t + 8 (+9)][8nt + g], packed BF16 pairs.
+__global__ void mlp_prepare_kernel(const float* __restrict__ p, uint32_t* __restrict__ frag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kMlpTiles * 32) return;
+  int tile = i / 32, lane = i % 32;
+  int l = 0;
+  while (l < 3 && tile >= layer(l + 1).tile) ++l;
+  LayerDesc d = layer(l);
+  int local = tile - d.tile;
+  int ntiles_n = d.n / 8;
+  int kt = local / ntiles_n, nt = local % ntiles_n;
+  int g = lane >> 2, t = lane & 3;
+  const float* W = p + d.w;
+  int col = 8 * nt + g;
+  int r0 = 16 * kt + 2 * t;
+  frag[2 * i] = pack_bf16(W[r0 * d.n + col], W[(r0 + 1) * d.n + col]);
+  frag[2 * i + 1] = pack_bf16(W[(r0 + 8) * d.n + col], W[(r0 + 9) * d.n + col]);
+}
+
+struct SmemModel {
+  uint2 frag[kMlpTiles * 32];
+  float bias[3 * kMlpH + kMlpKOut];
+  float mean[kMlpK], inv_std[kMlpK], out_scale[kMlpKOut];
+};
+
+__device__ void load_model(const MlpDev& m, SmemModel& s) {
+  const uint2* src = reinterpret_cast<const uint2*>(m.frag);
+  for (int i = threadIdx.x; i < kMlpTiles * 32; i += blockDim.x) s.frag[i] = src[i];
+  for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
+    s.bias[i] = m.params[kOffB1 + i];
+    s.bias[kMlpH + i] = m.params[kOffB2 + i];
+    s.bias[2 * kMlpH + i] = m.params[kOffB3 + i];
+  }
+  for (int i = threadIdx.x; i < kMlpKOut; i += blockDim.x) {
+    s.bias[3 * kMlpH + i] = m.params[kOffB4 + i];
+    s.out_scale[i] = m.params[kOffOutScale + i];
+  }
+  for (int i = threadIdx.x; i < kMlpK; i += blockDim.x) {
+    s.mean[i] = m.params[kOffMean + i];
+    s.inv_std[i] = 1.0f / m.params[kOffStd + i];
+  }
+  __syncthreads();
+}
+
+// Forward of 16 samples (rows) by one warp.  Row g and g + 8 of the tile are
+// samples s0 + g and s0 + g + 8 (rows >= n are zero input).  Returns the output
+// accumulators c (rows g, g+8; columns 2t, 2t+1).  With z != null the hidden
+// pre-activations are stored (z[l][row][64], stride n).
+__device__ void forward_tile(const SmemModel& s, const float* __restrict__ feat,
+                             const int* __restrict__ index, int s0, int n, float* z,
+                             float (&out)[4]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int ra = s0 + g, rb = s0 + g + 8;
+  const int ia = ra < n ? (index ? index[ra] : ra) : -1;
+  const int ib = rb < n ? (index ? index[rb] : rb) : -1;
+  auto xn = [&](int src, int c) -> float {
+    if (src < 0) return 0.0f;
+    return (feat[(size_t)src * kMlpK + c] - s.mean[c]) * s.inv_std[c];
+  };
+  // Layer-1 A fragment (K = 16).
+  uint32_t a[4][4];
+  a[0][0] = pack_bf16(xn(ia, 2 * t), xn(ia, 2 * t + 1));
+  a[0][1] = pack_bf16(xn(ib, 2 * t), xn(ib, 2 * t + 1));
+  a[0][2] = pack_bf16(xn(ia, 2 * t + 8), xn(ia, 2 * t + 9));
+  a[0][3] = pack_bf16(xn(ib, 2 * t + 8), xn(ib, 2 * t + 9));
+  int kts = 1;
+  float c[8][4];
+#pragma unroll
+  for (int l = 0; l < 3; ++l) {
+    const LayerDesc d = layer(l);
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      float b0 = s.bias[l * kMlpH + 8 * nt + 2 * t], b1 = s.bias[l * kMlpH + 8 * nt + 2 * t + 1];
+      c[nt][0] = b0;
+      c[nt][1] = b1;
+      c[nt][2] = b0;
+      c[nt][3] = b1;
+    }
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt) {
+      if (kt >= kts) break;
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt) {
+        uint2 b = s.frag[(d.tile + kt * 8 + nt) * 32 + lane];
+        mma(c[nt], a[kt][0], a[kt][1], a[kt][2], a[kt][3], b.x, b.y);
+      }
+    }
+    if (z) {
+      float* zl = z + (size_t)l * n * kMlpH;
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt) {
+        int col = 8 * nt + 2 * t;
+        if (ra < n) *reinterpret_cast<float2*>(zl + (size_t)ra * kMlpH + col) = make_float2(c[nt][0], c[nt][1]);
+        if (rb < n) *reinterpret_cast<float2*>(zl + (size_t)rb * kMlpH + col) = make_float2(c[nt][2], c[nt][3]);
+      }
+    }
+    // GELU; the accumulators of output tiles 2kt and 2kt+1 are the A
+    // fragment of the next layer's k-tile kt.
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt) {
+      a[kt][0] = pack_bf16(gelu(c[2 * kt][0]), gelu(c[2 * kt][1]));
+      a[kt][1] = pack_bf16(gelu(c[2 * kt][2]), gelu(c[2 * kt][3]));
+      a[kt][2] = pack_bf16(gelu(c[2 * kt + 1][0]), gelu(c[2 * kt + 1][1]));
+      a[kt][3] = pack_bf16(gelu(c[2 * kt + 1][2]), gelu(c[2 * kt + 1][3]));
+    }
+    kts = 4;
+  }
+  const LayerDesc d = layer(3);
+  float b0 = s.bias[3 * kMlpH + 2 * t], b1 = s.bias[3 * kMlpH + 2 * t + 1];
+  out[0] = b0;
+  out[1] = b1;
+  out[2] = b0;
+  out[3] = b1;
+#pragma unroll
+  for (int kt = 0; kt < 4; ++kt) {
+    uint2 b = s.frag[(d.tile + kt) * 32 + lane];
+    mma(out, a[kt][0], a[kt][1], a[kt][2], a[kt][3], b.x, b.y);
+  }
+}
+
+__global__ void __launch_bounds__(kFwdThreads) mlp_forward_kernel(MlpDev m,
+                                                                  const float* __restrict__ feat,
+                                                                  int n, float* __restrict__ out) {
+  __shared__ SmemModel s;
+  load_model(m, s);
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int warp = blockIdx.x * kFwdWarps + (threadIdx.x >> 5);
+  const int nwarps = gridDim.x * kFwdWarps;
+  for (int s0 = 16 * warp; s0 < n; s0 += 16 * nwarps) {
+    float o[4];
+    forward_tile(s, feat, nullptr, s0, n, nullptr, o);
+    if (t < 2) {
+      const int ra = s0 + g, rb = s0 + g + 8;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        int col = 2 * t + q;
+        if (col >= kMlpOut) continue;
+        if (ra < n) out[(size_t)ra * kMlpOut + col] = o[q];
+        if (rb < n) out[(size_t)rb * kMlpOut + col] = o[2 + q];
+      }
+    }
+  }
+}
+
+// Training forward: pre-activations, the output gradient d4 = 2 (o - t) / (3n)
+// (n x 8, columns >= 3 zero) and per-block loss partials.
+__global__ void __launch_bounds__(kFwdThreads) mlp_train_forward_kernel(
+    MlpDev m, const float* __restrict__ feat, const float* __restrict__ t_hat,
+    const int* __restrict__ index, int n, float* __restrict__ z, float* __restrict__ d4,
+    double* __restrict__ loss_part) {
+  __shared__ SmemModel s;
+  __shared__ double red[kFwdWarps];
+  load_model(m, s);
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int warp = blockIdx.x * kFwdWarps + (threadIdx.x >> 5);
+  const int nwarps = gridDim.x * kFwdWarps;
+  const float scale = 2.0f / (3.0f * (float)n);
+  double loss = 0.0;
+  for (int s0 = 16 * warp; s0 < n; s0 += 16 * nwarps) {
+    float o[4];
+    forward_tile(s, feat, index, s0, n, z, o);
+    const int rows[2] = {s0 + g, s0 + g + 8};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = rows[h];
+      if (r >= n) continue;
+      const int src = index ? index[r] : r;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int col = 2 * t + q;
+        float dv = 0.0f;
+        if (col < kMlpOut) {
+          float e = o[2 * h + q] - t_hat[(size_t)src * 4 + col];
+          loss += (double)e * e;
+          dv = scale * e;
+        }
+        d4[(size_t)r * kMlpKOut + col] = dv;
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, off);
+  if (lane == 0) red[threadIdx.x >> 5] = loss;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int w = 0; w < kFwdWarps; ++w) a += red[w];
+    loss_part[blockIdx.x] = a;
+  }
+}
+
+struct BwdSmem {
+  float W[3][kMlpH][kMlpH + 1];  // BF16-rounded W2, W3 and (first 8 columns) W4
+  float A[kBwdTile][kMlpH + 1];  // layer input of the current layer (rounded)
+  float D[kBwdTile][kMlpH + 1];  // output gradient of the current layer
+  float E[kBwdTile][kMlpH + 1];  // gradient propagated to the layer input
+};
+
+// Backward over tiles of 32 samples: per-block partial gradients of every
+// trainable parameter (layout of the parameter vector), summed later in a
+// fixed order.
+__global__ void __launch_bounds__(kBwdThreads) mlp_backward_kernel(
+    MlpDev m, const float* __restrict__ feat, const int* __restrict__ index, int n,
+    const float* __restrict__ z, const float* __restrict__ d4, float* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char bwd_raw[];
+  BwdSmem& s = *reinterpret_cast<BwdSmem*>(bwd_raw);
+  const int tid = threadIdx.x;
+  for (int i = tid; i < kMlpH * kMlpH; i += kBwdThreads) {
+    int r = i / kMlpH, c = i % kMlpH;
+    s.W[0][r][c] = bf16r(m.params[kOffW2 + i]);
+    s.W[1][r][c] = bf16r(m.params[kOffW3 + i]);
+    s.W[2][r][c] = c < kMlpKOut ? bf16r(m.params[kOffW4 + r * kMlpKOut + c]) : 0.0f;
+  }
+  // Accumulators: dW4 (512), dW3 (4096), dW2 (4096), dW1 (1024), biases.
+  float gW4[2] = {0.f, 0.f}, gW3[16], gW2[16], gW1[4] = {0.f, 0.f, 0.f, 0.f};
+  float gb1 = 0.f, gb2 = 0.f, gb3 = 0.f, gb4 = 0.f;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) gW3[k] = gW2[k] = 0.f;
+  __syncthreads();
+  const int ntiles = (n + kBwdTile - 1) / kBwdTile;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int s0 = tile * kBwdTile;
+    // Output layer: D = d4, A = bf16(gelu(z3)).
+    for (int i = tid; i < kBwdTile * kMlpH; i += kBwdThreads) {
+      int r = i / kMlpH, c = i % kMlpH, sidx = s0 + r;
+      bool ok = sidx < n;
+      s.A[r][c] = ok ? bf16r(gelu(z[(size_t)2 * n * kMlpH + (size_t)sidx * kMlpH + c])) : 0.f;
+      s.D[r][c] = (ok && c < kMlpKOut) ? d4[(size_t)sidx * kMlpKOut + c] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      int e = tid + kBwdThreads * k, i = e / kMlpKOut, j = e % kMlpKOut;
+      float acc = 0.f;
+      for (int r = 0; r < kBwdTile; ++r) acc += s.A[r][i] * s.D[r][j];
+      gW4[k] += acc;
+    }
+    if (tid < kMlpKOut)
+      for (int r = 0; r < kBwdTile; ++r) gb4 += s.D[r][tid];
+    // Hidden layers 3, 2, 1 (l = 2, 1, 0): E = D W^T of the layer above,
+    // D_l = E * gelu'(z_l), A_l = layer input.
+    for (int l = 2; l >= 0; --l) {
+      const int wi = l;  // W[l] holds the weights of layer l + 1 (W2 for l = 0)
+      const int kout = (l == 2) ? kMlpKOut : kMlpH;
+      __syncthreads();
+      for (int i = tid; i < kBwdTile * kMlpH; i += kBwdThreads) {
+        int r = i / kMlpH, c = i % kMlpH;
+        float acc = 0.f;
+        for (int j = 0; j < kout; ++j) acc += s.D[r][j] * s.W[wi][c][j];
+        int sidx = s0 + r;
+        float zz = sidx < n ? z[(size_t)l * n * kMlpH + (size_t)sidx * kMlpH + c] : 0.f;
+        s.E[r][c] = sidx < n ? acc * gelu_grad(zz) : 0.f;
+      }
+      __syncthreads();
+      // Layer input of hidden layer l: bf16(gelu(z_{l-1})) or the normalised
+      // features for l = 0.
+      for (int i = tid; i < kBwdTile * kMlpH; i += kBwdThreads) {
+        int r = i / kMlpH, c = i % kMlpH, sidx = s0 + r;
+        float v = 0.f;
+        if (sidx < n) {
+          if (l > 0) {
+            v = bf16r(gelu(z[(size_t)(l - 1) * n * kMlpH + (size_t)sidx * kMlpH + c]));
+          } else if (c < kMlpK) {
+            int src = index ? index[sidx] : sidx;
+            v = bf16r((feat[(size_t)src * kMlpK + c] - m.params[kOffMean + c]) /
+                      m.params[kOffStd + c]);
+          }
+        }
+        s.A[r][c] = v;
+      }
+      __syncthreads();
+      if (l > 0) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          int e = tid + kBwdThreads * k, i = e / kMlpH, j = e % kMlpH;
+          float acc = 0.f;
+          for (int r = 0; r < kBwdTile; ++r) acc += s.A[r][i] * s.E[r][j];
+          if (l == 2) gW3[k] += acc; else gW2[k] += acc;
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          int e = tid + kBwdThreads * k, i = e / kMlpH, j = e % kMlpH;
+          float acc = 0.f;
+          for (int r = 0; r < kBwdTile; ++r) acc += s.A[r][i] * s.E[r][j];
+          gW1[k] += acc;
+        }
+      }
+      if (tid < kMlpH) {
+        float acc = 0.f;
+        for (int r = 0; r < kBwdTile; ++r) acc += s.E[r][tid];
+        if (l == 2) gb3 += acc; else if (l == 1) gb2 += acc; else gb1 += acc;
+      }
+      __syncthreads();
+      // The propagated gradient becomes the output gradient of the layer below.
+      for (int i = tid; i < kBwdTile * kMlpH; i += kBwdThreads) {
+        int r = i / kMlpH, c = i % kMlpH;
+        s.D[r][c] = s.E[r][c];
+      }
+    }
+    __syncthreads();
+  }
+  float* out = part + (size_t)blockIdx.x * kMlpTrainParams;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) out[kOffW4 + tid + kBwdThreads * k] = gW4[k];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    out[kOffW3 + tid + kBwdThreads * k] = gW3[k];
+    out[kOffW2 + tid + kBwdThreads * k] = gW2[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) out[kOffW1 + tid + kBwdThreads * k] = gW1[k];
+  if (tid < kMlpH) {
+    out[kOffB1 + tid] = gb1;
+    out[kOffB2 + tid] = gb2;
+    out[kOffB3 + tid] = gb3;
+  }
+  if (tid < kMlpKOut) out[kOffB4 + tid] = gb4;
+}
+
+__global__ void mlp_reduce_kernel(const float* __restrict__ part, int nblocks,
+                                  const double* __restrict__ loss_part, int nloss,
+                                  double inv_count, float* __restrict__ grad,
+                                  double* __restrict__ loss_out) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < kMlpParams) {
+    float acc = 0.f;
+    if (p < kMlpTrainParams)
+      for (int b = 0; b < nblocks; ++b) acc += part[(size_t)b * kMlpTrainParams + p];
+    grad[p] = acc;
+  }
+  if (p == 0) {
+    double a = 0.0;
+    for (int b = 0; b < nloss; ++b) a += loss_part[b];
+    *loss_out = a * inv_count;
+  }
+}
+
+__global__ void mlp_adam_kernel(float* __restrict__ p, const float* __restrict__ g,
+                                float* __restrict__ m, float* __restrict__ v, float lr,
+                                float c1, float c2) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kMlpTrainParams) return;
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  float gi = g[i];
+  float mi = b1 * m[i] + (1.0f - b1) * gi;
+  float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+}
+
+__global__ void warm_features_kernel(int n, const float4* __restrict__ x0,
+                                     const float4* __restrict__ x1,
+                                     const float4* __restrict__ x2,
+                                     const float4* __restrict__ y,
+                                     const uint8_t* __restrict__ pin,
+                                     const int* __restrict__ ring_off,
+                                     const int* __restrict__ ring, float inv_sigma,
+                                     float* __restrict__ feat) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  float4 a = x0[v], b = x1[v], c = x2[v], p = y[v];
+  float mx = 0.f, my = 0.f, mz = 0.f;
+  int beg = ring_off[v], end = ring_off[v + 1];
+  for (int q = beg; q < end; ++q) {
+    int u = ring[q];
+    float4 ua = x0[u], ub = x1[u];
+    mx += ua.x - ub.x;
+    my += ua.y - ub.y;
+    mz += ua.z - ub.z;
+  }
+  float inv_cnt = end > beg ? 1.0f / (float)(end - beg) : 0.0f;
+  float4* f = reinterpret_cast<float4*>(feat + (size_t)v * kMlpK);
+  f[0] = make_float4((p.x - a.x) * inv_sigma, (p.y - a.y) * inv_sigma, (p.z - a.z) * inv_sigma,
+                     (a.x - b.x) * inv_sigma);
+  f[1] = make_float4((a.y - b.y) * inv_sigma, (a.z - b.z) * inv_sigma, (b.x - c.x) * inv_sigma,
+                     (b.y - c.y) * inv_sigma);
+  f[2] = make_float4((b.z - c.z) * inv_sigma, mx * inv_cnt * inv_sigma, my * inv_cnt * inv_sigma,
+                     mz * inv_cnt * inv_sigma);
+  f[3] = make_float4(pin[v] ? 1.0f : 0.0f, 0.f, 0.f, 0.f);
+}
+
+__global__ void warm_combine_kernel(int n, const float* __restrict__ o,
+                                    const float* __restrict__ params,
+                                    const float4* __restrict__ y, float sigma,
+                                    float4* __restrict__ xp) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  float4 b = y[v];
+  xp[v] = make_float4(b.x + sigma * params[kOffOutScale] * o[3 * v],
+                      b.y + sigma * params[kOffOutScale + 1] * o[3 * v + 1],
+                      b.z + sigma * params[kOffOutScale + 2] * o[3 * v + 2], 0.f);
+}
+
+__global__ void warm_target_kernel(int n, const float4* __restrict__ x,
+                                   const float4* __restrict__ y, float inv_sigma,
+                                   float* __restrict__ t) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  float4 a = x[v], b = y[v];
+  reinterpret_cast<float4*>(t)[v] =
+      make_float4((a.x - b.x) * inv_sigma, (a.y - b.y) * inv_sigma, (a.z - b.z) * inv_sigma, 0.f);
+}
+
+int fwd_grid(int n) {
+  int tiles = (n + 15) / 16;
+  int blocks = (tiles + kFwdWarps - 1) / kFwdWarps;
+  return blocks < 1 ? 1 : (blocks > 1184 ? 1184 : blocks);
+}
+
+}  // namespace
+
+void mlp_prepare(const float* params, uint32_t* frag, cudaStream_t st) {
+  mlp_prepare_kernel<<<div_up(kMlpTiles * 32, 128), 128, 0, st>>>(params, frag);
+  SILK_LAUNCHED();
+}
+
+void mlp_forward(const MlpDev& m, const float* feat, int n, float* out, cudaStream_t st) {
+  if (n <= 0) return;
+  mlp_forward_kernel<<<fwd_grid(n), kFwdThreads, 0, st>>>(m, feat, n, out);
+  SILK_LAUNCHED();
+}
+
+size_t mlp_work_floats(int n) {
+  // z (3 x n x 64) + d4 (n x 8) + backward partials + loss partials (doubles).
+  return (size_t)3 * n * kMlpH + (size_t)n * kMlpKOut +
+         (size_t)kBwdBlocks * kMlpTrainParams + 2 * (size_t)fwd_grid(n) + 4;
+}
+
+void mlp_loss_grad(const MlpDev& m, const float* feat, const float* t_hat, int n,
+                   const int* index, float* work, float* grad, double* loss_out,
+                   cudaStream_t st) {
+  float* z = work;
+  float* d4 = z + (size_t)3 * n * kMlpH;
+  float* part = d4 + (size_t)n * kMlpKOut;
+  size_t off = (size_t)3 * n * kMlpH + (size_t)n * kMlpKOut + (size_t)kBwdBlocks * kMlpTrainParams;
+  off = (off + 1) & ~(size_t)1;  // 8-byte alignment for the doubles
+  double* loss_part = reinterpret_cast<double*>(work + off);
+  const int fg = fwd_grid(n);
+  mlp_train_forward_kernel<<<fg, kFwdThreads, 0, st>>>(m, feat, t_hat, index, n, z, d4,
+                                                      loss_part);
+  SILK_LAUNCHED();
+  static bool attr = false;
+  if (!attr) {
+    CUDA_CHECK(cudaFuncSetAttribute(mlp_backward_kernel,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(BwdSmem)));
+    attr = true;
+  }
+  mlp_backward_kernel<<<kBwdBlocks, kBwdThreads, sizeof(BwdSmem), st>>>(m, feat, index, n, z, d4,
+                                                                        part);
+  SILK_LAUNCHED();
+  mlp_reduce_kernel<<<div_up(kMlpParams, 128), 128, 0, st>>>(
+      part, kBwdBlocks, loss_part, fg, 1.0 / (3.0 * n), grad, loss_out);
+  SILK_LAUNCHED();
+}
+
+void mlp_adam(float* params, const float* grad, float* m, float* v, int step, float lr,
+              cudaStream_t st) {
+  float c1 = 1.0f / (1.0f - powf(0.9f, (float)step));
+  float c2 = 1.0f / (1.0f - powf(0.999f, (float)step));
+  mlp_adam_kernel<<<div_up(kMlpTrainParams, 256), 256, 0, st>>>(params, grad, m, v, lr, c1, c2);
+  SILK_LAUNCHED();
+}
+
+void warm_features(int n, const float4* x0, const float4* x1, const float4* x2,
+                   const float4* y, const uint8_t* pin, const int* ring_off,
+                   const int* ring, float inv_sigma, float* feat, cudaStream_t st) {
+  if (n <= 0) return;
+  warm_features_kernel<<<div_up(n, 256), 256, 0, st>>>(n, x0, x1, x2, y, pin, ring_off, ring,
+                                                       inv_sigma, feat);
+  SILK_LAUNCHED();
+}
+
+void warm_predict(const MlpDev& m, int n, const float* feat, const float4* y, float sigma,
+                  float* out_tmp, float4* x_pred, cudaStream_t st) {
+  if (n <= 0) return;
+  mlp_forward(m, feat, n, out_tmp, st);
+  warm_combine_kernel<<<div_up(n, 256), 256, 0, st>>>(n, out_tmp, m.params, y, sigma, x_pred);
+  SILK_LAUNCHED();
+}
+
+void warm_target(int n, const float4* x, const float4* y, float inv_sigma, float* t,
+                 cudaStream_t st) {
+  if (n <= 0) return;
+  warm_target_kernel<<<div_up(n, 256), 256, 0, st>>>(n, x, y, inv_sigma, t);
+  SILK_LAUNCHED();
+}
+
+}  // namespace silkb

@@ -378,6 +378,34 @@ __device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm
   // r = b - A x.
   spmv_phase(a, a.x, a.r, 1);
   if (!bar.sync()) return mark_fail(a);
+  // Alternative start (see CgArgs::x_alt): its residual goes to Ap.
+  double rr_judge = -1.0;
+  if (a.x_alt) {
+    spmv_phase(a, a.x_alt, a.Ap, 1);
+    if (!bar.sync()) return mark_fail(a);
+    {
+      double v[2] = {0.0, 0.0};
+      for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nv; i += gridDim.x * blockDim.x) {
+        float4 q = a.r[i], w = a.Ap[i];
+        v[0] += (double)q.x * q.x + (double)q.y * q.y + (double)q.z * q.z;
+        v[1] += (double)w.x * w.x + (double)w.y * w.y + (double)w.z * w.z;
+      }
+      block_sum<2>(v, part);
+    }
+    if (!bar.sync()) return mark_fail(a);
+    const double rr_plain = grid_total(a.partials, 0, gridDim.x);
+    const double rr_alt = grid_total(a.partials, 1, gridDim.x);
+    if (!bar.sync()) return mark_fail(a);
+    rr_judge = rr_plain;
+    if (rr_alt < rr_plain) {
+      for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nv; i += gridDim.x * blockDim.x) {
+        a.x[i] = a.x_alt[i];
+        a.r[i] = a.Ap[i];
+      }
+      if (blockIdx.x == 0 && threadIdx.x == 0 && a.stats) atomicAdd(a.stats + 3, 1);
+      if (!bar.sync()) return mark_fail(a);
+    }
+  }
   {
     double v[2] = {0.0, 0.0};
     fine_phase(a, 0.f, false, sm_all, v[0], v[1]);
@@ -399,7 +427,7 @@ __device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm
     }
     return;
   }
-  const double rr0 = rr;
+  const double rr0 = rr_judge >= 0.0 ? rr_judge : rr;
   const double abs2 = (double)a.abs_tol * a.abs_tol;
   const double rel2 = (double)a.rel_tol * a.rel_tol;
   double beta = 0.0;
@@ -460,6 +488,7 @@ __device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm
     if (a.stats) {
       atomicAdd(a.stats, iter);
       atomicAdd(a.stats + 1, 1);
+      if (a.first_solve) atomicAdd(a.stats + 2, iter);
     }
   }
 }
@@ -734,6 +763,41 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     float3 y = res_row(a, s, a.p, rptr, rw, lane, d, x);
     r = own ? make_float3(b.x - y.x, b.y - y.y, b.z - y.z) : make_float3(0.f, 0.f, 0.f);
   }
+  // Alternative start: residual of x_alt (published through the Ap buffer),
+  // both residual norms summed over the grid, the smaller start taken by
+  // every block alike; the plain start's norm stays the stopping reference.
+  double rr_judge = -1.0;
+  if (a.x_alt) {
+    float3 xa = make_float3(0.f, 0.f, 0.f);
+    if (own) {
+      float4 q = a.x_alt[v];
+      xa = make_float3(q.x, q.y, q.z);
+    }
+    __syncthreads();
+    s.pl[tid] = make_float4(xa.x, xa.y, xa.z, 0.f);
+    if (own) a.Ap[v] = make_float4(xa.x, xa.y, xa.z, 0.f);
+    if (!bar.sync()) return fail();
+    float3 ra;
+    {
+      float3 y = res_row(a, s, a.Ap, rptr, rw, lane, d, xa);
+      ra = own ? make_float3(b.x - y.x, b.y - y.y, b.z - y.z) : make_float3(0.f, 0.f, 0.f);
+    }
+    const double v2[2] = {(double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z,
+                          (double)ra.x * ra.x + (double)ra.y * ra.y + (double)ra.z * ra.z};
+    res_block_sum<2>(v2, s, part);
+    if (!bar.sync()) return fail();
+    const double rr_plain = res_total(a.partials, 0, nblocks, s);
+    const double rr_alt = res_total(a.partials, 1, nblocks, s);
+    // Every block reads the partials before any block overwrites them in the
+    // next phase.
+    if (!bar.sync()) return fail();
+    rr_judge = rr_plain;
+    if (rr_alt < rr_plain) {
+      x = xa;
+      r = ra;
+      if (k == 0 && tid == 0 && a.stats) atomicAdd(a.stats + 3, 1);
+    }
+  }
 
   // Phase C body: fine and first-level MAS of r, restriction to level 2,
   // partials (r.z, r.r) of this block.
@@ -864,7 +928,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     }
     return;
   }
-  const double rr0 = rr;
+  const double rr0 = rr_judge >= 0.0 ? rr_judge : rr;
   const double abs2 = (double)a.abs_tol * a.abs_tol;
   const double rel2 = (double)a.rel_tol * a.rel_tol;
   double beta = 0.0;
@@ -934,6 +998,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     if (a.stats) {
       atomicAdd(a.stats, iter);
       atomicAdd(a.stats + 1, 1);
+      if (a.first_solve) atomicAdd(a.stats + 2, iter);
     }
   }
 }

@@ -64,7 +64,13 @@ struct CgArgs {
   float rel_tol = 1e-3f, abs_tol = 1e-7f;
   int max_iter = 1000;
   int* result = nullptr;  // [iterations, status]
-  int* stats = nullptr;   // accumulated [iterations, solves]
+  int* stats = nullptr;   // accumulated [iterations, solves, first-solve iterations,
+                          // learned starts taken]
+  // Alternative start (learned warm start; null = none): taken when its
+  // residual is smaller than that of x, while the stopping rule keeps the
+  // residual of x as rr0 (the plain start judges the alternative).
+  const float4* x_alt = nullptr;
+  int first_solve = 0;    // count this solve's iterations in stats[2]
   float* result_rr = nullptr;
   // Resident form: one block of kResThreads per first-level coarse bank (32
   // fine banks), see cg_resident_kernel.  res_blocks == 0: not available.

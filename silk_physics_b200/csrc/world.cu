@@ -9,6 +9,7 @@
 
 #include "collision.cuh"
 #include "world.hpp"
+#include "learned.cuh"
 
 namespace silkb {
 
@@ -531,7 +532,7 @@ void World::build_cloth_device(Cloth& c) {
   d.barrier.zero(st);
   d.result.alloc(2);
   d.result_rr.alloc(1);
-  d.stats.alloc(2);
+  d.stats.alloc(4);
   d.stats.zero(st);
   // Compulsory DRAM bytes of one CG iteration: off-diagonal entries (8 B),
   // per row Ldiag + dynamic diagonal + p read + Ap write (40 B) in the SpMV
@@ -696,6 +697,33 @@ void World::ensure_layout() {
   ctl.alloc(1);
   cg_fail.alloc(1);
   cg_fail.zero(st);
+  // Learned warm start: 1-ring CSR over all cloths, step history (starting at
+  // the current positions, i.e. zero displacements), feature buffers.
+  {
+    std::vector<int> roff(1, 0), rl;
+    for (auto& c : cloths) {
+      const ClothSetup& S = *c->setup;
+      std::vector<std::vector<int>> nb(S.nv);
+      for (size_t e = 0; e + 1 < S.E.size(); e += 2) {
+        nb[S.E[e]].push_back(c->voff + S.E[e + 1]);
+        nb[S.E[e + 1]].push_back(c->voff + S.E[e]);
+      }
+      for (int i = 0; i < S.nv; ++i) {
+        rl.insert(rl.end(), nb[i].begin(), nb[i].end());
+        roff.push_back((int)rl.size());
+      }
+    }
+    if (rl.empty()) rl.push_back(0);
+    ring_off.upload(roff, st);
+    ring.upload(rl, st);
+  }
+  for (DevBuf<float4>* b : {&hist1, &hist2, &step_start, &ypred, &xpred}) b->alloc(nv);
+  up4(hist1, hx);
+  up4(hist2, hx);
+  warm_feat.alloc((size_t)kMlpK * nv);
+  warm_tgt.alloc((size_t)4 * nv);
+  mlp_out.alloc((size_t)kMlpOut * nv);
+  samples_valid = false;
   pinned_dof = 0;
   for (auto& c : cloths) c->on_device = true;
   pins_dirty_ = true;
@@ -750,8 +778,16 @@ void World::factorize(Cloth& c) {
                        nullptr, stream);
 }
 
-void World::cg_solve(Cloth& c, float rel_tol) {
+float World::warm_sigma() const {
+  float ax = g.acceleration_x, ay = g.acceleration_y, az = g.acceleration_z;
+  float s = g.dt * g.dt * std::sqrt(ax * ax + ay * ay + az * az);
+  return std::max(s, 1e-12f);
+}
+
+void World::cg_solve(Cloth& c, float rel_tol, bool first) {
   CgArgs a = c.dev.cg;
+  a.first_solve = first ? 1 : 0;
+  if (first && has_model && opt.learned_warm_start) a.x_alt = xpred.p + c.voff;
   a.dyn = lhs.p + c.voff;
   a.b = rhs.p + c.voff;
   a.x = x.p + c.voff;
@@ -804,6 +840,43 @@ silk_status World::debug_cg_trace(uint32_t h, int64_t* out, int64_t cap, int32_t
   CUDA_CHECK(cudaMemcpy(out, c->dev.cg_trace.p, kCgTraceLen * sizeof(long long),
                         cudaMemcpyDeviceToHost));
   *n = kCgTraceLen;
+  return SILK_OK;
+}
+
+silk_status World::set_warm_start_model(const float* params, int64_t n) {
+  if (!params) {
+    has_model = false;
+    return SILK_OK;
+  }
+  if (n != kMlpParams) return SILK_ERR_INVALID_CONFIG;
+  for (int i = kOffStd; i < kOffStd + kMlpK; ++i)
+    if (!(params[i] > 0.0f)) return SILK_ERR_INVALID_CONFIG;
+  for (int64_t i = 0; i < n; ++i)
+    if (!std::isfinite(params[i])) return SILK_ERR_INVALID_CONFIG;
+  ensure_stream();
+  mlp_params.alloc(kMlpParams);
+  mlp_frag.alloc(kMlpFragWords);
+  CUDA_CHECK(cudaMemcpyAsync(mlp_params.p, params, kMlpParams * sizeof(float),
+                             cudaMemcpyHostToDevice, stream));
+  mlp_prepare(mlp_params.p, mlp_frag.p, stream);
+  sync();
+  has_model = true;
+  return SILK_OK;
+}
+
+silk_status World::get_warm_start_samples(uint32_t h, float* feat, float* target, int64_t nv,
+                                          int* valid) {
+  Cloth* c = find_cloth(h);
+  if (!c) return SILK_ERR_INVALID_HANDLE;
+  if (nv != c->nv()) return SILK_ERR_INVALID_POSITION;
+  *valid = 0;
+  if (!samples_valid || !c->on_device) return SILK_OK;
+  sync();
+  CUDA_CHECK(cudaMemcpy(feat, warm_feat.p + (size_t)kMlpK * c->voff,
+                        (size_t)kMlpK * nv * sizeof(float), cudaMemcpyDeviceToHost));
+  CUDA_CHECK(cudaMemcpy(target, warm_tgt.p + (size_t)4 * c->voff, (size_t)4 * nv * sizeof(float),
+                        cudaMemcpyDeviceToHost));
+  *valid = 1;
   return SILK_OK;
 }
 
@@ -866,7 +939,11 @@ bool World::admm_solve() {
     if (it != 0) {
       for (auto& c : cloths) {
         if (it == 1) factorize(*c);
-        cg_solve(*c, rel);
+        cg_solve(*c, rel, it == 1);
+      }
+      if (it == 1 && opt.capture_samples && warm_first_) {
+        warm_target(nv_total, x.p, ypred.p, 1.0f / warm_sigma(), warm_tgt.p, st);
+        samples_valid = true;
       }
     }
     std::pair<cudaEvent_t, cudaEvent_t>* oe = opt.profile ? next_event_pair(events_other, events_other_used) : nullptr;
@@ -914,6 +991,8 @@ silk_status World::solver_step() {
     for (auto& c : cloths) c->dev.stats.zero(st);
     events_used = 0;
     events_other_used = 0;
+    CUDA_CHECK(cudaMemcpyAsync(step_start.p, sx.p, nv * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    if (opt.capture_samples) samples_valid = false;
     // init (main_loop.cu:24-76): damped velocity, fresh ADMM aux variables.
     launch_damp(nv, damp.p, sv.p, prev_v.p, st);
     zu.zero(st);
@@ -939,6 +1018,17 @@ silk_status World::solver_step() {
       stats.outer_iterations += 1;
       launch_predict(nv, g.dt, make_float4(g.acceleration_x, g.acceleration_y, g.acceleration_z, 0.f),
                      outer.p, outer_v.p, x.p, st);
+      warm_first_ = oit == 0;
+      if (warm_active()) {
+        const float sigma = warm_sigma();
+        CUDA_CHECK(cudaMemcpyAsync(ypred.p, x.p, nv * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+        warm_features(nv, outer.p, hist1.p, hist2.p, ypred.p, pin_flag.p, ring_off.p, ring.p,
+                      1.0f / sigma, warm_feat.p, st);
+        if (has_model && opt.learned_warm_start) {
+          MlpDev m{mlp_params.p, mlp_frag.p};
+          warm_predict(m, nv, warm_feat.p, ypred.p, sigma, mlp_out.p, xpred.p, st);
+        }
+      }
       auto t_admm = clk::now();
       if (!admm_solve()) {
         int f = 0;
@@ -976,19 +1066,24 @@ silk_status World::solver_step() {
     // Final velocity from the whole accepted displacement (main_loop.cu:248).
     launch_velocity(nv, g.dt, outer.p, sx.p, sv.p, st);
     CUDA_CHECK(cudaMemcpyAsync(sx.p, outer.p, nv * sizeof(float4), cudaMemcpyDeviceToDevice, st));
-    std::vector<int> cgs(2 * cloths.size());
+    // Step history of the warm-start features.
+    CUDA_CHECK(cudaMemcpyAsync(hist2.p, hist1.p, nv * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    CUDA_CHECK(cudaMemcpyAsync(hist1.p, step_start.p, nv * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    std::vector<int> cgs(4 * cloths.size());
     for (size_t k = 0; k < cloths.size(); ++k)
-      CUDA_CHECK(cudaMemcpyAsync(&cgs[2 * k], cloths[k]->dev.stats.p, 2 * sizeof(int),
+      CUDA_CHECK(cudaMemcpyAsync(&cgs[4 * k], cloths[k]->dev.stats.p, 4 * sizeof(int),
                                  cudaMemcpyDeviceToHost, st));
     sync();
     for (size_t k = 0; k < cloths.size(); ++k) {
-      stats.cg_iterations += cgs[2 * k];
-      stats.cg_solves += cgs[2 * k + 1];
+      stats.cg_iterations += cgs[4 * k];
+      stats.cg_solves += cgs[4 * k + 1];
+      stats.cg_first_solve_iterations += cgs[4 * k + 2];
+      stats.learned_starts += cgs[4 * k + 3];
       if (opt.profile) {
         double bpi = opt.mas_bf16 ? cloths[k]->dev.bytes_per_iter_bf16
                                   : cloths[k]->dev.bytes_per_iter_fp32;
-        prof.cg_algorithmic_bytes += bpi * (cgs[2 * k] + cgs[2 * k + 1]);
-        prof.cg_iterations += cgs[2 * k];
+        prof.cg_algorithmic_bytes += bpi * (cgs[4 * k] + cgs[4 * k + 1]);
+        prof.cg_iterations += cgs[4 * k];
       }
     }
     if (opt.profile) {

@@ -164,6 +164,9 @@ class World {
   silk_status get_profile(silk_profile* p, bool reset);
   silk_status debug_cg_trace(uint32_t h, int64_t* out, int64_t cap, int32_t* n);
   silk_status get_cloth_velocity(uint32_t h, float* out, int64_t n);
+  silk_status set_warm_start_model(const float* params, int64_t n);
+  silk_status get_warm_start_samples(uint32_t h, float* feat, float* target, int64_t nv,
+                                     int* valid);
 
   // Inspection.
   silk_status debug_partition(uint32_t h, int* perm, int64_t perm_len,
@@ -197,6 +200,14 @@ class World {
   DevBuf<double> face_partials, vertex_partials;
   DevBuf<AdmmControl> ctl;
   DevBuf<int> cg_fail;  // set by a CG kernel whose barrier wait gave up
+  // Learned warm start: model, step history, features and training samples.
+  DevBuf<float> mlp_params, mlp_out, warm_feat, warm_tgt;
+  DevBuf<uint32_t> mlp_frag;
+  DevBuf<float4> hist1, hist2, step_start, ypred, xpred;
+  DevBuf<int> ring_off, ring;
+  bool has_model = false;
+  bool samples_valid = false;
+  bool warm_first_ = false;  // the current outer iteration is the step's first
   int pinned_dof = 0;
   silk_profile prof{};
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events, events_other;
@@ -222,7 +233,9 @@ class World {
   void build_resident_layout(Cloth& c);
   void upload_pins();
   void factorize(Cloth& c);
-  void cg_solve(Cloth& c, float rel_tol);
+  void cg_solve(Cloth& c, float rel_tol, bool first);
+  bool warm_active() const { return (has_model && opt.learned_warm_start) || opt.capture_samples; }
+  float warm_sigma() const;
   bool admm_solve();  // false on divergence
   void sync();
 };

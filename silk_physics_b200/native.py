@@ -76,7 +76,8 @@ class _CollisionConfigC(C.Structure):
 class _SolverOptionsC(C.Structure):
     _fields_ = [("fixed_linear_rel_tol", C.c_float), ("cg_max_iter", C.c_int32),
                 ("mas_bf16", C.c_int32), ("profile", C.c_int32), ("cg_form", C.c_int32),
-                ("reserved", C.c_int32 * 3)]
+                ("learned_warm_start", C.c_int32), ("capture_samples", C.c_int32),
+                ("reserved", C.c_int32 * 1)]
 
 
 class _ProfileC(C.Structure):
@@ -94,7 +95,8 @@ class _StepStatsC(C.Structure):
                 ("ccd_queries", C.c_int32), ("ccd_hits", C.c_int32),
                 ("min_toi", C.c_float), ("broadphase_candidates", C.c_int32),
                 ("kernel_launches", C.c_int64), ("cg_resident_solves", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+                ("cg_first_solve_iterations", C.c_int32), ("learned_starts", C.c_int32),
+                ("reserved", C.c_int32 * 3)]
 
 
 @dataclass
@@ -156,6 +158,8 @@ class SolverOptions:
     mas_bf16: bool = False
     profile: int = 0  # 1: CUDA-event kernel timing; 2: also the CG phase trace
     cg_form: int = 0  # 0: resident CG kernel where possible; 1: streaming form
+    learned_warm_start: bool = False  # offer the loaded model's first-solve start
+    capture_samples: bool = False     # record warm-start training samples
 
     def to_c(self) -> _SolverOptionsC:
         o = _SolverOptionsC()
@@ -164,6 +168,8 @@ class SolverOptions:
         o.mas_bf16 = int(self.mas_bf16)
         o.profile = int(self.profile)
         o.cg_form = int(self.cg_form)
+        o.learned_warm_start = int(self.learned_warm_start)
+        o.capture_samples = int(self.capture_samples)
         return o
 
 
@@ -181,6 +187,8 @@ class StepStats:
     broadphase_candidates: int = 0
     kernel_launches: int = 0
     cg_resident_solves: int = 0
+    cg_first_solve_iterations: int = 0
+    learned_starts: int = 0
 
 
 _F32P = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -243,6 +251,14 @@ def _load() -> C.CDLL:
                             C.c_float, _I32P, _F32P, _F32P], C.c_int),
         "silk_color_contacts": ([_I32P, _U64P, C.c_int64, _I32P, C.POINTER(C.c_int32)],
                                 C.c_int),
+        "silk_set_warm_start_model": ([_W, C.c_void_p, C.c_int64], C.c_int),
+        "silk_get_warm_start_samples": ([_W, C.c_uint32, _F32P, _F32P, C.c_int64,
+                                         C.POINTER(C.c_int32)], C.c_int),
+        "silk_mlp_forward": ([_F32P, _F32P, C.c_int64, _F32P], C.c_int),
+        "silk_mlp_loss_grad": ([_F32P, _F32P, _F32P, C.c_int64, _F32P,
+                                C.POINTER(C.c_double)], C.c_int),
+        "silk_mlp_train": ([_F32P, _F32P, _F32P, C.c_int64, C.c_int32, C.c_int32, C.c_float,
+                            C.c_uint64, C.c_void_p], C.c_int),
         "silk_ccd_batch_noalloc": ([C.c_int32, C.c_void_p, C.c_int64, _F32P, C.c_void_p,
                                     C.c_float, C.c_int32, C.c_float, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)], C.c_int),
@@ -453,6 +469,23 @@ class World:
             raise RuntimeError(_result(st, self._w).to_string())
         return toi.value, nq.value, nh.value
 
+    def set_warm_start_model(self, params: np.ndarray | None) -> Result:
+        if params is None:
+            return _result(lib.silk_set_warm_start_model(self._w, None, 0), self._w)
+        p = _f32(params)
+        return _result(lib.silk_set_warm_start_model(self._w, p.ctypes.data, p.size), self._w)
+
+    def warm_start_samples(self, handle: int, nv: int):
+        """(features n x 16, targets n x 4) of the last step, or None."""
+        f = np.zeros((nv, 16), np.float32)
+        t = np.zeros((nv, 4), np.float32)
+        valid = C.c_int32(0)
+        st = lib.silk_get_warm_start_samples(self._w, handle, f.reshape(-1), t.reshape(-1), nv,
+                                             C.byref(valid))
+        if st:
+            raise RuntimeError(_result(st, self._w).to_string())
+        return (f, t) if valid.value else None
+
     def debug_cg_trace(self, handle: int) -> dict | None:
         """Phase trace of the last CG solve (solver option profile = 2):
         kernel ns and cycles, the kernel form (0 streaming, 1 resident) and,
@@ -489,6 +522,45 @@ def ccd_batch(is_vertex_face: bool, x: np.ndarray, err3, min_separation,
     if st:
         raise RuntimeError(_result(st).to_string())
     return hit.astype(bool), toi, tup
+
+
+MLP_PARAMS = 9968  # SILK_MLP_PARAMS
+
+
+def mlp_forward(params, features) -> np.ndarray:
+    """GPU (tensor-core) model outputs, n x 3, of feature rows n x 16."""
+    f = _f32(features).reshape(-1, 16)
+    out = np.zeros((len(f), 3), np.float32)
+    st = lib.silk_mlp_forward(_f32(params), f.reshape(-1), len(f), out.reshape(-1))
+    if st:
+        raise RuntimeError(_result(st).to_string())
+    return out
+
+
+def mlp_loss_grad(params, features, targets) -> tuple[float, np.ndarray]:
+    f = _f32(features).reshape(-1, 16)
+    t = _f32(targets).reshape(-1, 4)
+    grad = np.zeros(MLP_PARAMS, np.float32)
+    loss = C.c_double(0)
+    st = lib.silk_mlp_loss_grad(_f32(params), f.reshape(-1), t.reshape(-1), len(f), grad,
+                                C.byref(loss))
+    if st:
+        raise RuntimeError(_result(st).to_string())
+    return loss.value, grad
+
+
+def mlp_train(params, features, targets, steps: int, batch: int, lr: float,
+              seed: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """Adam on the GPU; returns (trained parameters, loss per step)."""
+    p = _f32(params).copy()
+    f = _f32(features).reshape(-1, 16)
+    t = _f32(targets).reshape(-1, 4)
+    hist = np.zeros(max(steps, 1), np.float32)
+    st = lib.silk_mlp_train(p, f.reshape(-1), t.reshape(-1), len(f), steps, batch, lr, seed,
+                            hist.ctypes.data)
+    if st:
+        raise RuntimeError(_result(st).to_string())
+    return p, hist[:steps]
 
 
 # Mirrors SILK_CCD_NOALLOC_MAX_QUERIES / SILK_CCD_NOALLOC_MAX_ITER.
