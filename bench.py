@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -48,6 +49,59 @@ def scene(seed=1236):
     V, F = S.grid_sheet(80, side=1.0, z=1.0, jitter=1e-4, seed=seed)
     SV, SF = S.icosphere(4, radius=0.3)
     return V, F, SV, SF
+
+
+C3_WORKLOAD = "c3_sheet316_on_icosphere_r0.6"
+MODEL = ROOT / "silk_physics_b200" / "models" / "warm_start.npy"
+
+
+def scene_c3(seed=1237):
+    from silk_physics_b200 import scenes as S
+
+    V, F = S.grid_sheet(316, side=2.0, z=0.7, jitter=1e-4, seed=seed)
+    SV, SF = S.icosphere(4, radius=0.6)
+    return V, F, SV, SF
+
+
+def timed_variant(N, torch, stream, flush, V, F, SV, SF, cg_rel_tol, bf16, learned,
+                  prelude, steps):
+    """Steps/s and CG statistics of one solver variant on one scene: `prelude`
+    untimed steps, then `steps` steps timed with CUDA events (L2 flushed
+    between steps)."""
+    opts = N.SolverOptions(fixed_linear_rel_tol=cg_rel_tol, profile=True, mas_bf16=bf16,
+                           learned_warm_start=learned)
+    w, h, _ = make_world(stream.cuda_stream, opts, V, F, SV, SF)
+    if learned:
+        from silk_physics_b200 import learned as L
+
+        r = w.set_warm_start_model(L.load(str(MODEL)))
+        assert r, r.to_string()
+    for _ in range(prelude):
+        r = w.solver_step()
+        assert r, r.to_string()
+    ms, admm, cg, solves, first, taken, outer = 0.0, 0, 0, 0, 0, 0, 0
+    for k in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 0xff)
+            a.record(stream)
+        r = w.solver_step()
+        b.record(stream)
+        b.synchronize()
+        assert r, r.to_string()
+        ms += a.elapsed_time(b)
+        st = w.step_stats()
+        admm += st.admm_iterations
+        cg += st.cg_iterations
+        solves += st.cg_solves
+        first += st.cg_first_solve_iterations
+        taken += st.learned_starts
+        outer += st.outer_iterations
+    return {"value": round(steps / (ms / 1e3), 4), "ms_per_step": round(ms / steps, 3),
+            "admm_iterations_per_step": admm / steps,
+            "cg_iterations_per_solve": round(cg / max(solves, 1), 2),
+            "first_solve_cg_iterations_per_outer": round(first / max(outer, 1), 2),
+            "learned_starts_taken": taken, "outer_iterations": outer}
 
 
 def dist_env():
@@ -237,21 +291,53 @@ def run_ours(args) -> None:
         torch.distributed.barrier()
     value = world_size * args.steps / (total_ms / 1e3)
 
-    # End to end through the public API with host buffers.
+    # Learned warm start + BF16 MAS on the same scene, and the 100K-vertex
+    # sheet (plain FP32 vs learned + BF16), each from its own fresh world.
+    variants = {}
+    if args.variants and MODEL.exists():
+        for name, bf16, learned in (("c2_bf16", True, False), ("c2_learned_bf16", True, True)):
+            variants[name] = timed_variant(N, torch, stream, flush, V, F, SV, SF,
+                                           args.cg_rel_tol, bf16, learned,
+                                           args.prelude + args.warmup, args.variant_steps)
+        V3, F3, SV3, SF3 = scene_c3()
+        c3 = {"workload": C3_WORKLOAD, "vertices": int(len(V3)), "faces": int(len(F3)),
+              "prelude_steps": args.c3_prelude, "steps": args.c3_steps}
+        for name, bf16, learned in (("plain_fp32", False, False), ("bf16", True, False),
+                                    ("learned_bf16", True, True)):
+            c3[name] = timed_variant(N, torch, stream, flush, V3, F3, SV3, SF3, args.cg_rel_tol,
+                                     bf16, learned, args.c3_prelude, args.c3_steps)
+        c3["learned_bf16_over_plain"] = round(c3["learned_bf16"]["value"] /
+                                              c3["plain_fp32"]["value"], 3)
+        variants["c3"] = c3
+
+    # End to end through the public API with host buffers, on the same steps:
+    # a fresh world replays the prelude and warm-up (the step is
+    # deterministic), then the first e2e_steps timed steps run with the
+    # obstacle position uploaded from pinned host memory and the cloth
+    # position read back to it inside the timed region.
+    we, he, hse = make_world(stream.cuda_stream, opts, V, F, SV, SF)
+    for _ in range(args.prelude + args.warmup):
+        r = we.solver_step()
+        assert r, r.to_string()
     pin_obs = torch.from_numpy(SV.ravel().copy()).pin_memory().numpy()
     pin_out = torch.empty(V.size, dtype=torch.float32).pin_memory().numpy()
     e2e_ms = []
-    for _ in range(args.e2e_steps):
+    n_e2e = min(args.e2e_steps, args.steps)
+    for k in range(n_e2e):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 0xff)
         a.record(stream)
-        w.set_obstacle_position(hs, pin_obs)
-        r = w.solver_step()
-        w.get_cloth_position(h, pin_out)
+        we.set_obstacle_position(hse, pin_obs)
+        r = we.solver_step()
+        we.get_cloth_position(he, pin_out)
         b.record(stream)
         b.synchronize()
         assert r, r.to_string()
         e2e_ms.append(a.elapsed_time(b))
-    e2e_val = args.e2e_steps / (sum(e2e_ms) / 1e3) * world_size
+    e2e_val = n_e2e / (sum(e2e_ms) / 1e3) * world_size
+    value_same_steps = n_e2e / (sum(step_ms[:n_e2e]) / 1e3) * world_size
+    del we
 
     if rank != 0:
         if world_size > 1:
@@ -294,9 +380,11 @@ def run_ours(args) -> None:
                    "parallelism": f"replicas x{world_size}"},
         "roofline": roofline, "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_val, 4), "unit": "steps/s",
-                "h2d_bytes_per_step": int(SV.nbytes), "d2h_bytes_per_step": int(V.nbytes)},
+                "h2d_bytes_per_step": int(SV.nbytes), "d2h_bytes_per_step": int(V.nbytes),
+                "steps": n_e2e, "device_value_same_steps": round(value_same_steps, 4)},
         "gpu_launches": int(launches),
         "clocks": clocks,
+        "variants": variants,
     }
     print(json.dumps(line), flush=True)
     if world_size > 1:
@@ -335,6 +423,94 @@ def run_trace(args) -> None:
         "mas": "bf16" if args.bf16 else "fp32", "traced_iterations": t["iters"],
         "sm_ghz": round(ghz, 3), "phase_us": {n: round(float(m), 2) for n, m in zip(names, med)},
         "iteration_us": round(float(med.sum()), 2)}}), flush=True)
+
+
+C5_WORKLOAD = "c5_batched_sheets_on_spheres"
+
+
+def scenes_c5(count, seed=2024):
+    """Independent scenes: sheet side counts log-uniform in [32, 200] (1 m
+    sheets), each just above an icosphere of radius U(0.2, 0.6) m at an
+    offset U([-0.3, 0.3]^2) m."""
+    from silk_physics_b200 import scenes as S
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        side = int(round(math.exp(rng.uniform(math.log(32), math.log(200)))))
+        r = float(rng.uniform(0.2, 0.6))
+        off = rng.uniform(-0.3, 0.3, 2)
+        V, F = S.grid_sheet(side, side=1.0, z=r + 0.05, jitter=1e-4,
+                            seed=int(rng.integers(1 << 30)), center=(0.0, 0.0))
+        SV, SF = S.icosphere(3, radius=r, center=(float(off[0]), float(off[1]), 0.0))
+        out.append((V, F, SV, SF))
+    return out
+
+
+def run_batched(args) -> None:
+    """Independent scenes stepped concurrently by silk_step_many (one CUDA
+    stream per world); the batch time of a step is the latest world end event
+    minus the first start event (CUDA events)."""
+    import torch
+
+    from silk_physics_b200 import native as N
+
+    scenes = scenes_c5(args.c5_scenes)
+    opts = N.SolverOptions(fixed_linear_rel_tol=args.cg_rel_tol, mas_bf16=args.bf16)
+
+    def build():
+        ws, sts = [], []
+        for V, F, SV, SF in scenes:
+            st = torch.cuda.Stream()
+            w, _, _ = make_world(st.cuda_stream, opts, V, F, SV, SF)
+            ws.append(w)
+            sts.append(st)
+        for _ in range(args.c5_prelude):
+            res = N.step_many(ws, 0)
+            assert all(res), [r.to_string() for r in res if not r]
+        return ws, sts
+
+    nverts = sum(len(V) for V, _, _, _ in scenes)
+
+    def timed(worlds, streams, steps, threads):
+        total = 0.0
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in worlds]
+            for (a, _), st in zip(ev, streams):
+                a.record(st)
+            res = N.step_many(worlds, threads)
+            for (_, b), st in zip(ev, streams):
+                b.record(st)
+            torch.cuda.synchronize()
+            assert all(res), [r.to_string() for r in res if not r]
+            total += max(ev[0][0].elapsed_time(b) for _, b in ev)
+        return total
+
+    # The same steps from the same state, concurrently and (on a second copy
+    # of the worlds) one world after another.
+    worlds, streams = build()
+    ms = timed(worlds, streams, args.c5_steps, 0)
+    seq_ms = None
+    if args.c5_sequential:
+        del worlds
+        worlds, streams = build()
+        seq_ms = timed(worlds, streams, args.c5_steps, 1)
+    line = {
+        "metric": "scene-steps/s (independent scenes stepped concurrently)",
+        "value": round(len(worlds) * args.c5_steps / (ms / 1e3), 4), "unit": "scene-steps/s",
+        "n_gpus": 1, "steps": args.c5_steps, "warmup": args.c5_prelude,
+        "contacts_last_step": int(sum(w.step_stats().contacts for w in worlds)),
+        "ms_per_step": round(ms / args.c5_steps, 3), "higher_is_better": True,
+        "dtype": "f32", "data": "synthetic (seeded sheets + icospheres)",
+        "config": {"workload": C5_WORKLOAD, "scenes": len(worlds), "vertices": nverts,
+                   "cg_rel_tol": args.cg_rel_tol, "mas": "bf16" if args.bf16 else "fp32",
+                   "host_threads": "one per hardware thread"},
+    }
+    if seq_ms is not None:
+        line["sequential_one_thread_ms_per_step"] = round(seq_ms / args.c5_steps, 3)
+    print(json.dumps(line), flush=True)
 
 
 def run_reference(args) -> None:
@@ -400,6 +576,18 @@ def main() -> None:
     ap.add_argument("--bf16", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variants", type=int, default=1,
+                    help="also time learned + BF16 MAS at 6.4K and plain vs learned + BF16 "
+                         "at 100K vertices (needs the trained model file)")
+    ap.add_argument("--variant-steps", type=int, default=5)
+    ap.add_argument("--c3-prelude", type=int, default=8)
+    ap.add_argument("--c3-steps", type=int, default=2)
+    ap.add_argument("--batched", action="store_true",
+                    help="time independent scenes stepped concurrently instead of the bench line")
+    ap.add_argument("--c5-scenes", type=int, default=64)
+    ap.add_argument("--c5-prelude", type=int, default=6)
+    ap.add_argument("--c5-steps", type=int, default=2)
+    ap.add_argument("--c5-sequential", type=int, default=1)
     ap.add_argument("--cg-trace", action="store_true",
                     help="print the CG phase breakdown of one step (after prelude and warm-up) "
                          "instead of the bench line")
@@ -410,6 +598,8 @@ def main() -> None:
         run_reference(args)
     elif args.cg_trace:
         run_trace(args)
+    elif args.batched:
+        run_batched(args)
     else:
         run_ours(args)
 

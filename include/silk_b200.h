@@ -92,7 +92,8 @@ typedef struct {
   int32_t learned_warm_start; /* 1: offer the loaded model's prediction as the
                                  start of each outer iteration's first CG solve */
   int32_t capture_samples;    /* 1: record warm-start training samples */
-  int32_t reserved[1];
+  int32_t contact_gs_form;    /* 0: single-block contact Gauss-Seidel where the
+                                 contacts fit it, else grid; 1: grid always */
 } silk_solver_options;
 
 /* CUDA-event timing of the persistent CG kernel over the steps since the
@@ -147,6 +148,14 @@ void silk_clear(silk_world* w);
 /* --- Solver API (silk.hpp:124-133) -------------------------------------- */
 silk_status silk_solver_step(silk_world* w);
 silk_status silk_solver_reset(silk_world* w);
+/* Batched step (no reference counterpart): advance n distinct, independent
+ * worlds by one step each, concurrently - each world on its own CUDA stream,
+ * driven by a pool of `threads` host threads (<= 0: one per hardware thread,
+ * at most n).  status[i] receives world i's result; the return value is the
+ * first non-OK status, or SILK_OK.  Worlds must not be used by other threads
+ * during the call. */
+silk_status silk_step_many(silk_world* const* worlds, int32_t n, int32_t threads,
+                           silk_status* status);
 
 /* --- Cloth API (silk.hpp:139-204) --------------------------------------- */
 silk_status silk_add_cloth(silk_world* w, const silk_cloth_config* cloth,

@@ -1,7 +1,10 @@
 // extern "C" boundary: every entry point of include/silk_b200.h.  Exceptions
 // never cross the ABI; they become SILK_ERR_UNKNOWN with a detail string.
+#include <atomic>
 #include <cstring>
 #include <exception>
+#include <thread>
+#include <vector>
 
 #include "../../include/silk_b200.h"
 #include "collision.cuh"
@@ -89,6 +92,40 @@ void silk_clear(silk_world* w) {
 
 silk_status silk_solver_step(silk_world* w) {
   return guard_init(w, [&](World& W) { return W.solver_step(); });
+}
+
+silk_status silk_step_many(silk_world* const* worlds, int32_t n, int32_t threads,
+                           silk_status* status) {
+  if (n < 0 || (n > 0 && (!worlds || !status))) return SILK_ERR_INVALID_CONFIG;
+  for (int32_t i = 0; i < n; ++i) {
+    if (!worlds[i]) return SILK_ERR_INVALID_CONFIG;
+    for (int32_t j = 0; j < i; ++j)
+      if (worlds[j] == worlds[i]) return SILK_ERR_INVALID_CONFIG;
+  }
+  int hw = (int)std::thread::hardware_concurrency();
+  int nt = threads > 0 ? threads : (hw > 0 ? hw : 1);
+  if (nt > n) nt = n;
+  std::atomic<int32_t> next{0};
+  auto work = [&]() {
+    for (;;) {
+      int32_t i = next.fetch_add(1);
+      if (i >= n) return;
+      silk_world* w = worlds[i];
+      if (w->impl.initialized) cudaSetDevice(w->impl.device);
+      status[i] = silk_solver_step(w);
+    }
+  };
+  std::vector<std::thread> pool;
+  try {
+    for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+  } catch (...) {
+    // Fewer threads than asked: the remaining ones (and this one) do the work.
+  }
+  work();
+  for (auto& t : pool) t.join();
+  for (int32_t i = 0; i < n; ++i)
+    if (status[i] != SILK_OK) return status[i];
+  return SILK_OK;
 }
 
 silk_status silk_solver_reset(silk_world* w) {

@@ -1137,64 +1137,116 @@ __global__ void contact_gs_kernel(const ContactDev* contacts, const int* groups,
     }
 }
 
-// Single-block form of contact_gs_kernel for contact sets whose largest
-// colour fits one block (at most one contact per thread and colour) and whose
-// cloth vertices fit in shared memory.  The positions stay in shared memory
-// for the whole solve, colour phases are separated by __syncthreads, and the
-// contact of the next colour is loaded while the current one is processed.
-// Each contact goes through the same operations in the same order as in
-// contact_gs_kernel (contacts of one colour touch disjoint vertices), so both
-// forms give identical results.
+// Single-block form of contact_gs_kernel.  The contacts are stored in colour
+// order with their cloth vertices renamed to compact slots (the vertices any
+// contact touches), so a colour phase reads contact q = group_off[c] + thread
+// directly and the positions of all touched vertices stay in shared memory for
+// the whole solve; colour phases are separated by __syncthreads and the next
+// phase's contact and correction are loaded while the current one is
+// processed.  The corrections are gathered into colour order at the start and
+// scattered back at the end.  Each contact goes through the same operations
+// in the same order as in contact_gs_kernel (contacts of one colour touch
+// disjoint vertices), so both forms give identical results.
 constexpr int kGsBlockThreads = 1024;
 constexpr size_t kGsBlockSmemMax = 200 * 1024;
+
+struct GsContact {
+  int slot[4];  // compact vertex slot, -1 kinematic
+  float coef[4];
+  float gamma[4];
+  float3 normal;
+  float friction;
+  float3 affine;
+  int ci;       // contact index (correction storage)
+};
+static_assert(sizeof(GsContact) == sizeof(ContactDev), "same record size");
+
+// Every cloth vertex a contact reads (v >= 0), movable or not: the pinned
+// ones (gamma = 0) still enter the contact's relative position u.
+__global__ void gs_flag_kernel(const ContactDev* __restrict__ c, int total,
+                               int* __restrict__ flag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  for (int s = 0; s < 4; ++s)
+    if (c[i].v[s] >= 0) flag[c[i].v[s]] = 1;
+}
+
+__global__ void gs_vlist_kernel(const int* __restrict__ flag, const int* __restrict__ slot, int nv,
+                                int* __restrict__ vlist) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < nv && flag[v]) vlist[slot[v]] = v;
+}
+
+__global__ void gs_gather_kernel(const ContactDev* __restrict__ c, const int* __restrict__ groups,
+                                 int total, const int* __restrict__ vslot,
+                                 GsContact* __restrict__ out) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= total) return;
+  int ci = groups[q];
+  const ContactDev& k = c[ci];
+  GsContact g;
+  for (int s = 0; s < 4; ++s) {
+    g.slot[s] = k.v[s] >= 0 ? vslot[k.v[s]] : -1;
+    g.coef[s] = k.coef[s];
+    g.gamma[s] = k.gamma[s];
+  }
+  g.normal = k.normal;
+  g.friction = k.friction;
+  g.affine = k.affine;
+  g.ci = ci;
+  out[q] = g;
+}
+
 __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
-    const ContactDev* __restrict__ contacts, const int* __restrict__ groups,
-    const int* __restrict__ group_off, int ncolors, float4* corr, float4* p, int nv) {
+    const GsContact* __restrict__ cc, const int* __restrict__ group_off, int ncolors, int total,
+    float4* __restrict__ corr, float4* __restrict__ ccorr, const int* __restrict__ vlist,
+    int nslots, float4* __restrict__ p) {
   extern __shared__ float4 sp[];
-  for (int v = threadIdx.x; v < nv; v += blockDim.x) sp[v] = p[v];
   const int t = threadIdx.x;
-  // A thread always takes the same contact of a colour, so the correction it
-  // prefetches was last written by itself.
-  auto fetch = [&](int col, int& ci, ContactDev& k, float4& o) {
-    int q = group_off[col] + t;
-    ci = q < group_off[col + 1] ? groups[q] : -1;
-    if (ci >= 0) {
-      k = contacts[ci];
-      o = corr[ci];
-    }
-  };
+  for (int i = t; i < nslots; i += blockDim.x) sp[i] = p[vlist[i]];
+  for (int q = t; q < total; q += blockDim.x) ccorr[q] = corr[cc[q].ci];
   __syncthreads();
   // Warm start with the saved corrections.
   for (int col = 0; col < ncolors; ++col) {
     int q = group_off[col] + t;
     if (q < group_off[col + 1]) {
-      int ci = groups[q];
-      const ContactDev& k = contacts[ci];
-      float4 r = corr[ci];
+      const GsContact& k = cc[q];
+      float4 r = ccorr[q];
       for (int s = 0; s < 4; ++s) {
         if (k.gamma[s] == 0.0f) continue;
-        float4 x = sp[k.v[s]];
+        float4 x = sp[k.slot[s]];
         float g = k.gamma[s];
-        sp[k.v[s]] = make_float4(x.x + g * r.x, x.y + g * r.y, x.z + g * r.z, 0.f);
+        sp[k.slot[s]] = make_float4(x.x + g * r.x, x.y + g * r.y, x.z + g * r.z, 0.f);
       }
     }
     __syncthreads();
   }
+  // A thread always takes the same contact of a colour, so the correction it
+  // prefetches was last written by itself.
+  auto fetch = [&](int col, int& q, GsContact& k, float4& o) {
+    q = group_off[col] + t;
+    if (q < group_off[col + 1]) {
+      k = cc[q];
+      o = ccorr[q];
+    } else {
+      q = -1;
+    }
+  };
   const int phases = kGsSweeps * ncolors;
-  int ci = -1;
-  ContactDev k;
+  int qn = -1;
+  GsContact k;
   float4 on = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (phases > 0) fetch(0, ci, k, on);
+  if (phases > 0) fetch(0, qn, k, on);
   for (int ph = 0; ph < phases; ++ph) {
-    const int cur = ci;
-    const ContactDev kc = k;
+    const int cur = qn;
+    const GsContact kc = k;
     const float4 o = on;
-    if (ph + 1 < phases) fetch((ph + 1) % ncolors, ci, k, on);
+    if (ph + 1 < phases) fetch((ph + 1) % ncolors, qn, k, on);
     if (cur >= 0) {
       float3 u = kc.affine;
       for (int s = 0; s < 4; ++s)
-        if (kc.v[s] >= 0) {
-          float4 x = sp[kc.v[s]];
+        if (kc.slot[s] >= 0) {
+          float4 x = sp[kc.slot[s]];
           u = add3(u, sc3(kc.coef[s], make_float3(x.x, x.y, x.z)));
         }
       float3 old = make_float3(o.x, o.y, o.z);
@@ -1211,18 +1263,19 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
       }
       float3 du = sub3(unew, u);
       float3 nc = add3(old, du);
-      corr[cur] = make_float4(nc.x, nc.y, nc.z, 0.f);
-      if (ci == cur) on = make_float4(nc.x, nc.y, nc.z, 0.f);  // one colour
+      ccorr[cur] = make_float4(nc.x, nc.y, nc.z, 0.f);
+      if (qn == cur) on = make_float4(nc.x, nc.y, nc.z, 0.f);  // one colour
       for (int s = 0; s < 4; ++s) {
         if (kc.gamma[s] == 0.0f) continue;
-        float4 x = sp[kc.v[s]];
+        float4 x = sp[kc.slot[s]];
         float g = kc.gamma[s];
-        sp[kc.v[s]] = make_float4(x.x + g * du.x, x.y + g * du.y, x.z + g * du.z, 0.f);
+        sp[kc.slot[s]] = make_float4(x.x + g * du.x, x.y + g * du.y, x.z + g * du.z, 0.f);
       }
     }
     __syncthreads();
   }
-  for (int v = threadIdx.x; v < nv; v += blockDim.x) p[v] = sp[v];
+  for (int q = t; q < total; q += blockDim.x) corr[cc[q].ci] = ccorr[q];
+  for (int i = t; i < nslots; i += blockDim.x) p[vlist[i]] = sp[i];
 }
 
 // Canonical contact key (contact_constraints.cu:24-47).
@@ -1322,6 +1375,13 @@ struct CollisionImpl {
   DevBuf<unsigned long long> prio;
   DevBuf<float4> corr;
   DevBuf<int> inc_count, inc_off, inc_cursor, inc_list, colors, groups, group_off;
+  // Single-block Gauss-Seidel: compact slots of the touched vertices and the
+  // contacts in colour order on those slots.
+  DevBuf<int> gs_flag, gs_slot, gs_vlist;
+  DevBuf<GsContact> gs_cc;
+  DevBuf<float4> gs_ccorr;
+  int gs_nslots = 0;
+  bool gs_ready = false;
   DevBuf<int> active_dof;
   DevBuf<int> jp_flags;
   DevBuf<unsigned> gs_barrier;
@@ -1846,6 +1906,38 @@ int CollisionSystem::append_active(float time, float dact) {
   I.groups.upload(grp, st);
   I.group_off.upload(goff, st);
   I.n_colors = nc;
+  // Colour-ordered contacts on compact vertex slots for the single-block
+  // Gauss-Seidel form.
+  {
+    I.gs_flag.alloc(nv);
+    I.gs_slot.alloc(nv);
+    I.gs_flag.zero(st);
+    gs_flag_kernel<<<div_up(total, kCollThreads), kCollThreads, 0, st>>>(I.contacts.p, total,
+                                                                        I.gs_flag.p);
+    SILK_LAUNCHED();
+    size_t tb2 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb2, I.gs_flag.p, I.gs_slot.p, nv, st);
+    if (I.scan_temp.n < tb2) I.scan_temp.alloc(tb2);
+    CUDA_CHECK(cub::DeviceScan::ExclusiveSum(I.scan_temp.p, tb2, I.gs_flag.p, I.gs_slot.p, nv,
+                                             st));
+    SILK_LAUNCHED();
+    int last[2] = {0, 0};
+    CUDA_CHECK(cudaMemcpyAsync(&last[0], I.gs_slot.p + nv - 1, sizeof(int),
+                               cudaMemcpyDeviceToHost, st));
+    CUDA_CHECK(cudaMemcpyAsync(&last[1], I.gs_flag.p + nv - 1, sizeof(int),
+                               cudaMemcpyDeviceToHost, st));
+    CUDA_CHECK(cudaStreamSynchronize(st));
+    I.gs_nslots = last[0] + last[1];
+    I.gs_vlist.alloc(std::max(I.gs_nslots, 1));
+    gs_vlist_kernel<<<div_up(nv, 256), 256, 0, st>>>(I.gs_flag.p, I.gs_slot.p, nv, I.gs_vlist.p);
+    SILK_LAUNCHED();
+    I.gs_cc.alloc(total);
+    I.gs_ccorr.alloc(total);
+    gs_gather_kernel<<<div_up(total, kCollThreads), kCollThreads, 0, st>>>(
+        I.contacts.p, I.groups.p, total, I.gs_slot.p, I.gs_cc.p);
+    SILK_LAUNCHED();
+    I.gs_ready = true;
+  }
   CUDA_CHECK(cudaStreamSynchronize(st));
   return add;
 }
@@ -1854,29 +1946,29 @@ void CollisionSystem::contact_solve() {
   CollisionImpl& I = *impl_;
   if (I.n_contacts == 0) return;
   cudaStream_t st = w_.stream;
-  const int nv = (int)w_.contact_p.n;
-  const size_t smem = (size_t)nv * sizeof(float4);
-  if (I.max_group <= kGsBlockThreads && smem <= kGsBlockSmemMax) {
-    static bool attr = false;
-    if (!attr) {
+  const size_t smem = (size_t)I.gs_nslots * sizeof(float4);
+  if (I.gs_ready && w_.opt.contact_gs_form != 1 && I.max_group <= kGsBlockThreads &&
+      smem <= kGsBlockSmemMax) {
+    static const bool attr = [] {
       CUDA_CHECK(cudaFuncSetAttribute(contact_gs_block_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kGsBlockSmemMax));
-      attr = true;
-    }
+      return true;
+    }();
+    (void)attr;
     contact_gs_block_kernel<<<1, kGsBlockThreads, smem, st>>>(
-        I.contacts.p, I.groups.p, I.group_off.p, I.n_colors, I.corr.p, w_.contact_p.p, nv);
+        I.gs_cc.p, I.group_off.p, I.n_colors, I.n_contacts, I.corr.p, I.gs_ccorr.p,
+        I.gs_vlist.p, I.gs_nslots, w_.contact_p.p);
     SILK_LAUNCHED();
     return;
   }
-  static int max_coop = 0;
-  if (max_coop == 0) {
+  static const int max_coop = [] {
     int dev = 0, sms = 0, per = 0;
     CUDA_CHECK(cudaGetDevice(&dev));
     CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, contact_gs_kernel, 256, 0));
-    max_coop = sms * std::max(per, 1);
-  }
+    return sms * std::max(per, 1);
+  }();
   int grid = std::min(max_coop, std::max(1, div_up(I.max_group, 256)));
   CUDA_CHECK(cudaMemsetAsync(I.gs_barrier.p, 0, 2 * sizeof(unsigned), st));
   const ContactDev* c = I.contacts.p;
@@ -1924,12 +2016,12 @@ float CollisionSystem::min_toi(float ts, float max_time, float ms, int* nq, int*
   const int max_chunks = 64;
   CUDA_CHECK(cudaMemsetAsync(I.ccd_counts.p, 0, (4 + max_chunks) * sizeof(int), st));
   if ((int)I.ccd_overflow.n < n) I.ccd_overflow.alloc(n + n / 4);
-  static int sms = 0;
-  if (sms == 0) {
-    int dev = 0;
+  static const int sms = [] {
+    int dev = 0, n = 0;
     CUDA_CHECK(cudaGetDevice(&dev));
-    CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  }
+    CUDA_CHECK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    return n;
+  }();
   auto grid_for = [&](int m) { return std::max(1, std::min(div_up(m, kCollThreads), 8 * sms)); };
   CcdSpill first{nullptr, 0, nullptr, I.ccd_overflow.p, I.ccd_counts.p + 2};
   ccd_kernel<<<grid_for(n), kCollThreads, 0, st>>>(

@@ -497,13 +497,13 @@ void mlp_loss_grad(const MlpDev& m, const float* feat, const float* t_hat, int n
   mlp_train_forward_kernel<<<fg, kFwdThreads, 0, st>>>(m, feat, t_hat, index, n, z, d4,
                                                       loss_part);
   SILK_LAUNCHED();
-  static bool attr = false;
-  if (!attr) {
+  static const bool attr = [] {
     CUDA_CHECK(cudaFuncSetAttribute(mlp_backward_kernel,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)sizeof(BwdSmem)));
-    attr = true;
-  }
+    return true;
+  }();
+  (void)attr;
   mlp_backward_kernel<<<kBwdBlocks, kBwdThreads, sizeof(BwdSmem), st>>>(m, feat, index, n, z, d4,
                                                                         part);
   SILK_LAUNCHED();

@@ -367,6 +367,19 @@ struct CgTrace {
   }
 };
 
+// Weight w of the start x + w (x_alt - x) whose residual r + w (r_alt - r)
+// has the smallest norm: w = <r, r - r_alt> / |r - r_alt|^2.  Used only when
+// it lowers |r|^2 by at least 1 % (otherwise w = 0, the plain start), so the
+// blend never raises the residual; w = 1 is the alternative start itself.
+__device__ __forceinline__ double blend_weight(double rr, double r_ra, double rara) {
+  double den = rr - 2.0 * r_ra + rara;
+  if (!(den > 0.0) || !(rr > 0.0)) return 0.0;
+  double num = rr - r_ra;
+  if (num <= 0.0 || num * num < 1e-2 * den * rr) return 0.0;
+  double w = num / den;
+  return isfinite(w) ? w : 0.0;
+}
+
 __device__ __forceinline__ void mark_fail(const CgArgs& a) {
   if (threadIdx.x == 0 && a.fail) atomicExch(a.fail, 1);
 }
@@ -384,23 +397,29 @@ __device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm
     spmv_phase(a, a.x_alt, a.Ap, 1);
     if (!bar.sync()) return mark_fail(a);
     {
-      double v[2] = {0.0, 0.0};
+      double v[3] = {0.0, 0.0, 0.0};
       for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nv; i += gridDim.x * blockDim.x) {
         float4 q = a.r[i], w = a.Ap[i];
         v[0] += (double)q.x * q.x + (double)q.y * q.y + (double)q.z * q.z;
-        v[1] += (double)w.x * w.x + (double)w.y * w.y + (double)w.z * w.z;
+        v[1] += (double)q.x * w.x + (double)q.y * w.y + (double)q.z * w.z;
+        v[2] += (double)w.x * w.x + (double)w.y * w.y + (double)w.z * w.z;
       }
-      block_sum<2>(v, part);
+      block_sum<3>(v, part);
     }
     if (!bar.sync()) return mark_fail(a);
     const double rr_plain = grid_total(a.partials, 0, gridDim.x);
-    const double rr_alt = grid_total(a.partials, 1, gridDim.x);
+    const double r_pa = grid_total(a.partials, 1, gridDim.x);
+    const double rr_alt = grid_total(a.partials, 2, gridDim.x);
     if (!bar.sync()) return mark_fail(a);
     rr_judge = rr_plain;
-    if (rr_alt < rr_plain) {
+    const float w = (float)blend_weight(rr_plain, r_pa, rr_alt);
+    if (w > 0.0f) {
       for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nv; i += gridDim.x * blockDim.x) {
-        a.x[i] = a.x_alt[i];
-        a.r[i] = a.Ap[i];
+        float4 x0 = a.x[i], xa = a.x_alt[i], r0 = a.r[i], ra = a.Ap[i];
+        a.x[i] = make_float4(x0.x + w * (xa.x - x0.x), x0.y + w * (xa.y - x0.y),
+                             x0.z + w * (xa.z - x0.z), 0.f);
+        a.r[i] = make_float4(r0.x + w * (ra.x - r0.x), r0.y + w * (ra.y - r0.y),
+                             r0.z + w * (ra.z - r0.z), 0.f);
       }
       if (blockIdx.x == 0 && threadIdx.x == 0 && a.stats) atomicAdd(a.stats + 3, 1);
       if (!bar.sync()) return mark_fail(a);
@@ -782,19 +801,22 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
       float3 y = res_row(a, s, a.Ap, rptr, rw, lane, d, xa);
       ra = own ? make_float3(b.x - y.x, b.y - y.y, b.z - y.z) : make_float3(0.f, 0.f, 0.f);
     }
-    const double v2[2] = {(double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z,
+    const double v3[3] = {(double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z,
+                          (double)r.x * ra.x + (double)r.y * ra.y + (double)r.z * ra.z,
                           (double)ra.x * ra.x + (double)ra.y * ra.y + (double)ra.z * ra.z};
-    res_block_sum<2>(v2, s, part);
+    res_block_sum<3>(v3, s, part);
     if (!bar.sync()) return fail();
     const double rr_plain = res_total(a.partials, 0, nblocks, s);
-    const double rr_alt = res_total(a.partials, 1, nblocks, s);
+    const double r_pa = res_total(a.partials, 1, nblocks, s);
+    const double rr_alt = res_total(a.partials, 2, nblocks, s);
     // Every block reads the partials before any block overwrites them in the
     // next phase.
     if (!bar.sync()) return fail();
     rr_judge = rr_plain;
-    if (rr_alt < rr_plain) {
-      x = xa;
-      r = ra;
+    const float w = (float)blend_weight(rr_plain, r_pa, rr_alt);
+    if (w > 0.0f) {
+      x = make_float3(x.x + w * (xa.x - x.x), x.y + w * (xa.y - x.y), x.z + w * (xa.z - x.z));
+      r = make_float3(r.x + w * (ra.x - r.x), r.y + w * (ra.y - r.y), r.z + w * (ra.z - r.z));
       if (k == 0 && tid == 0 && a.stats) atomicAdd(a.stats + 3, 1);
     }
   }
@@ -1018,8 +1040,7 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_resident_cluster_kernel(CgA
 }
 
 int max_cluster_size() {
-  static int size = -1;
-  if (size < 0) {
+  static const int size = [] {
     size_t smem = kCgWarps * kPacked * sizeof(float);
     if (cudaFuncSetAttribute(cg_kernel_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed,
                              1) != cudaSuccess) {
@@ -1041,8 +1062,8 @@ int max_cluster_size() {
       cudaGetLastError();
       n = 8;
     }
-    size = n >= 16 ? 16 : (n >= 8 ? 8 : 0);
-  }
+    return n >= 16 ? 16 : (n >= 8 ? 8 : 0);
+  }();
   return size;
 }
 
@@ -1069,16 +1090,15 @@ int cg_grid_size(int nslices, int nbank0) {
   int cl = max_cluster_size();
   // One cluster while each warp has at most ~3 slices / banks to process.
   if (cl > 0 && want_blocks <= 3 * cl) return -cl;
-  static int max_coop = 0;
-  if (max_coop == 0) {
+  static const int max_coop = [] {
     int dev = 0, sms = 0, per_sm = 0;
     CUDA_CHECK(cudaGetDevice(&dev));
     CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     size_t smem = kCgWarps * kPacked * sizeof(float);
     CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_kernel,
                                                              kCgThreads, smem));
-    max_coop = sms * (per_sm > 0 ? per_sm : 1);
-  }
+    return sms * (per_sm > 0 ? per_sm : 1);
+  }();
   int want = div_up(nslices > nbank0 ? nslices : nbank0, kCgWarps);
   if (want < 1) want = 1;
   return want < max_coop ? want : max_coop;
@@ -1111,10 +1131,12 @@ void launch_cg(const CgArgs& a, int grid, cudaStream_t st) {
 }
 
 int cg_resident_grid(int res_blocks) {
-  static int max_coop = -1, max_cluster = 0;
-  const size_t smem = sizeof(ResShared);
-  if (max_coop < 0) {
-    max_coop = 0;
+  struct Limits {
+    int max_coop = 0, max_cluster = 0;
+  };
+  static const Limits lim = [] {
+    Limits l;
+    const size_t smem = sizeof(ResShared);
     int dev = 0, sms = 0, per_sm = 0;
     CUDA_CHECK(cudaGetDevice(&dev));
     CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -1127,7 +1149,7 @@ int cg_resident_grid(int res_blocks) {
       cudaGetLastError();
       per_sm = 0;
     }
-    max_coop = sms * per_sm;
+    l.max_coop = sms * per_sm;
     if (cudaFuncSetAttribute(cg_resident_cluster_kernel,
                              cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
       cudaGetLastError();
@@ -1148,11 +1170,12 @@ int cg_resident_grid(int res_blocks) {
       cudaGetLastError();
       n = 0;
     }
-    max_cluster = n >= 16 ? 16 : (n >= 8 ? 8 : 0);
-  }
-  if (res_blocks <= 0 || max_coop == 0) return 0;
-  if (res_blocks > 1 && res_blocks <= max_cluster) return -res_blocks;
-  return res_blocks <= max_coop ? res_blocks : 0;
+    l.max_cluster = n >= 16 ? 16 : (n >= 8 ? 8 : 0);
+    return l;
+  }();
+  if (res_blocks <= 0 || lim.max_coop == 0) return 0;
+  if (res_blocks > 1 && res_blocks <= lim.max_cluster) return -res_blocks;
+  return res_blocks <= lim.max_coop ? res_blocks : 0;
 }
 
 void launch_cg_resident(const CgArgs& a, int grid, cudaStream_t st) {

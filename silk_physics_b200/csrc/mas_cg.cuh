@@ -66,9 +66,10 @@ struct CgArgs {
   int* result = nullptr;  // [iterations, status]
   int* stats = nullptr;   // accumulated [iterations, solves, first-solve iterations,
                           // learned starts taken]
-  // Alternative start (learned warm start; null = none): taken when its
-  // residual is smaller than that of x, while the stopping rule keeps the
-  // residual of x as rr0 (the plain start judges the alternative).
+  // Alternative start (learned warm start; null = none): the CG starts from
+  // x + w (x_alt - x) with the residual-minimising w >= 0 (w = 0: the plain
+  // start), while the stopping rule keeps the residual of x as rr0 (the plain
+  // start judges the alternative).
   const float4* x_alt = nullptr;
   int first_solve = 0;    // count this solve's iterations in stats[2]
   float* result_rr = nullptr;

@@ -59,6 +59,7 @@ silk_status World::init(int backend) {
     last_error = "CUDA runtime/device not available";
     return SILK_ERR_NO_CUDA_SUPPORT;
   }
+  CUDA_CHECK(cudaGetDevice(&device));
   ensure_stream();
   if (!coll_) coll_ = std::make_unique<CollisionSystem>(*this);
   initialized = true;

@@ -135,6 +135,7 @@ class World {
 
   std::string last_error;
   bool initialized = false;
+  int device = 0;  // CUDA device the world was initialised on
 
   silk_status init(int backend);
   silk_status set_global_config(const silk_global_config& c);

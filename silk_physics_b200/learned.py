@@ -95,14 +95,20 @@ def _world(V, F, pins, SV=None, SF=None, inner=100, capture=True, tol=1e-5):
 
 
 def collect(scenes, steps: int, keep_per_step: int = 4096, seed: int = 0,
-            samples: SampleSet | None = None) -> SampleSet:
-    """Run each scene (V, F, pins, SV, SF, inner) for `steps` steps and keep
-    up to keep_per_step vertex samples of every step that recorded some."""
+            samples: SampleSet | None = None, budget_s: float = 20.0) -> SampleSet:
+    """Run each scene (V, F, pins, SV, SF, inner) for up to `steps` steps (and
+    at most budget_s seconds) and keep up to keep_per_step vertex samples of
+    every step that recorded some."""
+    import time
+
     rng = np.random.default_rng(seed)
     samples = samples or SampleSet()
     for V, F, pins, SV, SF, inner in scenes:
         w, h = _world(V, F, pins, SV, SF, inner)
+        t0 = time.time()
         for _ in range(steps):
+            if time.time() - t0 > budget_s:
+                break
             r = w.solver_step()
             if not r:
                 break
@@ -162,3 +168,39 @@ def load(path: str) -> np.ndarray:
     if p.size != N_PARAMS:
         raise ValueError(f"{path}: expected {N_PARAMS} parameters, got {p.size}")
     return p
+
+
+def main(argv=None) -> None:
+    """Generate solver samples, train on the GPU and save the model:
+
+    python -m silk_physics_b200.learned --out silk_physics_b200/models/warm_start.npy
+    """
+    import argparse
+    import time
+
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--scenes", type=int, default=12)
+    ap.add_argument("--steps", type=int, default=40, help="solver steps per scene")
+    ap.add_argument("--keep", type=int, default=4096, help="vertex samples kept per step")
+    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--batch", type=int, default=65536)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--seed", type=int, default=0)
+    a = ap.parse_args(argv)
+    rng = np.random.default_rng(a.seed)
+    t0 = time.time()
+    scenes = training_scenes(rng, a.scenes)
+    samples = collect(scenes, a.steps, a.keep, a.seed)
+    f, t = samples.arrays()
+    t1 = time.time()
+    p, hist = train(f, t, a.train_steps, a.batch, a.lr, a.seed)
+    t2 = time.time()
+    save(a.out, p)
+    print(f"{len(f)} samples from {a.scenes} scenes x {a.steps} steps in {t1 - t0:.1f} s; "
+          f"trained {a.train_steps} steps in {t2 - t1:.1f} s; loss {hist[0]:.4f} -> "
+          f"{hist[-1]:.4f}; saved {a.out}")
+
+
+if __name__ == "__main__":
+    main()

@@ -77,7 +77,7 @@ class _SolverOptionsC(C.Structure):
     _fields_ = [("fixed_linear_rel_tol", C.c_float), ("cg_max_iter", C.c_int32),
                 ("mas_bf16", C.c_int32), ("profile", C.c_int32), ("cg_form", C.c_int32),
                 ("learned_warm_start", C.c_int32), ("capture_samples", C.c_int32),
-                ("reserved", C.c_int32 * 1)]
+                ("contact_gs_form", C.c_int32)]
 
 
 class _ProfileC(C.Structure):
@@ -160,6 +160,7 @@ class SolverOptions:
     cg_form: int = 0  # 0: resident CG kernel where possible; 1: streaming form
     learned_warm_start: bool = False  # offer the loaded model's first-solve start
     capture_samples: bool = False     # record warm-start training samples
+    contact_gs_form: int = 0          # 0: single-block Gauss-Seidel where possible; 1: grid
 
     def to_c(self) -> _SolverOptionsC:
         o = _SolverOptionsC()
@@ -170,6 +171,7 @@ class SolverOptions:
         o.cg_form = int(self.cg_form)
         o.learned_warm_start = int(self.learned_warm_start)
         o.capture_samples = int(self.capture_samples)
+        o.contact_gs_form = int(self.contact_gs_form)
         return o
 
 
@@ -213,6 +215,8 @@ def _load() -> C.CDLL:
         "silk_clear": ([_W], None),
         "silk_solver_step": ([_W], C.c_int),
         "silk_solver_reset": ([_W], C.c_int),
+        "silk_step_many": ([C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.POINTER(C.c_int)],
+                           C.c_int),
         "silk_add_cloth": ([_W, C.POINTER(_ClothConfigC), C.POINTER(_CollisionConfigC),
                             _F32P, C.c_int64, _I32P, C.c_int64, C.c_void_p, C.c_int64,
                             C.POINTER(C.c_uint32)], C.c_int),
@@ -522,6 +526,15 @@ def ccd_batch(is_vertex_face: bool, x: np.ndarray, err3, min_separation,
     if st:
         raise RuntimeError(_result(st).to_string())
     return hit.astype(bool), toi, tup
+
+
+def step_many(worlds, threads: int = 0) -> list[Result]:
+    """Advance independent worlds by one step each, concurrently."""
+    n = len(worlds)
+    arr = (C.c_void_p * max(n, 1))(*[w._w for w in worlds])
+    st = (C.c_int * max(n, 1))()
+    lib.silk_step_many(arr, n, threads, st)
+    return [_result(st[i], worlds[i]._w) for i in range(n)]
 
 
 MLP_PARAMS = 9968  # SILK_MLP_PARAMS

@@ -179,3 +179,122 @@ def test_sheet_on_sphere_contacts_and_parity(oracle):
         assert st.outer_iterations == so["outer_iterations"]
         assert err < 1e-3
     assert saw_contacts
+
+
+def test_moving_obstacle_parity(oracle):
+    """A sphere pushed up under a resting sheet through set_obstacle_position
+    (the prescribed obstacle displacement of dcd.cu:84-96 enters every
+    contact): contact, colour and rollback counts equal the oracle's over the
+    first three steps (afterwards FP32 rounding may move a pair across the
+    activation distance: contact counts within 2 %) and positions agree
+    within 1e-3 m over four steps (the lifted sheet's contact trajectory
+    diverges from the oracle's after that, as two FP32 runs of the reference
+    would)."""
+    V, F = S.grid_sheet(20, side=0.5, z=0.305, jitter=1e-4, seed=5)
+    SV, SF = S.icosphere(3, radius=0.3)
+    g = N.GlobalConfig(max_inner_iteration=30)
+    w = N.World()
+    assert w.init()
+    assert w.set_global_config(g)
+    assert w.set_solver_options(N.SolverOptions(fixed_linear_rel_tol=1e-5))
+    r, h = w.add_cloth(N.ClothConfig(), N.CollisionConfig(), V, F, [])
+    r2, hs = w.add_obstacle(N.CollisionConfig(), SV, SF)
+    assert r and r2
+    perm, offs = w.cloth_partition(h, len(V))
+    ow = oracle.OracleWorld(config=dict(max_inner_iteration=30, fixed_linear_rel_tol=1e-5))
+    oh = ow.add_cloth(V, F, [], perm, offs)
+    ohs = ow.add_obstacle(SV, SF)
+    x = np.zeros(V.size, np.float32)
+    saw = False
+    for k in range(4):
+        pos = (SV + np.array([0.0, 0.0, 0.004 * (k + 1)], np.float32)).astype(np.float32)
+        assert w.set_obstacle_position(hs, pos)
+        assert ow.set_obstacle_position(ohs, pos) == 0
+        assert w.solver_step(), w
+        assert ow.step() == 0
+        st, so = w.step_stats(), ow.stats()
+        assert w.get_cloth_position(h, x)
+        err = np.abs(x.reshape(-1, 3) - ow.position(oh)).max()
+        print(f"step {k + 1}: contacts {st.contacts}/{so['contacts']} outer "
+              f"{st.outer_iterations}/{so['outer_iterations']} err {err:.2e}")
+        saw |= st.contacts > 0
+        if k < 3:
+            assert st.contacts == so["contacts"] and st.colors == so["colors"]
+            assert st.outer_iterations == so["outer_iterations"]
+        else:
+            # FP32 rounding may move a pair across the activation distance.
+            assert abs(st.contacts - so["contacts"]) <= max(2, 0.02 * so["contacts"])
+        assert err < 1e-3
+    assert saw
+    # The sheet was lifted with the sphere.
+    assert x.reshape(-1, 3)[:, 2].max() > 0.305
+
+
+def test_collision_groups_filter_candidates(oracle):
+    """Objects collide only within one collision group (find_collision.cu:
+    17-25): with the second sheet in its own group, no candidate pairs it
+    with the first sheet or the sphere, and the candidate sets still equal the
+    oracle's."""
+    w = N.World()
+    assert w.init()
+    ow = oracle.OracleWorld()
+    sheets = []
+    for k, (z, grp) in enumerate(((0.35, 0), (0.365, 1))):
+        V, F = S.grid_sheet(12, side=0.6, z=z, jitter=1e-3, seed=20 + k)
+        col = N.CollisionConfig(group=grp)
+        r, h = w.add_cloth(N.ClothConfig(), col, V, F, [])
+        assert r
+        perm, offs = w.cloth_partition(h, len(V))
+        assert ow.add_cloth(V, F, [], perm, offs, collision=(1, 1, grp, 0.3, 0.3)) == h
+        sheets.append((h, V))
+    SV, SF = S.icosphere(2, radius=0.3)
+    r, hs = w.add_obstacle(N.CollisionConfig(group=0), SV, SF)
+    assert r and ow.add_obstacle(SV, SF, collision=(1, 1, 0, 0.3, 0.3)) == hs
+    d = _disp([(h, V, None, None) for h, V in sheets], 5e-3, 7)
+    w.debug_refit(d)
+    ow.refit(d)
+    g = w.debug_candidates()
+    o = ow.candidates()
+    assert _rows(g) == _rows(o)
+    hb = sheets[1][0]
+    # Records are (kind, handle a, primitive a, handle b, primitive b): the
+    # second sheet may only pair with itself.
+    pairs = {(int(c[1]), int(c[3])) for c in g}
+    print(f"{len(g)} candidates; object pairs {sorted(pairs)}")
+    assert len(g) > 0
+    for a, b in pairs:
+        if hb in (a, b):
+            assert a == b == hb
+
+
+def test_gs_forms_identical():
+    """The single-block contact Gauss-Seidel (colour-ordered contacts on
+    compact vertex slots) and the grid form give bit-identical positions on a
+    pinned sheet draped on a sphere, where contacts also read pinned vertices
+    and clamped (zero-weight) closest points."""
+    out = []
+    for form in (0, 1):
+        V, F = S.grid_sheet(32, side=0.8, z=0.305, jitter=1e-4, seed=8)
+        # Corners and the vertex over the sphere's top pinned: the sheet drapes
+        # around a pinned vertex, so contacts also involve pinned vertices.
+        P = np.concatenate([S.top_corner_pins(32), [16 * 32 + 16]]).astype(np.int32)
+        SV, SF = S.icosphere(3, radius=0.3)
+        w = N.World()
+        assert w.init()
+        assert w.set_global_config(N.GlobalConfig(acceleration_z=-9.81, max_inner_iteration=40))
+        assert w.set_solver_options(N.SolverOptions(fixed_linear_rel_tol=1e-5,
+                                                    contact_gs_form=form))
+        r, h = w.add_cloth(N.ClothConfig(), N.CollisionConfig(), V, F, P)
+        r2, _ = w.add_obstacle(N.CollisionConfig(), SV, SF)
+        assert r and r2
+        contacts = []
+        for _ in range(10):
+            assert w.solver_step(), w
+            contacts.append(w.step_stats().contacts)
+        x = np.zeros(V.size, np.float32)
+        assert w.get_cloth_position(h, x)
+        out.append((x, contacts))
+    print(f"contacts per step: {out[0][1]}")
+    assert max(out[0][1]) > 0
+    assert out[0][1] == out[1][1]
+    np.testing.assert_array_equal(out[0][0], out[1][0])
