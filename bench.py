@@ -79,6 +79,7 @@ def timed_variant(N, torch, stream, flush, V, F, SV, SF, cg_rel_tol, bf16, learn
     for _ in range(prelude):
         r = w.solver_step()
         assert r, r.to_string()
+    w.profile(reset=True)
     ms, admm, cg, solves, first, taken, outer = 0.0, 0, 0, 0, 0, 0, 0
     for k in range(steps):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -97,7 +98,12 @@ def timed_variant(N, torch, stream, flush, V, F, SV, SF, cg_rel_tol, bf16, learn
         first += st.cg_first_solve_iterations
         taken += st.learned_starts
         outer += st.outer_iterations
+    prof = w.profile(reset=True)
     return {"value": round(steps / (ms / 1e3), 4), "ms_per_step": round(ms / steps, 3),
+            "cg_kernel_ms_per_step": round(prof["cg_time_ms"] / steps, 2),
+            "other_admm_kernels_ms_per_step": round(prof["admm_other_ms"] / steps, 2),
+            "ccd_host_ms_per_step": round(prof["ccd_host_ms"] / steps, 2),
+            "dcd_host_ms_per_step": round(prof["dcd_host_ms"] / steps, 2),
             "admm_iterations_per_step": admm / steps,
             "cg_iterations_per_solve": round(cg / max(solves, 1), 2),
             "first_solve_cg_iterations_per_outer": round(first / max(outer, 1), 2),
@@ -384,6 +390,13 @@ def run_ours(args) -> None:
                 "steps": n_e2e, "device_value_same_steps": round(value_same_steps, 4)},
         "gpu_launches": int(launches),
         "clocks": clocks,
+        "phases_ms_per_step": {
+            "cg_kernel_events": round(prof["cg_time_ms"] / args.steps, 2),
+            "other_admm_kernels_events": round(prof["admm_other_ms"] / args.steps, 2),
+            "admm_host_wall": round(prof["admm_host_ms"] / args.steps, 2),
+            "ccd_host_wall": round(prof["ccd_host_ms"] / args.steps, 2),
+            "dcd_host_wall": round(prof["dcd_host_ms"] / args.steps, 2),
+            "step_host_wall": round(prof["step_host_ms"] / args.steps, 2)},
         "variants": variants,
     }
     print(json.dumps(line), flush=True)
@@ -405,7 +418,8 @@ def run_trace(args) -> None:
 
     from silk_physics_b200 import native as N
 
-    V, F, SV, SF = scene()
+    c3 = args.trace_workload == "c3"
+    V, F, SV, SF = scene_c3() if c3 else scene()
     stream = torch.cuda.Stream()
     opts = N.SolverOptions(fixed_linear_rel_tol=args.cg_rel_tol, profile=1, mas_bf16=args.bf16)
     w, h, _ = make_world(stream.cuda_stream, opts, V, F, SV, SF)
@@ -419,7 +433,9 @@ def run_trace(args) -> None:
     names = RESIDENT_PHASES if t["form"] == 1 else STREAMING_PHASES
     med = np.median(t["phase_cycles"], axis=0)[:len(names)] / ghz / 1e3
     print(json.dumps({"cg_trace": {
-        "workload": WORKLOAD, "form": "resident" if t["form"] == 1 else "streaming",
+        "workload": C3_WORKLOAD if c3 else WORKLOAD,
+        "steps_before": args.prelude + args.warmup,
+        "form": "resident" if t["form"] == 1 else "streaming",
         "mas": "bf16" if args.bf16 else "fp32", "traced_iterations": t["iters"],
         "sm_ghz": round(ghz, 3), "phase_us": {n: round(float(m), 2) for n, m in zip(names, med)},
         "iteration_us": round(float(med.sum()), 2)}}), flush=True)
@@ -582,6 +598,7 @@ def main() -> None:
     ap.add_argument("--variant-steps", type=int, default=5)
     ap.add_argument("--c3-prelude", type=int, default=8)
     ap.add_argument("--c3-steps", type=int, default=2)
+    ap.add_argument("--trace-workload", choices=["c2", "c3"], default="c2")
     ap.add_argument("--batched", action="store_true",
                     help="time independent scenes stepped concurrently instead of the bench line")
     ap.add_argument("--c5-scenes", type=int, default=64)

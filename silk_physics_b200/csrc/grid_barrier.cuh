@@ -7,13 +7,17 @@
 
 namespace silkb {
 
-constexpr long long kBarrierSpinLimit = 1ll << 25;  // ~2 s with back-off
+constexpr long long kBarrierSpinLimit = 1ll << 22;  // polls: ~2-4 s (an L2 round trip each)
 
+// The k-th barrier of a launch waits until the arrival counter (zero at
+// launch, never reset) reaches k x nblocks: one atomic per block on the
+// critical path and no generation word for the last block to bump.
 struct GridBarrier {
   unsigned* count;
   unsigned* err;
-  unsigned* gen;
+  unsigned* unused;
   unsigned nblocks;
+  unsigned epoch = 0;  // barriers passed by this block
 
   __device__ bool sync() {
     __shared__ int s_ok;
@@ -21,33 +25,29 @@ struct GridBarrier {
       __syncthreads();
       return true;
     }
+    ++epoch;
     __syncthreads();
     if (threadIdx.x == 0) {
-      cuda::atomic_ref<unsigned, cuda::thread_scope_device> g(*gen), c(*count),
-          e(*err);
+      cuda::atomic_ref<unsigned, cuda::thread_scope_device> c(*count), e(*err);
       int ok = 1;
-      unsigned my = g.load(cuda::memory_order_relaxed);
       if (e.load(cuda::memory_order_relaxed) != 0u) {
         ok = 0;
       } else {
-        unsigned arrived = c.fetch_add(1u, cuda::memory_order_acq_rel);
-        if (arrived == nblocks - 1u) {
-          c.store(0u, cuda::memory_order_relaxed);
-          g.fetch_add(1u, cuda::memory_order_release);
-        } else {
-          long long spins = 0;
-          while (g.load(cuda::memory_order_acquire) == my) {
-            if (e.load(cuda::memory_order_relaxed) != 0u) {
-              ok = 0;
-              break;
-            }
-            if (++spins > kBarrierSpinLimit) {
-              e.store(1u, cuda::memory_order_relaxed);
-              ok = 0;
-              break;
-            }
-            __nanosleep(32);
+        const unsigned target = epoch * nblocks;
+        unsigned arrived = c.fetch_add(1u, cuda::memory_order_acq_rel) + 1u;
+        long long spins = 0;
+        while (arrived < target) {
+          if (e.load(cuda::memory_order_relaxed) != 0u) {
+            ok = 0;
+            break;
           }
+          if (++spins > kBarrierSpinLimit) {
+            e.store(1u, cuda::memory_order_relaxed);
+            ok = 0;
+            break;
+          }
+          __nanosleep(32);
+          arrived = c.load(cuda::memory_order_acquire);
         }
       }
       s_ok = ok;
