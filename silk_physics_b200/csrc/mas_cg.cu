@@ -544,6 +544,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel_cluster(CgArgs a) {
 // from other blocks first) differs.
 // ---------------------------------------------------------------------------
 constexpr int kResWarps = kResThreads / 32;
+static_assert(kResCoarseBanks <= kResWarps, "one warp per upper coarse bank");
 
 // A bank slot of shared memory holds either the packed FP32 inverse (528
 // floats) or, for BF16 storage, the inverse as mma.m16n8k16 A fragments:
@@ -880,34 +881,45 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     rz = s.tot[0];
     rr = s.tot[1];
     if (a.levels > 1) {
-      double rzc = 0.0;
+      // The restriction chain first (warp sums per connected component), then
+      // every upper bank applied at once, one warp per bank: the levels are
+      // additive, each inverse only needs its own level's input.
       int cb = 0;
-      for (int l = 1; l < a.levels; ++l) {
+      for (int l = 1; l + 1 < a.levels; ++l) {
         const MasLevelDev& lv = a.coarse[l];
-        const bool last = l + 1 >= a.levels;
         if (warp < lv.nbank) {
-          int slot = (cb + warp) * BANK + lane;
           bool valid = warp * BANK + lane < lv.nnode;
-          float4 q = s.rc[slot];
+          float4 q = s.rc[(cb + warp) * BANK + lane];
           float3 rl = valid ? make_float3(q.x, q.y, q.z) : make_float3(0.f, 0.f, 0.f);
-          float3 zl = apply(s.Mc[cb + warp], rl);
-          if (!valid) zl = make_float3(0.f, 0.f, 0.f);
-          s.zc[slot] = make_float4(zl.x, zl.y, zl.z, 0.f);
-          rzc += (double)rl.x * zl.x + (double)rl.y * zl.y + (double)rl.z * zl.z;
-          if (!last) {
-            int n = lv.ncco[warp], base = lv.cco_base[warp];
-            int mine = lv.slot_cco[(size_t)warp * BANK + lane];
-            int next = (cb + lv.nbank) * BANK;
-            for (int c = 0; c < n; ++c) {
-              float qx = warp_sum(mine == c ? rl.x : 0.f);
-              float qy = warp_sum(mine == c ? rl.y : 0.f);
-              float qz = warp_sum(mine == c ? rl.z : 0.f);
-              if (lane == 0) s.rc[next + base + c] = make_float4(qx, qy, qz, 0.f);
-            }
+          int n = lv.ncco[warp], base = lv.cco_base[warp];
+          int mine = lv.slot_cco[(size_t)warp * BANK + lane];
+          int next = (cb + lv.nbank) * BANK;
+          for (int c = 0; c < n; ++c) {
+            float qx = warp_sum(mine == c ? rl.x : 0.f);
+            float qy = warp_sum(mine == c ? rl.y : 0.f);
+            float qz = warp_sum(mine == c ? rl.z : 0.f);
+            if (lane == 0) s.rc[next + base + c] = make_float4(qx, qy, qz, 0.f);
           }
         }
         cb += lv.nbank;
         __syncthreads();
+      }
+      double rzc = 0.0;
+      int first = 0;
+      for (int l = 1; l < a.levels; ++l) {
+        const MasLevelDev& lv = a.coarse[l];
+        const int j = warp - first;
+        if (j >= 0 && j < lv.nbank) {
+          int slot = (first + j) * BANK + lane;
+          bool valid = j * BANK + lane < lv.nnode;
+          float4 q = s.rc[slot];
+          float3 rl = valid ? make_float3(q.x, q.y, q.z) : make_float3(0.f, 0.f, 0.f);
+          float3 zl = apply(s.Mc[first + j], rl);
+          if (!valid) zl = make_float3(0.f, 0.f, 0.f);
+          s.zc[slot] = make_float4(zl.x, zl.y, zl.z, 0.f);
+          rzc += (double)rl.x * zl.x + (double)rl.y * zl.y + (double)rl.z * zl.z;
+        }
+        first += lv.nbank;
       }
       tr.stamp(iter, 11);
       const double v1[1] = {rzc};
