@@ -102,6 +102,7 @@ def timed_variant(N, torch, stream, flush, V, F, SV, SF, cg_rel_tol, bf16, learn
     return {"value": round(steps / (ms / 1e3), 4), "ms_per_step": round(ms / steps, 3),
             "cg_kernel_ms_per_step": round(prof["cg_time_ms"] / steps, 2),
             "other_admm_kernels_ms_per_step": round(prof["admm_other_ms"] / steps, 2),
+            "contact_gs_ms_per_step": round(prof["contact_gs_ms"] / steps, 2),
             "ccd_host_ms_per_step": round(prof["ccd_host_ms"] / steps, 2),
             "dcd_host_ms_per_step": round(prof["dcd_host_ms"] / steps, 2),
             "admm_iterations_per_step": admm / steps,
@@ -393,6 +394,7 @@ def run_ours(args) -> None:
         "phases_ms_per_step": {
             "cg_kernel_events": round(prof["cg_time_ms"] / args.steps, 2),
             "other_admm_kernels_events": round(prof["admm_other_ms"] / args.steps, 2),
+            "contact_gs_events": round(prof["contact_gs_ms"] / args.steps, 2),
             "admm_host_wall": round(prof["admm_host_ms"] / args.steps, 2),
             "ccd_host_wall": round(prof["ccd_host_ms"] / args.steps, 2),
             "dcd_host_wall": round(prof["dcd_host_ms"] / args.steps, 2),

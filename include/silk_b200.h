@@ -110,7 +110,8 @@ typedef struct {
   double ccd_host_ms;        /* host wall time of refit + CCD */
   double dcd_host_ms;        /* host wall time of DCD + contact rebuild */
   double step_host_ms;       /* host wall time of solver_step */
-  double reserved[3];
+  double contact_gs_ms;      /* events: contact Gauss-Seidel (part of admm_other_ms) */
+  double reserved[2];
 } silk_profile;
 
 /* Statistics of the last solver_step. */

@@ -32,10 +32,11 @@ World::World() {
 
 World::~World() {
   coll_.reset();
-  for (auto& e : events) {
-    cudaEventDestroy(e.first);
-    cudaEventDestroy(e.second);
-  }
+  for (auto* pool : {&events, &events_other, &events_gs})
+    for (auto& e : *pool) {
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -952,7 +953,11 @@ bool World::admm_solve() {
     launch_face_step(s, face_partials.p, fb, st);
     if (contacts) {
       launch_contact_init(s, st);
+      std::pair<cudaEvent_t, cudaEvent_t>* ge =
+          opt.profile ? next_event_pair(events_gs, events_gs_used) : nullptr;
+      if (ge) CUDA_CHECK(cudaEventRecord(ge->first, st));
       coll_->contact_solve();
+      if (ge) CUDA_CHECK(cudaEventRecord(ge->second, st));
     }
     launch_vertex_step(s, vertex_partials.p, vb, st);
     if (oe) CUDA_CHECK(cudaEventRecord(oe->second, st));
@@ -992,6 +997,7 @@ silk_status World::solver_step() {
     for (auto& c : cloths) c->dev.stats.zero(st);
     events_used = 0;
     events_other_used = 0;
+    events_gs_used = 0;
     CUDA_CHECK(cudaMemcpyAsync(step_start.p, sx.p, nv * sizeof(float4), cudaMemcpyDeviceToDevice, st));
     if (opt.capture_samples) samples_valid = false;
     // init (main_loop.cu:24-76): damped velocity, fresh ADMM aux variables.
@@ -1094,6 +1100,11 @@ silk_status World::solver_step() {
         prof.cg_time_ms += ms;
       }
       prof.cg_launches += (int64_t)events_used;
+      for (size_t e = 0; e < events_gs_used; ++e) {
+        float ms = 0.f;
+        CUDA_CHECK(cudaEventElapsedTime(&ms, events_gs[e].first, events_gs[e].second));
+        prof.contact_gs_ms += ms;
+      }
       for (size_t e = 0; e < events_other_used; ++e) {
         float ms = 0.f;
         CUDA_CHECK(cudaEventElapsedTime(&ms, events_other[e].first, events_other[e].second));

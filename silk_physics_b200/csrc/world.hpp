@@ -20,21 +20,23 @@ namespace silkb {
 template <class T>
 struct DevBuf {
   T* p = nullptr;
-  size_t n = 0;
+  size_t n = 0;    // elements in use
+  size_t cap = 0;  // elements allocated
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) {
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), cap(o.cap) {
     o.p = nullptr;
-    o.n = 0;
+    o.n = o.cap = 0;
   }
   DevBuf& operator=(DevBuf&& o) noexcept {
     if (this != &o) {
       reset();
       p = o.p;
       n = o.n;
+      cap = o.cap;
       o.p = nullptr;
-      o.n = 0;
+      o.n = o.cap = 0;
     }
     return *this;
   }
@@ -42,11 +44,20 @@ struct DevBuf {
   void reset() {
     if (p) cudaFree(p);
     p = nullptr;
-    n = 0;
+    n = cap = 0;
   }
+  // Size the buffer to `count` elements.  The storage only grows: a smaller
+  // or equal request reuses it (cudaFree synchronises the whole device, and
+  // the per-outer-iteration buffers of the contact build are resized often).
+  // Contents are unspecified afterwards.  All work of a world is ordered on
+  // its stream, so reusing storage that earlier launches read is safe.
   void alloc(size_t count) {
+    if (count <= cap && p) {
+      n = count;
+      return;
+    }
     reset();
-    n = count;
+    n = cap = count;
     if (count) CUDA_CHECK(cudaMalloc(&p, count * sizeof(T)));
   }
   void zero(cudaStream_t st) {
@@ -211,8 +222,8 @@ class World {
   bool warm_first_ = false;  // the current outer iteration is the step's first
   int pinned_dof = 0;
   silk_profile prof{};
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events, events_other;
-  size_t events_used = 0, events_other_used = 0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events, events_other, events_gs;
+  size_t events_used = 0, events_other_used = 0, events_gs_used = 0;
   std::pair<cudaEvent_t, cudaEvent_t>* next_event_pair(
       std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& pool, size_t& used);
 

@@ -85,7 +85,8 @@ class _ProfileC(C.Structure):
                 ("cg_iterations", C.c_int64), ("cg_algorithmic_bytes", C.c_double),
                 ("admm_other_ms", C.c_double), ("admm_host_ms", C.c_double),
                 ("ccd_host_ms", C.c_double), ("dcd_host_ms", C.c_double),
-                ("step_host_ms", C.c_double), ("reserved", C.c_double * 3)]
+                ("step_host_ms", C.c_double), ("contact_gs_ms", C.c_double),
+                ("reserved", C.c_double * 2)]
 
 
 class _StepStatsC(C.Structure):
