@@ -1278,6 +1278,127 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
   for (int i = t; i < nslots; i += blockDim.x) p[vlist[i]] = sp[i];
 }
 
+// Pipelined single-block form: the contacts of the next kGsStages - 1 colour
+// phases stream into shared memory with cp.async while the current phase is
+// processed, and the corrections and colour offsets stay in shared memory for
+// the whole call, so a phase never waits on a global load.  Same per-contact
+// operations as contact_gs_kernel.
+constexpr int kGsStages = 4;
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gmem_src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+struct GsPipeLayout {
+  size_t sp, sc, go, stage, bytes;
+};
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+__host__ __device__ inline GsPipeLayout gs_pipe_layout(int nslots, int total, int ncolors,
+                                                       int threads) {
+  GsPipeLayout L;
+  L.sp = 0;
+  L.sc = align16(L.sp + (size_t)nslots * sizeof(float4));
+  L.go = align16(L.sc + (size_t)total * sizeof(float4));
+  L.stage = align16(L.go + (size_t)(ncolors + 1) * sizeof(int));
+  L.bytes = L.stage + (size_t)kGsStages * threads * sizeof(GsContact);
+  return L;
+}
+
+__global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
+    const GsContact* __restrict__ cc, const int* __restrict__ group_off, int ncolors, int total,
+    float4* __restrict__ corr, const int* __restrict__ vlist, int nslots, float4* __restrict__ p) {
+  extern __shared__ __align__(16) unsigned char gs_raw[];
+  const GsPipeLayout L = gs_pipe_layout(nslots, total, ncolors, blockDim.x);
+  float4* sp = reinterpret_cast<float4*>(gs_raw + L.sp);
+  float4* sc = reinterpret_cast<float4*>(gs_raw + L.sc);
+  int* sgo = reinterpret_cast<int*>(gs_raw + L.go);
+  GsContact* stage = reinterpret_cast<GsContact*>(gs_raw + L.stage);
+  const int t = threadIdx.x, nt = blockDim.x;
+  for (int i = t; i < nslots; i += nt) sp[i] = p[vlist[i]];
+  for (int q = t; q < total; q += nt) sc[q] = corr[cc[q].ci];
+  for (int c = t; c <= ncolors; c += nt) sgo[c] = group_off[c];
+  __syncthreads();
+  // Warm start with the saved corrections.
+  for (int col = 0; col < ncolors; ++col) {
+    int q = sgo[col] + t;
+    if (q < sgo[col + 1]) {
+      const GsContact& k = cc[q];
+      float4 r = sc[q];
+      for (int s = 0; s < 4; ++s) {
+        if (k.gamma[s] == 0.0f) continue;
+        float4 x = sp[k.slot[s]];
+        float g = k.gamma[s];
+        sp[k.slot[s]] = make_float4(x.x + g * r.x, x.y + g * r.y, x.z + g * r.z, 0.f);
+      }
+    }
+    __syncthreads();
+  }
+  const int phases = kGsSweeps * ncolors;
+  // Stage ph % kGsStages of this thread receives the contact of phase ph.
+  auto issue = [&](int ph) {
+    if (ph < phases) {
+      int col = ph % ncolors;
+      int q = sgo[col] + t;
+      if (q < sgo[col + 1]) {
+        const char* src = reinterpret_cast<const char*>(cc + q);
+        char* dst = reinterpret_cast<char*>(stage + (size_t)(ph % kGsStages) * nt + t);
+#pragma unroll
+        for (int b = 0; b < (int)sizeof(GsContact); b += 16) cp_async16(dst + b, src + b);
+      }
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int s = 0; s < kGsStages - 1; ++s) issue(s);
+  for (int ph = 0; ph < phases; ++ph) {
+    issue(ph + kGsStages - 1);
+    cp_async_wait<kGsStages - 1>();
+    const int col = ph % ncolors;
+    const int cur = sgo[col] + t;
+    if (cur < sgo[col + 1]) {
+      const GsContact kc = stage[(size_t)(ph % kGsStages) * nt + t];
+      const float4 o = sc[cur];
+      float3 u = kc.affine;
+      for (int s = 0; s < 4; ++s)
+        if (kc.slot[s] >= 0) {
+          float4 x = sp[kc.slot[s]];
+          u = add3(u, sc3(kc.coef[s], make_float3(x.x, x.y, x.z)));
+        }
+      float3 old = make_float3(o.x, o.y, o.z);
+      float3 us = sub3(u, old);
+      float un = dot3(us, kc.normal);
+      float3 unew;
+      if (un >= 0.0f) {
+        unew = us;
+      } else {
+        float3 ut = sub3(us, sc3(un, kc.normal));
+        float utn = sqrtf(dot3(ut, ut));
+        float radius = -kc.friction * un;
+        unew = utn <= radius ? make_float3(0.f, 0.f, 0.f) : sc3(1.0f - radius / utn, ut);
+      }
+      float3 du = sub3(unew, u);
+      float3 nc = add3(old, du);
+      sc[cur] = make_float4(nc.x, nc.y, nc.z, 0.f);
+      for (int s = 0; s < 4; ++s) {
+        if (kc.gamma[s] == 0.0f) continue;
+        float4 x = sp[kc.slot[s]];
+        float g = kc.gamma[s];
+        sp[kc.slot[s]] = make_float4(x.x + g * du.x, x.y + g * du.y, x.z + g * du.z, 0.f);
+      }
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+  for (int q = t; q < total; q += nt) corr[cc[q].ci] = sc[q];
+  for (int i = t; i < nslots; i += nt) p[vlist[i]] = sp[i];
+}
+
 // Canonical contact key (contact_constraints.cu:24-47).
 struct Key {
   int type;
@@ -1956,7 +2077,25 @@ void CollisionSystem::contact_solve() {
       return true;
     }();
     (void)attr;
-    contact_gs_block_kernel<<<1, kGsBlockThreads, smem, st>>>(
+    // Only as many warps as the largest colour needs: every colour phase ends
+    // in a block barrier, whose cost grows with the number of warps.
+    const int threads = std::max(32, div_up(I.max_group, 32) * 32);
+    const GsPipeLayout L = gs_pipe_layout(I.gs_nslots, I.n_contacts, I.n_colors, threads);
+    if (L.bytes <= kGsBlockSmemMax) {
+      static const bool pattr = [] {
+        CUDA_CHECK(cudaFuncSetAttribute(contact_gs_pipe_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kGsBlockSmemMax));
+        return true;
+      }();
+      (void)pattr;
+      contact_gs_pipe_kernel<<<1, threads, L.bytes, st>>>(
+          I.gs_cc.p, I.group_off.p, I.n_colors, I.n_contacts, I.corr.p, I.gs_vlist.p,
+          I.gs_nslots, w_.contact_p.p);
+      SILK_LAUNCHED();
+      return;
+    }
+    contact_gs_block_kernel<<<1, threads, smem, st>>>(
         I.gs_cc.p, I.group_off.p, I.n_colors, I.n_contacts, I.corr.p, I.gs_ccorr.p,
         I.gs_vlist.p, I.gs_nslots, w_.contact_p.p);
     SILK_LAUNCHED();
