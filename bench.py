@@ -269,7 +269,7 @@ def run_ours(args) -> None:
     w.profile(reset=True)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
-    launches = admm = cg = solves = contacts = 0
+    launches = admm = cg = solves = contacts = admm_first = 0
     if world_size > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -284,6 +284,8 @@ def run_ours(args) -> None:
             st = w.step_stats()
             launches += st.kernel_launches
             admm += st.admm_iterations
+            if k < args.e2e_steps:
+                admm_first += st.admm_iterations
             cg += st.cg_iterations
             solves += st.cg_solves
             contacts = st.contacts
@@ -329,6 +331,7 @@ def run_ours(args) -> None:
     pin_obs = torch.from_numpy(SV.ravel().copy()).pin_memory().numpy()
     pin_out = torch.empty(V.size, dtype=torch.float32).pin_memory().numpy()
     e2e_ms = []
+    e2e_admm = 0
     n_e2e = min(args.e2e_steps, args.steps)
     for k in range(n_e2e):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -342,6 +345,7 @@ def run_ours(args) -> None:
         b.synchronize()
         assert r, r.to_string()
         e2e_ms.append(a.elapsed_time(b))
+        e2e_admm += we.step_stats().admm_iterations
     e2e_val = n_e2e / (sum(e2e_ms) / 1e3) * world_size
     value_same_steps = n_e2e / (sum(step_ms[:n_e2e]) / 1e3) * world_size
     del we
@@ -388,7 +392,8 @@ def run_ours(args) -> None:
         "roofline": roofline, "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_val, 4), "unit": "steps/s",
                 "h2d_bytes_per_step": int(SV.nbytes), "d2h_bytes_per_step": int(V.nbytes),
-                "steps": n_e2e, "device_value_same_steps": round(value_same_steps, 4)},
+                "steps": n_e2e, "device_value_same_steps": round(value_same_steps, 4),
+                "admm_iterations": e2e_admm, "device_admm_iterations_same_steps": admm_first},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "phases_ms_per_step": {

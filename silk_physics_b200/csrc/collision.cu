@@ -1157,7 +1157,7 @@ struct GsContact {
   float3 normal;
   float friction;
   float3 affine;
-  int ci;       // contact index (correction storage)
+  int ci;       // contact index (correction storage); bit 31: distinct slots
 };
 static_assert(sizeof(GsContact) == sizeof(ContactDev), "same record size");
 
@@ -1193,7 +1193,14 @@ __global__ void gs_gather_kernel(const ContactDev* __restrict__ c, const int* __
   g.normal = k.normal;
   g.friction = k.friction;
   g.affine = k.affine;
-  g.ci = ci;
+  // Bit 31 of ci: the contact's cloth vertices are pairwise distinct, so the
+  // positions gathered for its relative position are still current when it
+  // is applied (the pipelined kernel then skips re-reading them).
+  bool distinct = true;
+  for (int a = 0; a < 4; ++a)
+    for (int b = a + 1; b < 4; ++b)
+      if (g.slot[a] >= 0 && g.slot[a] == g.slot[b]) distinct = false;
+  g.ci = ci | (distinct ? (int)0x80000000u : 0);
   out[q] = g;
 }
 
@@ -1204,7 +1211,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
   extern __shared__ float4 sp[];
   const int t = threadIdx.x;
   for (int i = t; i < nslots; i += blockDim.x) sp[i] = p[vlist[i]];
-  for (int q = t; q < total; q += blockDim.x) ccorr[q] = corr[cc[q].ci];
+  for (int q = t; q < total; q += blockDim.x) ccorr[q] = corr[cc[q].ci & 0x7fffffff];
   __syncthreads();
   // Warm start with the saved corrections.
   for (int col = 0; col < ncolors; ++col) {
@@ -1274,7 +1281,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
     }
     __syncthreads();
   }
-  for (int q = t; q < total; q += blockDim.x) corr[cc[q].ci] = ccorr[q];
+  for (int q = t; q < total; q += blockDim.x) corr[cc[q].ci & 0x7fffffff] = ccorr[q];
   for (int i = t; i < nslots; i += blockDim.x) p[vlist[i]] = sp[i];
 }
 
@@ -1283,7 +1290,8 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
 // processed, and the corrections and colour offsets stay in shared memory for
 // the whole call, so a phase never waits on a global load.  Same per-contact
 // operations as contact_gs_kernel.
-constexpr int kGsStages = 4;
+constexpr int kGsStages = 4;  // a power of two (stage = phase & (kGsStages - 1))
+static_assert((kGsStages & (kGsStages - 1)) == 0, "power of two");
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
   unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
@@ -1321,7 +1329,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
   GsContact* stage = reinterpret_cast<GsContact*>(gs_raw + L.stage);
   const int t = threadIdx.x, nt = blockDim.x;
   for (int i = t; i < nslots; i += nt) sp[i] = p[vlist[i]];
-  for (int q = t; q < total; q += nt) sc[q] = corr[cc[q].ci];
+  for (int q = t; q < total; q += nt) sc[q] = corr[cc[q].ci & 0x7fffffff];
   for (int c = t; c <= ncolors; c += nt) sgo[c] = group_off[c];
   __syncthreads();
   // Warm start with the saved corrections.
@@ -1340,35 +1348,43 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
     __syncthreads();
   }
   const int phases = kGsSweeps * ncolors;
-  // Stage ph % kGsStages of this thread receives the contact of phase ph.
-  auto issue = [&](int ph) {
+  // Stage ph % kGsStages of this thread receives the contact of phase ph
+  // (colour col_of_ph, tracked incrementally: no division per phase).
+  auto issue = [&](int ph, int col) {
     if (ph < phases) {
-      int col = ph % ncolors;
       int q = sgo[col] + t;
       if (q < sgo[col + 1]) {
         const char* src = reinterpret_cast<const char*>(cc + q);
-        char* dst = reinterpret_cast<char*>(stage + (size_t)(ph % kGsStages) * nt + t);
+        char* dst = reinterpret_cast<char*>(stage + (size_t)(ph & (kGsStages - 1)) * nt + t);
 #pragma unroll
         for (int b = 0; b < (int)sizeof(GsContact); b += 16) cp_async16(dst + b, src + b);
       }
     }
     cp_async_commit();
   };
+  int col_issue = 0;
 #pragma unroll
-  for (int s = 0; s < kGsStages - 1; ++s) issue(s);
+  for (int s = 0; s < kGsStages - 1; ++s) {
+    issue(s, col_issue);
+    col_issue = col_issue + 1 == ncolors ? 0 : col_issue + 1;
+  }
+  int col = 0;
   for (int ph = 0; ph < phases; ++ph) {
-    issue(ph + kGsStages - 1);
+    issue(ph + kGsStages - 1, col_issue);
+    col_issue = col_issue + 1 == ncolors ? 0 : col_issue + 1;
     cp_async_wait<kGsStages - 1>();
-    const int col = ph % ncolors;
     const int cur = sgo[col] + t;
-    if (cur < sgo[col + 1]) {
-      const GsContact kc = stage[(size_t)(ph % kGsStages) * nt + t];
+    const bool active = cur < sgo[col + 1];
+    col = col + 1 == ncolors ? 0 : col + 1;
+    if (active) {
+      const GsContact kc = stage[(size_t)(ph & (kGsStages - 1)) * nt + t];
       const float4 o = sc[cur];
       float3 u = kc.affine;
+      float4 xs[4];
       for (int s = 0; s < 4; ++s)
         if (kc.slot[s] >= 0) {
-          float4 x = sp[kc.slot[s]];
-          u = add3(u, sc3(kc.coef[s], make_float3(x.x, x.y, x.z)));
+          xs[s] = sp[kc.slot[s]];
+          u = add3(u, sc3(kc.coef[s], make_float3(xs[s].x, xs[s].y, xs[s].z)));
         }
       float3 old = make_float3(o.x, o.y, o.z);
       float3 us = sub3(u, old);
@@ -1385,9 +1401,10 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
       float3 du = sub3(unew, u);
       float3 nc = add3(old, du);
       sc[cur] = make_float4(nc.x, nc.y, nc.z, 0.f);
+      const bool distinct = kc.ci < 0;
       for (int s = 0; s < 4; ++s) {
         if (kc.gamma[s] == 0.0f) continue;
-        float4 x = sp[kc.slot[s]];
+        float4 x = distinct ? xs[s] : sp[kc.slot[s]];
         float g = kc.gamma[s];
         sp[kc.slot[s]] = make_float4(x.x + g * du.x, x.y + g * du.y, x.z + g * du.z, 0.f);
       }
@@ -1395,7 +1412,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
     __syncthreads();
   }
   cp_async_wait<0>();
-  for (int q = t; q < total; q += nt) corr[cc[q].ci] = sc[q];
+  for (int q = t; q < total; q += nt) corr[cc[q].ci & 0x7fffffff] = sc[q];
   for (int i = t; i < nslots; i += nt) p[vlist[i]] = sp[i];
 }
 
