@@ -644,8 +644,10 @@ __device__ __forceinline__ float3 bank_apply_mma(const float* slot, float3 r, in
 
 // Block sums of up to three doubles per thread, in a fixed order; thread 0
 // of the block stores them to out (global) when out is not null.  The sums
-// are left in s.tot.
-template <int N>
+// are left in s.tot.  kFinalSync = false skips the closing block barrier
+// where the caller's next step is a grid or cluster barrier anyway (which
+// also orders the next reuse of s.red and s.tot).
+template <int N, bool kFinalSync = true>
 __device__ void res_block_sum(const double (&v)[N], ResShared& s, double* out) {
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -664,7 +666,7 @@ __device__ void res_block_sum(const double (&v)[N], ResShared& s, double* out) {
       }
     }
   }
-  __syncthreads();
+  if (kFinalSync) __syncthreads();
 }
 
 // Sum of slot `slot` of every block's partials, the same in every block.
@@ -853,7 +855,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     }
     tr.stamp(iter, 7);
     const double v2[2] = {rz, rr};
-    res_block_sum<2>(v2, s, part);
+    res_block_sum<2, false>(v2, s, part);
     tr.stamp(iter, 8);
   };
   // Phase A head: totals and the redundant coarse levels >= 2.
@@ -987,7 +989,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
       tr.stamp(iter, 2);
       const double v1[1] = {own ? (double)p.x * Ap.x + (double)p.y * Ap.y + (double)p.z * Ap.z
                                 : 0.0};
-      res_block_sum<1>(v1, s, part + 2);
+      res_block_sum<1, false>(v1, s, part + 2);
     }
     tr.stamp(iter, 3);
     if (!bar.sync()) return fail();

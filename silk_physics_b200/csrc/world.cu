@@ -37,6 +37,9 @@ World::~World() {
       cudaEventDestroy(e.first);
       cudaEventDestroy(e.second);
     }
+  for (cudaStream_t cs : cloth_streams_) cudaStreamDestroy(cs);
+  for (cudaEvent_t e : cloth_done_) cudaEventDestroy(e);
+  if (fork_ev_) cudaEventDestroy(fork_ev_);
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -48,6 +51,18 @@ void World::ensure_stream() {
 }
 
 void World::sync() { CUDA_CHECK(cudaStreamSynchronize(stream)); }
+
+void World::ensure_cloth_streams(size_t n) {
+  if (!fork_ev_) CUDA_CHECK(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
+  while (cloth_streams_.size() < n) {
+    cudaStream_t s;
+    cudaEvent_t e;
+    CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cloth_streams_.push_back(s);
+    cloth_done_.push_back(e);
+  }
+}
 
 silk_status World::init(int backend) {
   if (backend != SILK_BACKEND_GPU) {
@@ -760,7 +775,7 @@ void World::upload_pins() {
 }
 
 // MASPreconditioner::factorize on A = L + diag(lhs) (mas_preconditioner.cu:903).
-void World::factorize(Cloth& c) {
+void World::factorize(Cloth& c, cudaStream_t st) {
   ClothDev& d = c.dev;
   const ClothSetup& S = *c.setup;
   const float* dyn = lhs.p + c.voff;
@@ -772,12 +787,12 @@ void World::factorize(Cloth& c) {
     gd.diag_off = k == 0 ? d.gal[k].diag_off.p : nullptr;
     gd.diag = k == 0 ? d.gal[k].diag.p : nullptr;
     gd.vals = d.gal[k].vals.p;
-    launch_galerkin_fill(gd, k == 0 ? d.Lvals.p : d.gal[k - 1].vals.p, dyn, stream);
+    launch_galerkin_fill(gd, k == 0 ? d.Lvals.p : d.gal[k - 1].vals.p, dyn, st);
   }
-  launch_bank_invert(d.cg.fine, true, d.part_off.p, d.Lvals.p, dyn, stream);
+  launch_bank_invert(d.cg.fine, true, d.part_off.p, d.Lvals.p, dyn, st);
   for (int l = 1; l <= S.levels; ++l)
     launch_bank_invert(d.cg.coarse[l - 1], false, nullptr, d.gal[l - 1].vals.p,
-                       nullptr, stream);
+                       nullptr, st);
 }
 
 float World::warm_sigma() const {
@@ -786,7 +801,7 @@ float World::warm_sigma() const {
   return std::max(s, 1e-12f);
 }
 
-void World::cg_solve(Cloth& c, float rel_tol, bool first) {
+void World::cg_solve(Cloth& c, float rel_tol, bool first, cudaStream_t st) {
   CgArgs a = c.dev.cg;
   a.first_solve = first ? 1 : 0;
   if (first && has_model && opt.learned_warm_start) a.x_alt = xpred.p + c.voff;
@@ -807,15 +822,15 @@ void World::cg_solve(Cloth& c, float rel_tol, bool first) {
   if (resident) stats.cg_resident_solves += 1;
   auto launch = [&]() {
     if (resident)
-      launch_cg_resident(a, c.dev.res_grid, stream);
+      launch_cg_resident(a, c.dev.res_grid, st);
     else
-      launch_cg(a, c.dev.cg_grid, stream);
+      launch_cg(a, c.dev.cg_grid, st);
   };
   if (opt.profile) {
     auto* ev = next_event_pair(events, events_used);
-    CUDA_CHECK(cudaEventRecord(ev->first, stream));
+    CUDA_CHECK(cudaEventRecord(ev->first, st));
     launch();
-    CUDA_CHECK(cudaEventRecord(ev->second, stream));
+    CUDA_CHECK(cudaEventRecord(ev->second, st));
   } else {
     launch();
   }
@@ -939,10 +954,36 @@ bool World::admm_solve() {
   bool contacts = coll_ && coll_->contact_count() > 0;
   for (int it = 0; it < g.max_inner_iteration; ++it) {
     if (it != 0) {
-      for (auto& c : cloths) {
-        if (it == 1) factorize(*c);
-        cg_solve(*c, rel, it == 1);
+      // Cloths are independent systems.  Those whose CG runs as one
+      // thread-block cluster (scheduled as a unit) go on their own streams,
+      // forked from and joined back into the world's stream; cooperative
+      // grids stay on the world's stream, one after another.
+      std::vector<int> forked;
+      for (int k = 0; k < (int)cloths.size(); ++k) {
+        const ClothDev& d = cloths[k]->dev;
+        const bool resident = d.res_grid != 0 && opt.cg_form != 1;
+        if (cloths.size() > 1 && (resident ? d.res_grid < 0 : d.cg_grid < 0)) forked.push_back(k);
       }
+      if (!forked.empty()) {
+        ensure_cloth_streams(cloths.size());
+        CUDA_CHECK(cudaEventRecord(fork_ev_, st));
+      }
+      size_t f = 0;
+      for (int k = 0; k < (int)cloths.size(); ++k) {
+        Cloth& c = *cloths[k];
+        cudaStream_t cs = st;
+        if (f < forked.size() && forked[f] == k) {
+          cs = cloth_streams_[k];
+          CUDA_CHECK(cudaStreamWaitEvent(cs, fork_ev_, 0));
+        }
+        if (it == 1) factorize(c, cs);
+        cg_solve(c, rel, it == 1, cs);
+        if (cs != st) {
+          CUDA_CHECK(cudaEventRecord(cloth_done_[k], cs));
+          ++f;
+        }
+      }
+      for (int k : forked) CUDA_CHECK(cudaStreamWaitEvent(st, cloth_done_[k], 0));
       if (it == 1 && opt.capture_samples && warm_first_) {
         warm_target(nv_total, x.p, ypred.p, 1.0f / warm_sigma(), warm_tgt.p, st);
         samples_valid = true;

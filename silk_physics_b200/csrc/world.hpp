@@ -244,8 +244,12 @@ class World {
   void build_cloth_device(Cloth& c);
   void build_resident_layout(Cloth& c);
   void upload_pins();
-  void factorize(Cloth& c);
-  void cg_solve(Cloth& c, float rel_tol, bool first);
+  void factorize(Cloth& c, cudaStream_t st);
+  void cg_solve(Cloth& c, float rel_tol, bool first, cudaStream_t st);
+  void ensure_cloth_streams(size_t n);
+  std::vector<cudaStream_t> cloth_streams_;  // per-cloth CG streams (multi-cloth worlds)
+  std::vector<cudaEvent_t> cloth_done_;
+  cudaEvent_t fork_ev_ = nullptr;
   bool warm_active() const { return (has_model && opt.learned_warm_start) || opt.capture_samples; }
   float warm_sigma() const;
   bool admm_solve();  // false on divergence

@@ -187,3 +187,40 @@ def test_resident_and_streaming_forms_against_oracle(oracle, s):
     print(f"s={s}: CG iterations resident {ir} streaming {is_}, resident solves {nres}")
     assert nres > 0 and nstr == 0
     assert all(abs(a - b) <= 0.05 * b for a, b in zip(ir, is_))
+
+
+def test_two_cloths_concurrent_cg_against_oracle(oracle):
+    """Two pinned sheets of different sizes in one world: their CG solves run
+    concurrently on per-cloth streams (each a thread-block cluster); both
+    stay within the FP32 parity bound of the FP64 oracle after two steps."""
+    sheets = [(24, 11, 0.0), (32, 12, 2.0)]
+    g = dict(max_inner_iteration=10, admm_abs_tol=0.0, admm_rel_tol=0.0,
+             fixed_linear_rel_tol=1e-6)
+    w = N.World()
+    assert w.init()
+    assert w.set_global_config(N.GlobalConfig(max_inner_iteration=10, admm_abs_tol=0.0,
+                                              admm_rel_tol=0.0))
+    assert w.set_solver_options(N.SolverOptions(fixed_linear_rel_tol=1e-6))
+    o32 = oracle.OracleWorld(config=g)
+    o64 = oracle.OracleWorld(fp64=True, config=g)
+    hs = []
+    for s, seed, x0 in sheets:
+        V, F = S.grid_sheet(s, jitter=1e-4, seed=seed, center=(x0, 0.0))
+        P = S.top_corner_pins(s)
+        r, h = w.add_cloth(N.ClothConfig(), NO_COLLISION, V, F, P)
+        assert r
+        perm, offs = w.cloth_partition(h, len(V))
+        h32 = o32.add_cloth(V, F, P, perm, offs, collision=(0, 0, 0, 0.3, 0.3))
+        h64 = o64.add_cloth(V, F, P, perm, offs, collision=(0, 0, 0, 0.3, 0.3))
+        hs.append((h, h32, h64, V))
+    for _ in range(2):
+        assert w.solver_step(), w
+        assert o32.step() == 0 and o64.step() == 0
+    for h, h32, h64, V in hs:
+        x = np.zeros(V.size, np.float32)
+        assert w.get_cloth_position(h, x)
+        xg = x.reshape(-1, 3).astype(np.float64)
+        e3264 = np.abs(o32.position(h32) - o64.position(h64)).max()
+        eg64 = np.abs(xg - o64.position(h64)).max()
+        print(f"cloth {h}: |gpu-o64| {eg64:.2e} |o32-o64| {e3264:.2e}")
+        assert eg64 <= max(3.0 * e3264, 2e-5)
