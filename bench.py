@@ -64,12 +64,12 @@ def scene_c3(seed=1237):
 
 
 def timed_variant(N, torch, stream, flush, V, F, SV, SF, cg_rel_tol, bf16, learned,
-                  prelude, steps):
+                  prelude, steps, extrap=False):
     """Steps/s and CG statistics of one solver variant on one scene: `prelude`
     untimed steps, then `steps` steps timed with CUDA events (L2 flushed
     between steps)."""
     opts = N.SolverOptions(fixed_linear_rel_tol=cg_rel_tol, profile=True, mas_bf16=bf16,
-                           learned_warm_start=learned)
+                           learned_warm_start=learned, admm_extrapolated_start=extrap)
     w, h, _ = make_world(stream.cuda_stream, opts, V, F, SV, SF)
     if learned:
         from silk_physics_b200 import learned as L
@@ -80,7 +80,7 @@ def timed_variant(N, torch, stream, flush, V, F, SV, SF, cg_rel_tol, bf16, learn
         r = w.solver_step()
         assert r, r.to_string()
     w.profile(reset=True)
-    ms, admm, cg, solves, first, taken, outer = 0.0, 0, 0, 0, 0, 0, 0
+    ms, admm, cg, solves, first, taken, outer, ext = 0.0, 0, 0, 0, 0, 0, 0, 0
     for k in range(steps):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(stream):
@@ -97,6 +97,7 @@ def timed_variant(N, torch, stream, flush, V, F, SV, SF, cg_rel_tol, bf16, learn
         solves += st.cg_solves
         first += st.cg_first_solve_iterations
         taken += st.learned_starts
+        ext += st.extrapolated_starts
         outer += st.outer_iterations
     prof = w.profile(reset=True)
     return {"value": round(steps / (ms / 1e3), 4), "ms_per_step": round(ms / steps, 3),
@@ -108,7 +109,8 @@ def timed_variant(N, torch, stream, flush, V, F, SV, SF, cg_rel_tol, bf16, learn
             "admm_iterations_per_step": admm / steps,
             "cg_iterations_per_solve": round(cg / max(solves, 1), 2),
             "first_solve_cg_iterations_per_outer": round(first / max(outer, 1), 2),
-            "learned_starts_taken": taken, "outer_iterations": outer}
+            "learned_starts_taken": taken, "extrapolated_starts_taken": ext,
+            "outer_iterations": outer}
 
 
 def dist_env():
@@ -304,19 +306,25 @@ def run_ours(args) -> None:
     # sheet (plain FP32 vs learned + BF16), each from its own fresh world.
     variants = {}
     if args.variants and MODEL.exists():
-        for name, bf16, learned in (("c2_bf16", True, False), ("c2_learned_bf16", True, True)):
+        for name, bf16, learned, extrap in (("c2_bf16", True, False, False),
+                                            ("c2_learned_bf16", True, True, False),
+                                            ("c2_extrapolated", False, False, True),
+                                            ("c2_learned_extrapolated_bf16", True, True, True)):
             variants[name] = timed_variant(N, torch, stream, flush, V, F, SV, SF,
                                            args.cg_rel_tol, bf16, learned,
-                                           args.prelude + args.warmup, args.variant_steps)
+                                           args.prelude + args.warmup, args.variant_steps,
+                                           extrap)
         V3, F3, SV3, SF3 = scene_c3()
         c3 = {"workload": C3_WORKLOAD, "vertices": int(len(V3)), "faces": int(len(F3)),
               "prelude_steps": args.c3_prelude, "steps": args.c3_steps}
-        for name, bf16, learned in (("plain_fp32", False, False), ("bf16", True, False),
-                                    ("learned_bf16", True, True)):
+        for name, bf16, learned, extrap in (("plain_fp32", False, False, False),
+                                            ("bf16", True, False, False),
+                                            ("learned_bf16", True, True, False),
+                                            ("learned_extrapolated_bf16", True, True, True)):
             c3[name] = timed_variant(N, torch, stream, flush, V3, F3, SV3, SF3, args.cg_rel_tol,
-                                     bf16, learned, args.c3_prelude, args.c3_steps)
-        c3["learned_bf16_over_plain"] = round(c3["learned_bf16"]["value"] /
-                                              c3["plain_fp32"]["value"], 3)
+                                     bf16, learned, args.c3_prelude, args.c3_steps, extrap)
+        for name in ("learned_bf16", "learned_extrapolated_bf16"):
+            c3[name + "_over_plain"] = round(c3[name]["value"] / c3["plain_fp32"]["value"], 3)
         variants["c3"] = c3
 
     # End to end through the public API with host buffers, on the same steps:

@@ -94,6 +94,10 @@ typedef struct {
   int32_t capture_samples;    /* 1: record warm-start training samples */
   int32_t contact_gs_form;    /* 0: single-block contact Gauss-Seidel where the
                                  contacts fit it, else grid; 1: grid always */
+  int32_t admm_extrapolated_start; /* 1: offer 2 x_k - x_(k-1) (the last two ADMM
+                                 iterates of the same ADMM solve) as the start
+                                 of each later CG solve; the plain start's
+                                 residual stays the stopping reference */
 } silk_solver_options;
 
 /* CUDA-event timing of the persistent CG kernel over the steps since the
@@ -131,7 +135,8 @@ typedef struct {
   int32_t cg_first_solve_iterations; /* iterations of each outer iteration's
                                         first CG solve, summed */
   int32_t learned_starts;      /* first solves that started from the model */
-  int32_t reserved[3];
+  int32_t extrapolated_starts; /* solves that started from the extrapolation */
+  int32_t reserved[2];
 } silk_step_stats;
 
 /* --- World lifetime (silk.hpp:92-100) ---------------------------------- */

@@ -421,7 +421,7 @@ __device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm
         a.r[i] = make_float4(r0.x + w * (ra.x - r0.x), r0.y + w * (ra.y - r0.y),
                              r0.z + w * (ra.z - r0.z), 0.f);
       }
-      if (blockIdx.x == 0 && threadIdx.x == 0 && a.stats) atomicAdd(a.stats + 3, 1);
+      if (blockIdx.x == 0 && threadIdx.x == 0 && a.stats) atomicAdd(a.stats + a.alt_stat, 1);
       if (!bar.sync()) return mark_fail(a);
     }
   }
@@ -820,7 +820,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     if (w > 0.0f) {
       x = make_float3(x.x + w * (xa.x - x.x), x.y + w * (xa.y - x.y), x.z + w * (xa.z - x.z));
       r = make_float3(r.x + w * (ra.x - r.x), r.y + w * (ra.y - r.y), r.z + w * (ra.z - r.z));
-      if (k == 0 && tid == 0 && a.stats) atomicAdd(a.stats + 3, 1);
+      if (k == 0 && tid == 0 && a.stats) atomicAdd(a.stats + a.alt_stat, 1);
     }
   }
 

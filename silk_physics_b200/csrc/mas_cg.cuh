@@ -65,12 +65,13 @@ struct CgArgs {
   int max_iter = 1000;
   int* result = nullptr;  // [iterations, status]
   int* stats = nullptr;   // accumulated [iterations, solves, first-solve iterations,
-                          // learned starts taken]
-  // Alternative start (learned warm start; null = none): the CG starts from
-  // x + w (x_alt - x) with the residual-minimising w >= 0 (w = 0: the plain
-  // start), while the stopping rule keeps the residual of x as rr0 (the plain
-  // start judges the alternative).
+                          // learned starts taken, extrapolated starts taken, -]
+  // Alternative start (learned warm start or ADMM extrapolation; null =
+  // none): the CG starts from x + w (x_alt - x) with the residual-minimising
+  // w >= 0 (w = 0: the plain start), while the stopping rule keeps the
+  // residual of x as rr0 (the plain start judges the alternative).
   const float4* x_alt = nullptr;
+  int alt_stat = 3;       // stats slot counting the alternative starts taken
   int first_solve = 0;    // count this solve's iterations in stats[2]
   float* result_rr = nullptr;
   // Resident form: one block of kResThreads per first-level coarse bank (32
@@ -87,6 +88,8 @@ struct CgArgs {
   long long* trace = nullptr;
 };
 
+// Per-cloth CG statistics words (CgArgs::stats).
+constexpr int kCgStats = 6;
 constexpr int kCgTraceIters = 64;
 constexpr int kCgTraceSlots = 16;
 constexpr int kCgTraceLen = 8 + kCgTraceIters * kCgTraceSlots;

@@ -369,6 +369,20 @@ __global__ void velocity_kernel(int nv, float dt, const float4* a,
   v[i] = make_float4((p.x - q.x) / dt, (p.y - q.y) / dt, (p.z - q.z) / dt, 0.f);
 }
 
+// Extrapolated CG start from the last two ADMM iterates of one ADMM solve:
+// ext = 2 x_k - x_(k-1) when prev holds x_(k-1) (valid), then prev = x_k.
+__global__ void extrapolate_kernel(int nv, int valid, const float4* x, float4* prev,
+                                   float4* ext) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  float4 p = x[i];
+  if (valid) {
+    float4 q = prev[i];
+    ext[i] = make_float4(p.x + (p.x - q.x), p.y + (p.y - q.y), p.z + (p.z - q.z), 0.f);
+  }
+  prev[i] = p;
+}
+
 // out = w * a + (1 - w) * b with the second term in double (main_loop.cu:111).
 __global__ void mix_kernel(int nv, float w, const float4* a, float4* b) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -436,6 +450,12 @@ void launch_predict(int nv, float dt, float4 acc, const float4* x,
 void launch_velocity(int nv, float dt, const float4* a, const float4* b,
                      float4* v, cudaStream_t st) {
   velocity_kernel<<<div_up(nv, THREADS), THREADS, 0, st>>>(nv, dt, a, b, v);
+  SILK_LAUNCHED();
+}
+
+void launch_extrapolate(int nv, bool valid, const float4* x, float4* prev, float4* ext,
+                        cudaStream_t st) {
+  extrapolate_kernel<<<div_up(nv, THREADS), THREADS, 0, st>>>(nv, valid ? 1 : 0, x, prev, ext);
   SILK_LAUNCHED();
 }
 

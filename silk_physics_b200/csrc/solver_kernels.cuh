@@ -95,6 +95,9 @@ void launch_admm_finalize(const AdmmFinalizeArgs& a, cudaStream_t st);
 void launch_enforce(const SolverView& s, cudaStream_t st);
 void launch_predict(int nv, float dt, float4 acc, const float4* x,
                     const float4* v, float4* out, cudaStream_t st);
+// ext = 2 x - prev where valid, then prev = x (ADMM-extrapolated CG start).
+void launch_extrapolate(int nv, bool valid, const float4* x, float4* prev, float4* ext,
+                        cudaStream_t st);
 void launch_velocity(int nv, float dt, const float4* a, const float4* b,
                      float4* v, cudaStream_t st);
 void launch_mix(int nv, float w, const float4* a, float4* b, cudaStream_t st);

@@ -549,7 +549,7 @@ void World::build_cloth_device(Cloth& c) {
   d.barrier.zero(st);
   d.result.alloc(2);
   d.result_rr.alloc(1);
-  d.stats.alloc(4);
+  d.stats.alloc(kCgStats);
   d.stats.zero(st);
   // Compulsory DRAM bytes of one CG iteration: off-diagonal entries (8 B),
   // per row Ldiag + dynamic diagonal + p read + Ap write (40 B) in the SpMV
@@ -804,7 +804,13 @@ float World::warm_sigma() const {
 void World::cg_solve(Cloth& c, float rel_tol, bool first, cudaStream_t st) {
   CgArgs a = c.dev.cg;
   a.first_solve = first ? 1 : 0;
-  if (first && has_model && opt.learned_warm_start) a.x_alt = xpred.p + c.voff;
+  if (first && has_model && opt.learned_warm_start) {
+    a.x_alt = xpred.p + c.voff;
+    a.alt_stat = 3;
+  } else if (!first && admm_ext_ready) {
+    a.x_alt = admm_ext.p + c.voff;
+    a.alt_stat = 4;
+  }
   a.dyn = lhs.p + c.voff;
   a.b = rhs.p + c.voff;
   a.x = x.p + c.voff;
@@ -952,8 +958,20 @@ bool World::admm_solve() {
   fa.ctl = ctl.p;
   fa.cg_fail = cg_fail.p;
   bool contacts = coll_ && coll_->contact_count() > 0;
+  admm_ext_ready = false;
   for (int it = 0; it < g.max_inner_iteration; ++it) {
     if (it != 0) {
+      // Extrapolated start: from the third solve on, 2 x_k - x_(k-1) of the
+      // last two iterates of this ADMM solve (the first solve starts from the
+      // outer state, whose step to x_1 is not an ADMM iterate difference).
+      if (opt.admm_extrapolated_start && it >= 2) {
+        if (admm_prev.n < (size_t)nv_total) {
+          admm_prev.alloc(nv_total);
+          admm_ext.alloc(nv_total);
+        }
+        launch_extrapolate(nv_total, it >= 3, x.p, admm_prev.p, admm_ext.p, st);
+        admm_ext_ready = it >= 3;
+      }
       // Cloths are independent systems.  Those whose CG runs as one
       // thread-block cluster (scheduled as a unit) go on their own streams,
       // forked from and joined back into the world's stream; cooperative
@@ -1117,21 +1135,23 @@ silk_status World::solver_step() {
     // Step history of the warm-start features.
     CUDA_CHECK(cudaMemcpyAsync(hist2.p, hist1.p, nv * sizeof(float4), cudaMemcpyDeviceToDevice, st));
     CUDA_CHECK(cudaMemcpyAsync(hist1.p, step_start.p, nv * sizeof(float4), cudaMemcpyDeviceToDevice, st));
-    std::vector<int> cgs(4 * cloths.size());
+    std::vector<int> cgs(kCgStats * cloths.size());
     for (size_t k = 0; k < cloths.size(); ++k)
-      CUDA_CHECK(cudaMemcpyAsync(&cgs[4 * k], cloths[k]->dev.stats.p, 4 * sizeof(int),
-                                 cudaMemcpyDeviceToHost, st));
+      CUDA_CHECK(cudaMemcpyAsync(&cgs[kCgStats * k], cloths[k]->dev.stats.p,
+                                 kCgStats * sizeof(int), cudaMemcpyDeviceToHost, st));
     sync();
     for (size_t k = 0; k < cloths.size(); ++k) {
-      stats.cg_iterations += cgs[4 * k];
-      stats.cg_solves += cgs[4 * k + 1];
-      stats.cg_first_solve_iterations += cgs[4 * k + 2];
-      stats.learned_starts += cgs[4 * k + 3];
+      const int* q = &cgs[kCgStats * k];
+      stats.cg_iterations += q[0];
+      stats.cg_solves += q[1];
+      stats.cg_first_solve_iterations += q[2];
+      stats.learned_starts += q[3];
+      stats.extrapolated_starts += q[4];
       if (opt.profile) {
         double bpi = opt.mas_bf16 ? cloths[k]->dev.bytes_per_iter_bf16
                                   : cloths[k]->dev.bytes_per_iter_fp32;
-        prof.cg_algorithmic_bytes += bpi * (cgs[4 * k] + cgs[4 * k + 1]);
-        prof.cg_iterations += cgs[4 * k];
+        prof.cg_algorithmic_bytes += bpi * (q[0] + q[1]);
+        prof.cg_iterations += q[0];
       }
     }
     if (opt.profile) {

@@ -216,6 +216,9 @@ class World {
   DevBuf<float> mlp_params, mlp_out, warm_feat, warm_tgt;
   DevBuf<uint32_t> mlp_frag;
   DevBuf<float4> hist1, hist2, step_start, ypred, xpred;
+  // ADMM-extrapolated CG start: the previous ADMM iterate and 2 x_k - x_(k-1).
+  DevBuf<float4> admm_prev, admm_ext;
+  bool admm_ext_ready = false;
   DevBuf<int> ring_off, ring;
   bool has_model = false;
   bool samples_valid = false;

@@ -77,7 +77,7 @@ class _SolverOptionsC(C.Structure):
     _fields_ = [("fixed_linear_rel_tol", C.c_float), ("cg_max_iter", C.c_int32),
                 ("mas_bf16", C.c_int32), ("profile", C.c_int32), ("cg_form", C.c_int32),
                 ("learned_warm_start", C.c_int32), ("capture_samples", C.c_int32),
-                ("contact_gs_form", C.c_int32)]
+                ("contact_gs_form", C.c_int32), ("admm_extrapolated_start", C.c_int32)]
 
 
 class _ProfileC(C.Structure):
@@ -97,7 +97,7 @@ class _StepStatsC(C.Structure):
                 ("min_toi", C.c_float), ("broadphase_candidates", C.c_int32),
                 ("kernel_launches", C.c_int64), ("cg_resident_solves", C.c_int32),
                 ("cg_first_solve_iterations", C.c_int32), ("learned_starts", C.c_int32),
-                ("reserved", C.c_int32 * 3)]
+                ("extrapolated_starts", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 @dataclass
@@ -162,6 +162,7 @@ class SolverOptions:
     learned_warm_start: bool = False  # offer the loaded model's first-solve start
     capture_samples: bool = False     # record warm-start training samples
     contact_gs_form: int = 0          # 0: single-block Gauss-Seidel where possible; 1: grid
+    admm_extrapolated_start: bool = False  # offer 2 x_k - x_(k-1) as later CG starts
 
     def to_c(self) -> _SolverOptionsC:
         o = _SolverOptionsC()
@@ -173,6 +174,7 @@ class SolverOptions:
         o.learned_warm_start = int(self.learned_warm_start)
         o.capture_samples = int(self.capture_samples)
         o.contact_gs_form = int(self.contact_gs_form)
+        o.admm_extrapolated_start = int(self.admm_extrapolated_start)
         return o
 
 
@@ -192,6 +194,7 @@ class StepStats:
     cg_resident_solves: int = 0
     cg_first_solve_iterations: int = 0
     learned_starts: int = 0
+    extrapolated_starts: int = 0
 
 
 _F32P = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
