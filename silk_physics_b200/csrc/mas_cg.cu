@@ -572,7 +572,7 @@ struct ResShared {
   float Mf[kResWarps][kPacked];
   float M1[kPacked];
   float Mc[kResCoarseBanks][kPacked];
-  float4 pl[kResThreads];
+  float4 pl[kResThreads + kResHalo];  // the block's slots, then its halo
   float4 r1[32];
   float4 z1[32];
   float4 rc[kResCoarseBanks * BANK];
@@ -795,10 +795,22 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
       cm[3] = c.w;
     }
   }
+  // Halo: thread i < nhalo gathers halo vertex i of the block into slot
+  // kResThreads + i before each product (one round trip, all loads in flight).
+  int hcol = -1;
+  if (a.halo_off) {
+    const int h0 = a.halo_off[k], nh = a.halo_off[k + 1] - h0;
+    if (tid < nh) hcol = a.halo_col[h0 + tid];
+  }
+  auto gather_halo = [&](const float4* ex) {
+    if (hcol >= 0) s.pl[kResThreads + tid] = ldcg4(ex + hcol);
+    __syncthreads();
+  };
   // Publish x for r = b - A x.
   s.pl[tid] = make_float4(x.x, x.y, x.z, 0.f);
   if (own) a.p[v] = make_float4(x.x, x.y, x.z, 0.f);
   if (!bar.sync()) return fail();
+  gather_halo(a.p);
   float3 r;
   {
     float3 y = res_row(a, s, a.p, rptr, rw, lane, d, x);
@@ -818,6 +830,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     s.pl[tid] = make_float4(xa.x, xa.y, xa.z, 0.f);
     if (own) a.Ap[v] = make_float4(xa.x, xa.y, xa.z, 0.f);
     if (!bar.sync()) return fail();
+    gather_halo(a.Ap);
     float3 ra;
     {
       float3 y = res_row(a, s, a.Ap, rptr, rw, lane, d, xa);
@@ -1016,6 +1029,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     tr.stamp(iter, 1);
     // B: Ap and p.Ap.
     {
+      gather_halo(a.p);
       Ap = res_row(a, s, a.p, rptr, rw, lane, d, p);
       if (!own) Ap = make_float3(0.f, 0.f, 0.f);
       tr.stamp(iter, 2);

@@ -80,6 +80,9 @@ struct CgArgs {
   const int* rb_ptr = nullptr;  // per fine bank: first entry of its ELL slice
   const int* rb_w = nullptr;    // per fine bank: slice width
   const int2* rent = nullptr;   // (column, value bits); column < 0: slot -1-c of the block
+                                // (slots >= kResThreads: the block's halo)
+  const int* halo_off = nullptr;  // per block: first entry of its halo in halo_col
+  const int* halo_col = nullptr;  // halo vertices (outside the block, read by its rows)
   int* fail = nullptr;          // set to 1 when a barrier wait gives up
   // Optional phase trace of block 0 (null = off): [0] globaltimer and [1]
   // clock64 at entry, [2] and [3] at exit, [4] traced iterations, [5] kernel
@@ -90,6 +93,9 @@ struct CgArgs {
 
 // Per-cloth CG statistics words (CgArgs::stats).
 constexpr int kCgStats = 6;
+// Halo slots per block of the resident CG kernel (shared memory after the
+// block's own kResThreads slots).
+constexpr int kResHalo = 1024;
 constexpr int kCgTraceIters = 64;
 constexpr int kCgTraceSlots = 16;
 constexpr int kCgTraceLen = 8 + kCgTraceIters * kCgTraceSlots;

@@ -376,6 +376,78 @@ SolverView World::view() {
 // above fit the shared memory of a block.  The off-diagonal part of L is
 // re-sliced per fine bank; a column inside the block is stored as -1 - slot,
 // and the entries from other blocks come first in each row.
+// Order of the entries of one bank's rows in its ELL slice (round j of lane
+// l at out[j * BANK + l]).  In round j the 32 lanes of the warp gather p from
+// shared memory (float4 per slot), and a 128-bit shared load is served per
+// quarter-warp: two lanes of a quarter whose slots differ but share slot % 8
+// (the 16-byte bank group) cost an extra pass.  Each quarter's entries are
+// placed round by round, the lanes with the least slack first, each taking
+// an entry whose bank group is still free in the round (or whose slot is
+// already read, a broadcast), else an entry outside the block (a global
+// load, no shared-memory access), else, when it has no slack left, any
+// entry.  Padding entries (value 0) read a slot another lane of the quarter
+// reads.  Entries outside the block have column >= 0; the kernel reads slot
+// -1 - column otherwise.  A row's terms are summed in round order.
+static void schedule_bank_rows(std::vector<std::vector<int2>>& rows, int width, int slot0,
+                               int2* out) {
+  for (int q = 0; q < BANK / 8; ++q) {
+    std::vector<std::vector<int2>> rem(8);
+    for (int l = 0; l < 8; ++l) rem[l] = rows[8 * q + l];
+    for (int j = 0; j < width; ++j) {
+      const int left = width - j;
+      int order[8];
+      for (int l = 0; l < 8; ++l) order[l] = l;
+      std::stable_sort(order, order + 8, [&](int a, int b) {
+        return left - (int)rem[a].size() < left - (int)rem[b].size();
+      });
+      int group_slot[8];  // slot read in this round per bank group, -1: free
+      for (int g = 0; g < 8; ++g) group_slot[g] = -1;
+      bool pad[8] = {false, false, false, false, false, false, false, false};
+      for (int oi = 0; oi < 8; ++oi) {
+        const int l = order[oi];
+        auto& r = rem[l];
+        if (r.empty()) {
+          pad[l] = true;
+          continue;
+        }
+        int pick = -1;
+        for (int e = 0; e < (int)r.size() && pick < 0; ++e)
+          if (r[e].x < 0) {
+            int slot = -1 - r[e].x;
+            int g = slot & 7;
+            if (group_slot[g] < 0 || group_slot[g] == slot) pick = e;
+          }
+        if (pick < 0)
+          for (int e = 0; e < (int)r.size() && pick < 0; ++e)
+            if (r[e].x >= 0) pick = e;
+        if (pick < 0 && (int)r.size() >= left) pick = 0;
+        if (pick < 0) {
+          pad[l] = true;
+          continue;
+        }
+        int2 e = r[pick];
+        r.erase(r.begin() + pick);
+        if (e.x < 0) {
+          int slot = -1 - e.x;
+          if (group_slot[slot & 7] < 0) group_slot[slot & 7] = slot;
+        }
+        out[j * BANK + 8 * q + l] = e;
+      }
+      for (int l = 0; l < 8; ++l) {
+        if (!pad[l]) continue;
+        int slot = slot0 + 8 * q + l;
+        for (int g = 0; g < 8; ++g)
+          if (group_slot[g] >= 0) {
+            slot = group_slot[g];
+            break;
+          }
+        if (group_slot[slot & 7] < 0) group_slot[slot & 7] = slot;
+        out[j * BANK + 8 * q + l] = make_int2(-1 - slot, 0);
+      }
+    }
+  }
+}
+
 void World::build_resident_layout(Cloth& c) {
   const ClothSetup& S = *c.setup;
   ClothDev& d = c.dev;
@@ -408,36 +480,65 @@ void World::build_resident_layout(Cloth& c) {
     width[b] = w;
     ptr[b + 1] = ptr[b] + BANK * w;
   }
-  std::vector<int2> ent(std::max(ptr[nbank0], 1));
-  for (int b = 0; b < nbank0; ++b) {
-    const int k = b / BANK;
-    for (int lane = 0; lane < BANK; ++lane) {
-      const int own_slot = (b - k * BANK) * BANK + lane;
-      const int v = S.part_offsets[b] + lane;
-      std::vector<int2> far, near;
-      if (v < S.part_offsets[b + 1])
+  // Halo of each block: the vertices outside it that its rows read, gathered
+  // into shared memory once per product (at most kResHalo; any further ones
+  // are read from global memory by the rows themselves).
+  std::vector<int> halo_off(nblocks + 1, 0), halo_col;
+  std::vector<int> halo_slot(nv, -1), halo_mark(nv, -1);
+  for (int k = 0; k < nblocks; ++k) {
+    halo_off[k] = (int)halo_col.size();
+    for (int bb = k * BANK; bb < std::min(nbank0, (k + 1) * BANK); ++bb)
+      for (int v = S.part_offsets[bb]; v < S.part_offsets[bb + 1]; ++v)
         for (int q = S.Lrows[v]; q < S.Lrows[v + 1]; ++q) {
           int col = S.Lcols[q];
-          if (col == v) continue;
-          float val = (float)S.Lvals[q];
-          int bits;
-          std::memcpy(&bits, &val, 4);
-          int cb = part_of[col];
-          if (cb / BANK == k)
-            near.push_back(make_int2(-1 - ((cb - k * BANK) * BANK + lane_of[col]), bits));
-          else
-            far.push_back(make_int2(col, bits));
+          if (part_of[col] / BANK == k || halo_mark[col] == k) continue;
+          if ((int)halo_col.size() - halo_off[k] >= kResHalo) continue;
+          halo_mark[col] = k;
+          halo_col.push_back(col);
         }
-      int j = 0;
-      for (auto& e : far) ent[ptr[b] + BANK * j++ + lane] = e;
-      for (auto& e : near) ent[ptr[b] + BANK * j++ + lane] = e;
-      for (; j < width[b]; ++j) ent[ptr[b] + BANK * j + lane] = make_int2(-1 - own_slot, 0);
+  }
+  halo_off[nblocks] = (int)halo_col.size();
+  std::vector<int2> ent(std::max(ptr[nbank0], 1));
+  std::vector<std::vector<int2>> row(BANK);
+  int halo_block = -1;
+  for (int b = 0; b < nbank0; ++b) {
+    const int k = b / BANK;
+    if (k != halo_block) {
+      if (halo_block >= 0)
+        for (int i = halo_off[halo_block]; i < halo_off[halo_block + 1]; ++i)
+          halo_slot[halo_col[i]] = -1;
+      for (int i = halo_off[k]; i < halo_off[k + 1]; ++i)
+        halo_slot[halo_col[i]] = kResThreads + i - halo_off[k];
+      halo_block = k;
     }
+    for (int lane = 0; lane < BANK; ++lane) {
+      row[lane].clear();
+      const int v = S.part_offsets[b] + lane;
+      if (v >= S.part_offsets[b + 1]) continue;
+      for (int q = S.Lrows[v]; q < S.Lrows[v + 1]; ++q) {
+        int col = S.Lcols[q];
+        if (col == v) continue;
+        float val = (float)S.Lvals[q];
+        int bits;
+        std::memcpy(&bits, &val, 4);
+        int cb = part_of[col];
+        if (cb / BANK == k)
+          row[lane].push_back(make_int2(-1 - ((cb - k * BANK) * BANK + lane_of[col]), bits));
+        else if (halo_slot[col] >= 0)
+          row[lane].push_back(make_int2(-1 - halo_slot[col], bits));
+        else
+          row[lane].push_back(make_int2(col, bits));
+      }
+    }
+    schedule_bank_rows(row, width[b], (b - k * BANK) * BANK, &ent[ptr[b]]);
   }
   cudaStream_t st = stream;
   d.rb_ptr.upload(ptr, st);
   d.rb_w.upload(width, st);
   d.rent.upload(ent, st);
+  d.res_halo_off.upload(halo_off, st);
+  if (halo_col.empty()) halo_col.push_back(0);
+  d.res_halo_col.upload(halo_col, st);
   d.res_blocks = nblocks;
   d.res_grid = grid;
 }
@@ -607,6 +708,8 @@ void World::build_cloth_device(Cloth& c) {
     a.rb_ptr = d.rb_ptr.p;
     a.rb_w = d.rb_w.p;
     a.rent = d.rent.p;
+    a.halo_off = d.res_halo_off.p;
+    a.halo_col = d.res_halo_col.p;
   }
   a.partials = d.partials.p;
   a.coarse_partial = d.coarse_partial.p;
