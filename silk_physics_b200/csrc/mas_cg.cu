@@ -573,6 +573,7 @@ struct ResShared {
   float M1[kPacked];
   float Mc[kResCoarseBanks][kPacked];
   float4 pl[kResThreads + kResHalo];  // the block's slots, then its halo
+  int4 hcm[kResHalo];                 // coarse nodes of the halo vertices (cmap)
   float4 r1[32];
   float4 z1[32];
   float4 rc[kResCoarseBanks * BANK];
@@ -802,6 +803,12 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     const int h0 = a.halo_off[k], nh = a.halo_off[k + 1] - h0;
     if (tid < nh) hcol = a.halo_col[h0 + tid];
   }
+  // With every off-block column in the halo, the block computes p at its
+  // halo vertices itself (owner's two-level z, published before the barrier
+  // that ends phase C, plus the upper levels every block holds), so p needs
+  // no publication barrier.
+  const bool halo_p = a.halo_full != 0;
+  if (halo_p && hcol >= 0 && has1) s.hcm[tid] = a.cmap[hcol];
   auto gather_halo = [&](const float4* ex) {
     if (hcol >= 0) s.pl[kResThreads + tid] = ldcg4(ex + hcol);
     __syncthreads();
@@ -858,7 +865,8 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
 
   // Phase C body: fine and first-level MAS of r, restriction to level 2,
   // partials (r.z, r.r) of this block.
-  float3 z0, p = make_float3(0.f, 0.f, 0.f), Ap = p;
+  float3 z0, zl, p = make_float3(0.f, 0.f, 0.f), Ap = p;
+  float4 hz = make_float4(0.f, 0.f, 0.f, 0.f);  // two-level z of halo vertex tid
   auto mas_fine = [&]() {
     double rr = own ? (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z : 0.0;
     if (!bank_ok) {
@@ -898,6 +906,16 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     tr.stamp(iter, 7);
     const double v2[2] = {rz, rr};
     res_block_sum<2, false>(v2, s, part);
+    // Two-level z of this vertex (s.z1 is complete after the block sum's
+    // barrier), published for the blocks whose halo holds the vertex.
+    zl = z0;
+    if (own && has1) {
+      float4 q = s.z1[warp];
+      zl.x += q.x;
+      zl.y += q.y;
+      zl.z += q.z;
+    }
+    if (halo_p && own) a.z0[v] = make_float4(zl.x, zl.y, zl.z, 0.f);
     tr.stamp(iter, 8);
   };
   // Phase A head: totals and the redundant coarse levels >= 2.
@@ -971,26 +989,25 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
       rz += s.tot[0];
     }
   };
-  // Phase A tail: full preconditioned residual of this vertex.
-  auto mas_total = [&]() {
-    float3 z = z0;
-    if (own && has1) {
-      float4 q = s.z1[warp];
+  // Phase A tail: full preconditioned residual of a vertex from its
+  // two-level z and its coarse nodes (the same operations for a vertex of
+  // this block and for a halo vertex, so both give its owner's bits).
+  auto upper_z = [&](float3 z, const int (&c)[4]) {
+    int cb = 0;
+#pragma unroll
+    for (int l = 1; l < 4; ++l) {
+      if (l >= a.levels) break;
+      float4 q = s.zc[cb * BANK + c[l]];
       z.x += q.x;
       z.y += q.y;
       z.z += q.z;
-      int cb = 0;
-#pragma unroll
-      for (int l = 1; l < 4; ++l) {
-        if (l >= a.levels) break;
-        float4 c = s.zc[cb * BANK + cm[l]];
-        z.x += c.x;
-        z.y += c.y;
-        z.z += c.z;
-        cb += a.coarse[l].nbank;
-      }
+      cb += a.coarse[l].nbank;
     }
     return z;
+  };
+  auto mas_total = [&]() { return own && has1 ? upper_z(zl, cm) : zl; };
+  auto p_update = [&](float3 z, float3 po, float bt) {
+    return bt == 0.0f ? z : make_float3(z.x + bt * po.x, z.y + bt * po.y, z.z + bt * po.z);
   };
 
   // Every warp has finished reading pl in the residual rows before mas_fine
@@ -998,6 +1015,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
   __syncthreads();
   mas_fine();
   if (!bar.sync()) return fail();
+  if (halo_p && hcol >= 0) hz = ldcg4(a.z0 + hcol);
   double rz, rr;
   totals(rz, rr);
   iter = 0;
@@ -1015,21 +1033,36 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
   double beta = 0.0;
   int status = kCgMaxIter;
   while (true) {
-    // A tail: p = z + beta p, published.
+    // A tail: p = z + beta p, published (or, with halo_p, computed at the
+    // halo vertices by this block).
     {
-      float3 z = mas_total();
       const float bt = (float)beta;
-      p = bt == 0.0f ? z : make_float3(z.x + bt * p.x, z.y + bt * p.y, z.z + bt * p.z);
+      p = p_update(mas_total(), p, bt);
       if (!own) p = make_float3(0.f, 0.f, 0.f);
       s.pl[tid] = make_float4(p.x, p.y, p.z, 0.f);
-      if (own) a.p[v] = make_float4(p.x, p.y, p.z, 0.f);
+      if (!halo_p && own) a.p[v] = make_float4(p.x, p.y, p.z, 0.f);
+      if (halo_p && hcol >= 0) {
+        float3 zh = make_float3(hz.x, hz.y, hz.z);
+        if (has1) {
+          int4 c4 = s.hcm[tid];
+          const int c[4] = {c4.x, c4.y, c4.z, c4.w};
+          zh = upper_z(zh, c);
+        }
+        float4 po = s.pl[kResThreads + tid];
+        float3 ph = p_update(zh, make_float3(po.x, po.y, po.z), bt);
+        s.pl[kResThreads + tid] = make_float4(ph.x, ph.y, ph.z, 0.f);
+      }
     }
     tr.stamp(iter, 0);
-    if (!bar.sync()) return fail();
+    if (halo_p) {
+      __syncthreads();
+    } else if (!bar.sync()) {
+      return fail();
+    }
     tr.stamp(iter, 1);
     // B: Ap and p.Ap.
     {
-      gather_halo(a.p);
+      if (!halo_p) gather_halo(a.p);
       Ap = res_row(a, s, a.p, rptr, rw, lane, d, p);
       if (!own) Ap = make_float3(0.f, 0.f, 0.f);
       tr.stamp(iter, 2);
@@ -1051,6 +1084,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
       mas_fine();
     }
     if (!bar.sync()) return fail();
+    if (halo_p && hcol >= 0) hz = ldcg4(a.z0 + hcol);
     tr.stamp(iter, 9);
     // A head: totals, coarse levels, stopping rules.
     double rz_old = rz;

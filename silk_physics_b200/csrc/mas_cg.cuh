@@ -83,6 +83,7 @@ struct CgArgs {
                                 // (slots >= kResThreads: the block's halo)
   const int* halo_off = nullptr;  // per block: first entry of its halo in halo_col
   const int* halo_col = nullptr;  // halo vertices (outside the block, read by its rows)
+  int halo_full = 0;  // every off-block column of the resident rows is in its block's halo
   int* fail = nullptr;          // set to 1 when a barrier wait gives up
   // Optional phase trace of block 0 (null = off): [0] globaltimer and [1]
   // clock64 at entry, [2] and [3] at exit, [4] traced iterations, [5] kernel

@@ -485,6 +485,7 @@ void World::build_resident_layout(Cloth& c) {
   // are read from global memory by the rows themselves).
   std::vector<int> halo_off(nblocks + 1, 0), halo_col;
   std::vector<int> halo_slot(nv, -1), halo_mark(nv, -1);
+  bool halo_overflow = false;
   for (int k = 0; k < nblocks; ++k) {
     halo_off[k] = (int)halo_col.size();
     for (int bb = k * BANK; bb < std::min(nbank0, (k + 1) * BANK); ++bb)
@@ -492,7 +493,10 @@ void World::build_resident_layout(Cloth& c) {
         for (int q = S.Lrows[v]; q < S.Lrows[v + 1]; ++q) {
           int col = S.Lcols[q];
           if (part_of[col] / BANK == k || halo_mark[col] == k) continue;
-          if ((int)halo_col.size() - halo_off[k] >= kResHalo) continue;
+          if ((int)halo_col.size() - halo_off[k] >= kResHalo) {
+            halo_overflow = true;
+            continue;
+          }
           halo_mark[col] = k;
           halo_col.push_back(col);
         }
@@ -537,6 +541,7 @@ void World::build_resident_layout(Cloth& c) {
   d.rb_w.upload(width, st);
   d.rent.upload(ent, st);
   d.res_halo_off.upload(halo_off, st);
+  d.res_halo_full = !halo_overflow;
   if (halo_col.empty()) halo_col.push_back(0);
   d.res_halo_col.upload(halo_col, st);
   d.res_blocks = nblocks;
@@ -710,6 +715,7 @@ void World::build_cloth_device(Cloth& c) {
     a.rent = d.rent.p;
     a.halo_off = d.res_halo_off.p;
     a.halo_col = d.res_halo_col.p;
+    a.halo_full = d.res_halo_full ? 1 : 0;
   }
   a.partials = d.partials.p;
   a.coarse_partial = d.coarse_partial.p;

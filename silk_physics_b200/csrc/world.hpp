@@ -101,6 +101,7 @@ struct ClothDev {
   DevBuf<int> rb_ptr, rb_w;   // resident form: ELL slices per fine bank
   DevBuf<int2> rent;
   DevBuf<int> res_halo_off, res_halo_col;  // resident form: per-block halo vertices
+  bool res_halo_full = false;              // every off-block column is in a halo
   int res_blocks = 0;         // resident form: blocks (0 = streaming form only)
   int res_grid = 0;           // cg_resident_grid(res_blocks)
   CgArgs cg;
