@@ -419,10 +419,11 @@ def run_ours(args) -> None:
         torch.distributed.destroy_process_group()
 
 
-RESIDENT_PHASES = ["A: p update + publish", "barrier 1", "B: SpMV rows", "B: p.Ap block sum",
+RESIDENT_PHASES = ["A: p update", "barrier 1", "B: SpMV rows", "B: p.Ap block sum",
                    "barrier 2", "C: pAp total", "C: fine MAS + restriction",
-                   "C: first coarse level", "C: r.z/r.r block sum", "barrier 3",
-                   "A: partial + coarse loads", "A: upper coarse levels", "A: rz sum"]
+                   "C: first coarse level", "C: r.z/r.r block sum + two-level z", "barrier 3",
+                   "A: partial + coarse loads", "A: upper restriction chain",
+                   "A: upper bank solves", "A: rz sum"]
 STREAMING_PHASES = ["prolongation", "barrier 1", "SpMV", "barrier 2", "fine MAS", "barrier 3",
                     "coarse levels", "barrier 4"]
 

@@ -966,24 +966,75 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
         cb += lv.nbank;
         __syncthreads();
       }
-      double rzc = 0.0;
-      int first = 0;
-      for (int l = 1; l < a.levels; ++l) {
-        const MasLevelDev& lv = a.coarse[l];
-        const int j = warp - first;
-        if (j >= 0 && j < lv.nbank) {
-          int slot = (first + j) * BANK + lane;
-          bool valid = j * BANK + lane < lv.nnode;
-          float4 q = s.rc[slot];
-          float3 rl = valid ? make_float3(q.x, q.y, q.z) : make_float3(0.f, 0.f, 0.f);
-          float3 zl = apply(s.Mc[first + j], rl);
-          if (!valid) zl = make_float3(0.f, 0.f, 0.f);
-          s.zc[slot] = make_float4(zl.x, zl.y, zl.z, 0.f);
-          rzc += (double)rl.x * zl.x + (double)rl.y * zl.y + (double)rl.z * zl.z;
-        }
-        first += lv.nbank;
-      }
       tr.stamp(iter, 11);
+      double rzc = 0.0;
+      // Upper banks g = 0, 1, ... (every level >= 2, level by level).  BF16:
+      // one warp per bank on the tensor cores.  FP32: a bank's columns are
+      // split over `split` warps (at most 16 banks, 32 warps), each writing
+      // its partial rows to zs; the bank's first warp adds them in warp
+      // order, so a bank solve is a chain of 32 / split columns.
+      int nup = 0;
+      for (int l = 1; l < a.levels; ++l) nup += a.coarse[l].nbank;
+      const int split = tc ? 1 : (nup <= kResWarps / 4 ? 4 : (nup <= kResWarps / 2 ? 2 : 1));
+      const int g = warp / split, part = warp - g * split;
+      int gj = -1, gnode = 0;  // bank within its level, nodes of that level
+      {
+        int first = 0;
+        for (int l = 1; l < a.levels; ++l) {
+          const MasLevelDev& lv = a.coarse[l];
+          if (g >= first && g < first + lv.nbank) {
+            gj = g - first;
+            gnode = lv.nnode;
+          }
+          first += lv.nbank;
+        }
+      }
+      const bool gvalid = gj >= 0 && gj * BANK + lane < gnode;
+      if (tc) {
+        if (gj >= 0) {
+          const int slot = g * BANK + lane;
+          float4 q = s.rc[slot];
+          float3 rl = gvalid ? make_float3(q.x, q.y, q.z) : make_float3(0.f, 0.f, 0.f);
+          float3 zq = apply(s.Mc[g], rl);
+          if (!gvalid) zq = make_float3(0.f, 0.f, 0.f);
+          s.zc[slot] = make_float4(zq.x, zq.y, zq.z, 0.f);
+          rzc += (double)rl.x * zq.x + (double)rl.y * zq.y + (double)rl.z * zq.z;
+        }
+      } else {
+        if (gj >= 0) {
+          // Slots of s.rc past a level's nodes are never written (zero).
+          const int cols = BANK / split, k0 = part * cols;
+          const float* sm = s.Mc[g];
+          const float4* rs = s.rc + g * BANK;
+          float zx = 0.f, zy = 0.f, zz = 0.f;
+#pragma unroll 8
+          for (int kk = k0; kk < k0 + cols; ++kk) {
+            float m = sm[upper_index(BANK, lane, kk)];
+            float4 rk = rs[kk];
+            zx += m * rk.x;
+            zy += m * rk.y;
+            zz += m * rk.z;
+          }
+          s.zs[warp][lane] = make_float4(zx, zy, zz, 0.f);
+        }
+        __syncthreads();
+        if (gj >= 0 && part == 0) {
+          float4 acc = s.zs[warp][lane];
+          for (int q = 1; q < split; ++q) {
+            float4 t = s.zs[warp + q][lane];
+            acc.x += t.x;
+            acc.y += t.y;
+            acc.z += t.z;
+          }
+          const int slot = g * BANK + lane;
+          float4 q = s.rc[slot];
+          float3 rl = gvalid ? make_float3(q.x, q.y, q.z) : make_float3(0.f, 0.f, 0.f);
+          float3 zq = gvalid ? make_float3(acc.x, acc.y, acc.z) : make_float3(0.f, 0.f, 0.f);
+          s.zc[slot] = make_float4(zq.x, zq.y, zq.z, 0.f);
+          rzc += (double)rl.x * zq.x + (double)rl.y * zq.y + (double)rl.z * zq.z;
+        }
+      }
+      tr.stamp(iter, 12);
       const double v1[1] = {rzc};
       res_block_sum<1>(v1, s, nullptr);
       rz += s.tot[0];
@@ -1089,7 +1140,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     // A head: totals, coarse levels, stopping rules.
     double rz_old = rz;
     totals(rz, rr);
-    tr.stamp(iter, 12);
+    tr.stamp(iter, 13);
     ++iter;
     bool stop = false;
     if (iter >= a.max_iter) {
