@@ -1522,6 +1522,7 @@ struct CollisionImpl {
   bool gs_ready = false;
   DevBuf<int> active_dof;
   DevBuf<int> jp_flags;
+  DevBuf<int> pick_d;  // DCD records picked as new contacts (grow-only)
   DevBuf<unsigned> gs_barrier;
   DevBuf<char> scan_temp;
   int n_colors = 0;
@@ -1972,13 +1973,12 @@ int CollisionSystem::append_active(float time, float dact) {
     I.key_list.push_back(fresh[i].first);
     I.prio_host.push_back(pr[i]);
   }
-  DevBuf<int> pick_d;
-  pick_d.upload(pick, st);
+  I.pick_d.upload(pick, st);
   CUDA_CHECK(cudaMemcpyAsync(I.prio.p + old, pr.data(), add * sizeof(unsigned long long),
                              cudaMemcpyHostToDevice, st));
   CUDA_CHECK(cudaMemsetAsync(I.corr.p + old, 0, add * sizeof(float4), st));
   build_contacts_kernel<<<div_up(add, kCollThreads), kCollThreads, 0, st>>>(
-      I.table_d.p, I.cols.p, pick_d.p, add, w_.contact_w_base.p, I.contacts.p + old);
+      I.table_d.p, I.cols.p, I.pick_d.p, add, w_.contact_w_base.p, I.contacts.p + old);
   SILK_LAUNCHED();
   I.n_contacts = total;
   // Vertex incidence (contact_constraints.cu:139-201).
@@ -2009,15 +2009,22 @@ int CollisionSystem::append_active(float time, float dact) {
                                                            w_.contact_w_base.p,
                                                            w_.contact_w.p, I.active_dof.p);
   SILK_LAUNCHED();
-  // Colouring by Jones-Plassmann rounds.
+  // Colouring by Jones-Plassmann rounds, kJpBatch rounds between host
+  // checks: a round after the last contact is coloured changes nothing, so
+  // the colours equal those of checking after every round.  The overflow
+  // count accumulates over the rounds; the remaining count is per round.
+  constexpr int kJpBatch = 8;
   I.colors.alloc(total);
   I.colors.zero(st);
-  for (int round = 0; round < 4096; ++round) {
-    CUDA_CHECK(cudaMemsetAsync(I.jp_flags.p, 0, 2 * sizeof(int), st));
-    jp_round_kernel<<<div_up(total, kCollThreads), kCollThreads, 0, st>>>(
-        I.contacts.p, I.prio.p, total, I.inc_off.p, I.inc_list.p, I.colors.p,
-        I.jp_flags.p, I.jp_flags.p + 1);
-    SILK_LAUNCHED();
+  CUDA_CHECK(cudaMemsetAsync(I.jp_flags.p + 1, 0, sizeof(int), st));
+  for (int round = 0; round < 4096; round += kJpBatch) {
+    for (int b = 0; b < kJpBatch; ++b) {
+      CUDA_CHECK(cudaMemsetAsync(I.jp_flags.p, 0, sizeof(int), st));
+      jp_round_kernel<<<div_up(total, kCollThreads), kCollThreads, 0, st>>>(
+          I.contacts.p, I.prio.p, total, I.inc_off.p, I.inc_list.p, I.colors.p,
+          I.jp_flags.p, I.jp_flags.p + 1);
+      SILK_LAUNCHED();
+    }
     int flags[2];
     CUDA_CHECK(cudaMemcpyAsync(flags, I.jp_flags.p, sizeof(flags), cudaMemcpyDeviceToHost, st));
     CUDA_CHECK(cudaStreamSynchronize(st));
