@@ -271,7 +271,7 @@ def run_ours(args) -> None:
     w.profile(reset=True)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
-    launches = admm = cg = solves = contacts = admm_first = 0
+    launches = admm = cg = solves = contacts = admm_first = ccd_first = 0
     if world_size > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -288,6 +288,7 @@ def run_ours(args) -> None:
             admm += st.admm_iterations
             if k < args.e2e_steps:
                 admm_first += st.admm_iterations
+                ccd_first += st.ccd_queries
             cg += st.cg_iterations
             solves += st.cg_solves
             contacts = st.contacts
@@ -339,7 +340,8 @@ def run_ours(args) -> None:
     pin_obs = torch.from_numpy(SV.ravel().copy()).pin_memory().numpy()
     pin_out = torch.empty(V.size, dtype=torch.float32).pin_memory().numpy()
     e2e_ms = []
-    e2e_admm = 0
+    e2e_admm = e2e_ccd = 0
+    we.profile(reset=True)
     n_e2e = min(args.e2e_steps, args.steps)
     for k in range(n_e2e):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -354,6 +356,8 @@ def run_ours(args) -> None:
         assert r, r.to_string()
         e2e_ms.append(a.elapsed_time(b))
         e2e_admm += we.step_stats().admm_iterations
+        e2e_ccd += we.step_stats().ccd_queries
+    e2e_prof = we.profile(reset=True)
     e2e_val = n_e2e / (sum(e2e_ms) / 1e3) * world_size
     value_same_steps = n_e2e / (sum(step_ms[:n_e2e]) / 1e3) * world_size
     del we
@@ -401,7 +405,20 @@ def run_ours(args) -> None:
         "e2e": {"value": round(e2e_val, 4), "unit": "steps/s",
                 "h2d_bytes_per_step": int(SV.nbytes), "d2h_bytes_per_step": int(V.nbytes),
                 "steps": n_e2e, "device_value_same_steps": round(value_same_steps, 4),
-                "admm_iterations": e2e_admm, "device_admm_iterations_same_steps": admm_first},
+                "admm_iterations": e2e_admm, "device_admm_iterations_same_steps": admm_first,
+                # set_obstacle_position marks the obstacle as moving (as the
+                # reference does), so the e2e steps run the moving-obstacle
+                # collision path: its CCD queries beside the device run's.
+                "ccd_queries": e2e_ccd, "device_ccd_queries_same_steps": ccd_first,
+                "ms_per_step": [round(t, 1) for t in e2e_ms],
+                "device_ms_per_step": [round(t, 1) for t in step_ms[:n_e2e]],
+                "phases_ms_per_step": {
+                    "cg_kernel_events": round(e2e_prof["cg_time_ms"] / n_e2e, 2),
+                    "other_admm_kernels_events": round(e2e_prof["admm_other_ms"] / n_e2e, 2),
+                    "admm_host_wall": round(e2e_prof["admm_host_ms"] / n_e2e, 2),
+                    "ccd_host_wall": round(e2e_prof["ccd_host_ms"] / n_e2e, 2),
+                    "dcd_host_wall": round(e2e_prof["dcd_host_ms"] / n_e2e, 2),
+                    "step_host_wall": round(e2e_prof["step_host_ms"] / n_e2e, 2)}},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "phases_ms_per_step": {
