@@ -98,6 +98,13 @@ typedef struct {
                                  iterates of the same ADMM solve) as the start
                                  of each later CG solve; the plain start's
                                  residual stays the stopping reference */
+  int32_t resident_halo_limit; /* > 0: at most this many (and at most 1024)
+                                 off-block vertices per resident-CG block are
+                                 gathered into shared memory; further ones are
+                                 read from global memory and p is published
+                                 through the grid (applies when the solver
+                                 layout is built: first step after a change of
+                                 the cloths); 0: 1024 */
 } silk_solver_options;
 
 /* CUDA-event timing of the persistent CG kernel over the steps since the

@@ -486,6 +486,8 @@ void World::build_resident_layout(Cloth& c) {
   std::vector<int> halo_off(nblocks + 1, 0), halo_col;
   std::vector<int> halo_slot(nv, -1), halo_mark(nv, -1);
   bool halo_overflow = false;
+  const int halo_cap = opt.resident_halo_limit > 0 ? std::min(opt.resident_halo_limit, kResHalo)
+                                                   : kResHalo;
   for (int k = 0; k < nblocks; ++k) {
     halo_off[k] = (int)halo_col.size();
     for (int bb = k * BANK; bb < std::min(nbank0, (k + 1) * BANK); ++bb)
@@ -493,7 +495,7 @@ void World::build_resident_layout(Cloth& c) {
         for (int q = S.Lrows[v]; q < S.Lrows[v + 1]; ++q) {
           int col = S.Lcols[q];
           if (part_of[col] / BANK == k || halo_mark[col] == k) continue;
-          if ((int)halo_col.size() - halo_off[k] >= kResHalo) {
+          if ((int)halo_col.size() - halo_off[k] >= halo_cap) {
             halo_overflow = true;
             continue;
           }

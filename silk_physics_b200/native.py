@@ -77,7 +77,8 @@ class _SolverOptionsC(C.Structure):
     _fields_ = [("fixed_linear_rel_tol", C.c_float), ("cg_max_iter", C.c_int32),
                 ("mas_bf16", C.c_int32), ("profile", C.c_int32), ("cg_form", C.c_int32),
                 ("learned_warm_start", C.c_int32), ("capture_samples", C.c_int32),
-                ("contact_gs_form", C.c_int32), ("admm_extrapolated_start", C.c_int32)]
+                ("contact_gs_form", C.c_int32), ("admm_extrapolated_start", C.c_int32),
+                ("resident_halo_limit", C.c_int32)]
 
 
 class _ProfileC(C.Structure):
@@ -163,6 +164,7 @@ class SolverOptions:
     capture_samples: bool = False     # record warm-start training samples
     contact_gs_form: int = 0          # 0: single-block Gauss-Seidel where possible; 1: grid
     admm_extrapolated_start: bool = False  # offer 2 x_k - x_(k-1) as later CG starts
+    resident_halo_limit: int = 0  # > 0: fewer halo slots per resident-CG block (0: 1024)
 
     def to_c(self) -> _SolverOptionsC:
         o = _SolverOptionsC()
@@ -175,6 +177,7 @@ class SolverOptions:
         o.capture_samples = int(self.capture_samples)
         o.contact_gs_form = int(self.contact_gs_form)
         o.admm_extrapolated_start = int(self.admm_extrapolated_start)
+        o.resident_halo_limit = int(self.resident_halo_limit)
         return o
 
 

@@ -11,7 +11,7 @@ NO_COLLISION = N.CollisionConfig(is_collision_on=False, is_self_collision_on=Fal
 
 
 def _pair(oracle, s, steps, fp64=False, inner=10, admm_tol=0.0, cg_rel=1e-6, bf16=False,
-          pins=True, cloth=None, jitter=0.0, form=0, extrap=False):
+          pins=True, cloth=None, jitter=0.0, form=0, extrap=False, halo_limit=0):
     V, F = S.grid_sheet(s, jitter=jitter, seed=7)
     P = S.top_corner_pins(s) if pins else np.zeros(0, np.int32)
     cloth = cloth or N.ClothConfig()
@@ -20,7 +20,8 @@ def _pair(oracle, s, steps, fp64=False, inner=10, admm_tol=0.0, cg_rel=1e-6, bf1
     assert w.init()
     assert w.set_global_config(g)
     assert w.set_solver_options(N.SolverOptions(fixed_linear_rel_tol=cg_rel, mas_bf16=bf16,
-                                                cg_form=form, admm_extrapolated_start=extrap))
+                                                cg_form=form, admm_extrapolated_start=extrap,
+                                                resident_halo_limit=halo_limit))
     r, h = w.add_cloth(cloth, NO_COLLISION, V, F, P)
     assert r, r.to_string()
     perm, offs = w.cloth_partition(h, len(V))
@@ -258,3 +259,27 @@ def test_two_cloths_concurrent_cg_against_oracle(oracle):
         eg64 = np.abs(xg - o64.position(h64)).max()
         print(f"cloth {h}: |gpu-o64| {eg64:.2e} |o32-o64| {e3264:.2e}")
         assert eg64 <= max(3.0 * e3264, 2e-5)
+
+
+
+@pytest.mark.parametrize("s", [80, 128])
+def test_resident_halo_overflow_against_oracle(oracle, s):
+    """Halo limit 16 (solver option): every block of the resident CG reads
+    more vertices outside itself than its halo holds, so p is published
+    through the cluster or grid and the overflow columns are read from
+    global memory.  Same parity bound as the full-halo form: within 3x the
+    FP32 oracle's drift of the FP64 oracle (floor 2e-6 m), resident form in
+    use (80: a 7-block cluster; 128: a 17-block cooperative grid)."""
+    cloth = N.ClothConfig(elastic_stiffness=10.0, bending_stiffness=1e-4, density=5.0,
+                          damping=0.01)
+    kw = dict(inner=50, admm_tol=1e-6, cg_rel=1e-6, cloth=cloth, jitter=1e-4)
+    _, _, _, o32, _ = _pair(oracle, s, 1, **kw)
+    _, _, _, o64, _ = _pair(oracle, s, 1, fp64=True, **kw)
+    e3264 = np.abs(o32[0][2] - o64[0][2]).max()
+    w, _, _, og, _ = _pair(oracle, s, 1, halo_limit=16, **kw)
+    st = w.step_stats()
+    eg64 = np.abs(og[0][1] - o64[0][2]).max()
+    print(f"s={s} halo limit 16: |gpu-o64| {eg64:.2e} |o32-o64| {e3264:.2e}, "
+          f"resident solves {st.cg_resident_solves} of {st.cg_solves}")
+    assert st.cg_resident_solves == st.cg_solves > 0
+    assert eg64 <= max(3.0 * e3264, 2e-6)
