@@ -261,6 +261,15 @@ silk_status silk_partition_mesh(const float* verts, int64_t verts_len,
                                 const int32_t* faces, int64_t faces_len,
                                 int32_t* perm, int32_t* part_offsets,
                                 int64_t offsets_cap, int32_t* nparts);
+/* Entry order of one MAS bank's 32 matrix rows in the resident CG kernel's
+ * ELL slice (no reference counterpart; inspection entry point for the
+ * tests): row l holds cols/vals[row_ptr[l] .. row_ptr[l + 1]) (a column < 0
+ * is shared-memory slot -1 - column), width >= the longest row, slot0 the
+ * bank's first slot; out_cols/out_vals receive width x 32 entries, round j
+ * of row l at [j * 32 + l] (padding: value 0). */
+silk_status silk_schedule_bank_rows(const int32_t* row_ptr, const int32_t* cols,
+                                    const int32_t* vals, int32_t width, int32_t slot0,
+                                    int32_t* out_cols, int32_t* out_vals);
 /* Static assembly of one cloth in solver order (ClothAssemblyL2Cache +
  * ClothAssemblyL1Cache, cloth_assembly_l2_cache.cpp:71-136,
  * cloth_assembly_l1_cache.cu:16-97): dense scalar matrix L (nv x nv, may be

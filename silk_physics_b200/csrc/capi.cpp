@@ -301,6 +301,30 @@ silk_status silk_debug_min_toi(silk_world* w, float time_start, float max_time,
   });
 }
 
+silk_status silk_schedule_bank_rows(const int32_t* row_ptr, const int32_t* cols,
+                                    const int32_t* vals, int32_t width, int32_t slot0,
+                                    int32_t* out_cols, int32_t* out_vals) {
+  if (!row_ptr || !out_cols || !out_vals || width < 0 || slot0 < 0)
+    return SILK_ERR_INVALID_CONFIG;
+  try {
+    std::vector<std::vector<std::pair<int, int>>> rows(32);
+    for (int l = 0; l < 32; ++l) {
+      const int n = row_ptr[l + 1] - row_ptr[l];
+      if (n < 0 || n > width || (n > 0 && (!cols || !vals))) return SILK_ERR_INVALID_CONFIG;
+      for (int i = row_ptr[l]; i < row_ptr[l + 1]; ++i) rows[l].emplace_back(cols[i], vals[i]);
+    }
+    std::vector<std::pair<int, int>> out((size_t)width * 32);
+    silkb::schedule_bank_rows(rows, width, slot0, out.data());
+    for (size_t i = 0; i < out.size(); ++i) {
+      out_cols[i] = out[i].first;
+      out_vals[i] = out[i].second;
+    }
+    return SILK_OK;
+  } catch (...) {
+    return SILK_ERR_UNKNOWN;
+  }
+}
+
 silk_status silk_partition_mesh(const float* verts, int64_t verts_len,
                                 const int32_t* faces, int64_t faces_len,
                                 int32_t* perm, int32_t* part_offsets,

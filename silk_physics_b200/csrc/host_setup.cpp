@@ -670,4 +670,79 @@ void contact_weights(const ClothSetup& S, double dt, std::vector<double>& w) {
   }
 }
 
+// Rows per bank (one per lane of a warp) of the resident CG's ELL slices.
+constexpr int kSchedRows = 32;
+
+// Order of the entries of one bank's rows in its ELL slice (round j of lane
+// l at out[j * kSchedRows + l]).  In round j the 32 lanes of the warp gather p from
+// shared memory (float4 per slot), and a 128-bit shared load is served per
+// quarter-warp: two lanes of a quarter whose slots differ but share slot % 8
+// (the 16-byte bank group) cost an extra pass.  Each quarter's entries are
+// placed round by round, the lanes with the least slack first, each taking
+// an entry whose bank group is still free in the round (or whose slot is
+// already read, a broadcast), else an entry outside the block (a global
+// load, no shared-memory access), else, when it has no slack left, any
+// entry.  Padding entries (value 0) read a slot another lane of the quarter
+// reads.  Entries outside the block have column >= 0; the kernel reads slot
+// -1 - column otherwise.  A row's terms are summed in round order.
+void schedule_bank_rows(const std::vector<std::vector<std::pair<int, int>>>& rows, int width,
+                        int slot0, std::pair<int, int>* out) {
+  for (int q = 0; q < kSchedRows / 8; ++q) {
+    std::vector<std::vector<std::pair<int, int>>> rem(8);
+    for (int l = 0; l < 8; ++l) rem[l] = rows[8 * q + l];
+    for (int j = 0; j < width; ++j) {
+      const int left = width - j;
+      int order[8];
+      for (int l = 0; l < 8; ++l) order[l] = l;
+      std::stable_sort(order, order + 8, [&](int a, int b) {
+        return left - (int)rem[a].size() < left - (int)rem[b].size();
+      });
+      int group_slot[8];  // slot read in this round per bank group, -1: free
+      for (int g = 0; g < 8; ++g) group_slot[g] = -1;
+      bool pad[8] = {false, false, false, false, false, false, false, false};
+      for (int oi = 0; oi < 8; ++oi) {
+        const int l = order[oi];
+        auto& r = rem[l];
+        if (r.empty()) {
+          pad[l] = true;
+          continue;
+        }
+        int pick = -1;
+        for (int e = 0; e < (int)r.size() && pick < 0; ++e)
+          if (r[e].first < 0) {
+            int slot = -1 - r[e].first;
+            int g = slot & 7;
+            if (group_slot[g] < 0 || group_slot[g] == slot) pick = e;
+          }
+        if (pick < 0)
+          for (int e = 0; e < (int)r.size() && pick < 0; ++e)
+            if (r[e].first >= 0) pick = e;
+        if (pick < 0 && (int)r.size() >= left) pick = 0;
+        if (pick < 0) {
+          pad[l] = true;
+          continue;
+        }
+        std::pair<int, int> e = r[pick];
+        r.erase(r.begin() + pick);
+        if (e.first < 0) {
+          int slot = -1 - e.first;
+          if (group_slot[slot & 7] < 0) group_slot[slot & 7] = slot;
+        }
+        out[j * kSchedRows + 8 * q + l] = e;
+      }
+      for (int l = 0; l < 8; ++l) {
+        if (!pad[l]) continue;
+        int slot = slot0 + 8 * q + l;
+        for (int g = 0; g < 8; ++g)
+          if (group_slot[g] >= 0) {
+            slot = group_slot[g];
+            break;
+          }
+        if (group_slot[slot & 7] < 0) group_slot[slot & 7] = slot;
+        out[j * kSchedRows + 8 * q + l] = std::make_pair(-1 - slot, 0);
+      }
+    }
+  }
+}
+
 }  // namespace silkb

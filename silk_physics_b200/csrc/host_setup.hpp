@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace silkb {
@@ -84,5 +85,11 @@ void build_cloth_setup(const float* verts, int nv, const int* faces, int nf,
 
 // Per-vertex contact weight (cloth_assembly_l1_cache.cu:58-75) for a dt.
 void contact_weights(const ClothSetup& s, double dt, std::vector<double>& w);
+
+// Entry order of one bank's 32 rows in the resident CG's ELL slice: out has
+// width x 32 (column, value bits) pairs, round j of row l at out[j * 32 + l];
+// a column < 0 is shared-memory slot -1 - column.  Rows no longer than width.
+void schedule_bank_rows(const std::vector<std::vector<std::pair<int, int>>>& rows, int width,
+                        int slot0, std::pair<int, int>* out);
 
 }  // namespace silkb

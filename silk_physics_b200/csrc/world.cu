@@ -376,78 +376,6 @@ SolverView World::view() {
 // above fit the shared memory of a block.  The off-diagonal part of L is
 // re-sliced per fine bank; a column inside the block is stored as -1 - slot,
 // and the entries from other blocks come first in each row.
-// Order of the entries of one bank's rows in its ELL slice (round j of lane
-// l at out[j * BANK + l]).  In round j the 32 lanes of the warp gather p from
-// shared memory (float4 per slot), and a 128-bit shared load is served per
-// quarter-warp: two lanes of a quarter whose slots differ but share slot % 8
-// (the 16-byte bank group) cost an extra pass.  Each quarter's entries are
-// placed round by round, the lanes with the least slack first, each taking
-// an entry whose bank group is still free in the round (or whose slot is
-// already read, a broadcast), else an entry outside the block (a global
-// load, no shared-memory access), else, when it has no slack left, any
-// entry.  Padding entries (value 0) read a slot another lane of the quarter
-// reads.  Entries outside the block have column >= 0; the kernel reads slot
-// -1 - column otherwise.  A row's terms are summed in round order.
-static void schedule_bank_rows(std::vector<std::vector<int2>>& rows, int width, int slot0,
-                               int2* out) {
-  for (int q = 0; q < BANK / 8; ++q) {
-    std::vector<std::vector<int2>> rem(8);
-    for (int l = 0; l < 8; ++l) rem[l] = rows[8 * q + l];
-    for (int j = 0; j < width; ++j) {
-      const int left = width - j;
-      int order[8];
-      for (int l = 0; l < 8; ++l) order[l] = l;
-      std::stable_sort(order, order + 8, [&](int a, int b) {
-        return left - (int)rem[a].size() < left - (int)rem[b].size();
-      });
-      int group_slot[8];  // slot read in this round per bank group, -1: free
-      for (int g = 0; g < 8; ++g) group_slot[g] = -1;
-      bool pad[8] = {false, false, false, false, false, false, false, false};
-      for (int oi = 0; oi < 8; ++oi) {
-        const int l = order[oi];
-        auto& r = rem[l];
-        if (r.empty()) {
-          pad[l] = true;
-          continue;
-        }
-        int pick = -1;
-        for (int e = 0; e < (int)r.size() && pick < 0; ++e)
-          if (r[e].x < 0) {
-            int slot = -1 - r[e].x;
-            int g = slot & 7;
-            if (group_slot[g] < 0 || group_slot[g] == slot) pick = e;
-          }
-        if (pick < 0)
-          for (int e = 0; e < (int)r.size() && pick < 0; ++e)
-            if (r[e].x >= 0) pick = e;
-        if (pick < 0 && (int)r.size() >= left) pick = 0;
-        if (pick < 0) {
-          pad[l] = true;
-          continue;
-        }
-        int2 e = r[pick];
-        r.erase(r.begin() + pick);
-        if (e.x < 0) {
-          int slot = -1 - e.x;
-          if (group_slot[slot & 7] < 0) group_slot[slot & 7] = slot;
-        }
-        out[j * BANK + 8 * q + l] = e;
-      }
-      for (int l = 0; l < 8; ++l) {
-        if (!pad[l]) continue;
-        int slot = slot0 + 8 * q + l;
-        for (int g = 0; g < 8; ++g)
-          if (group_slot[g] >= 0) {
-            slot = group_slot[g];
-            break;
-          }
-        if (group_slot[slot & 7] < 0) group_slot[slot & 7] = slot;
-        out[j * BANK + 8 * q + l] = make_int2(-1 - slot, 0);
-      }
-    }
-  }
-}
-
 void World::build_resident_layout(Cloth& c) {
   const ClothSetup& S = *c.setup;
   ClothDev& d = c.dev;
@@ -505,7 +433,8 @@ void World::build_resident_layout(Cloth& c) {
   }
   halo_off[nblocks] = (int)halo_col.size();
   std::vector<int2> ent(std::max(ptr[nbank0], 1));
-  std::vector<std::vector<int2>> row(BANK);
+  std::vector<std::vector<std::pair<int, int>>> row(BANK);
+  std::vector<std::pair<int, int>> sched;
   int halo_block = -1;
   for (int b = 0; b < nbank0; ++b) {
     const int k = b / BANK;
@@ -529,14 +458,17 @@ void World::build_resident_layout(Cloth& c) {
         std::memcpy(&bits, &val, 4);
         int cb = part_of[col];
         if (cb / BANK == k)
-          row[lane].push_back(make_int2(-1 - ((cb - k * BANK) * BANK + lane_of[col]), bits));
+          row[lane].emplace_back(-1 - ((cb - k * BANK) * BANK + lane_of[col]), bits);
         else if (halo_slot[col] >= 0)
-          row[lane].push_back(make_int2(-1 - halo_slot[col], bits));
+          row[lane].emplace_back(-1 - halo_slot[col], bits);
         else
-          row[lane].push_back(make_int2(col, bits));
+          row[lane].emplace_back(col, bits);
       }
     }
-    schedule_bank_rows(row, width[b], (b - k * BANK) * BANK, &ent[ptr[b]]);
+    sched.resize((size_t)BANK * width[b]);
+    schedule_bank_rows(row, width[b], (b - k * BANK) * BANK, sched.data());
+    for (size_t i = 0; i < sched.size(); ++i)
+      ent[ptr[b] + i] = make_int2(sched[i].first, sched[i].second);
   }
   cudaStream_t st = stream;
   d.rb_ptr.upload(ptr, st);

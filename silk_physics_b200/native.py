@@ -275,6 +275,8 @@ def _load() -> C.CDLL:
                                     C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)], C.c_int),
         "silk_partition_mesh": ([_F32P, C.c_int64, _I32P, C.c_int64, _I32P, _I32P, C.c_int64,
                                  C.POINTER(C.c_int32)], C.c_int),
+        "silk_schedule_bank_rows": ([_I32P, _I32P, _I32P, C.c_int32, C.c_int32, _I32P, _I32P],
+                                    C.c_int),
         "silk_assemble_cloth_host": ([C.POINTER(_ClothConfigC), _F32P, C.c_int64, _I32P,
                                       C.c_int64, C.c_float, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p], C.c_int),
@@ -612,6 +614,23 @@ def partition_mesh(verts, faces) -> tuple[np.ndarray, np.ndarray]:
     if st:
         raise RuntimeError(_result(st).to_string())
     return perm, offs[: n.value + 1].copy()
+
+
+def schedule_bank_rows(rows, width: int, slot0: int) -> tuple[np.ndarray, np.ndarray]:
+    """Entry order of one bank's 32 rows (lists of (column, value bits)) in
+    the resident CG's ELL slice: (columns, values), each width x 32, round j
+    of row l at [j, l]."""
+    assert len(rows) == 32
+    ptr = np.zeros(33, np.int32)
+    ptr[1:] = np.cumsum([len(r) for r in rows])
+    cols = np.array([c for r in rows for c, _ in r] or [0], np.int32)
+    vals = np.array([v for r in rows for _, v in r] or [0], np.int32)
+    oc = np.zeros(width * 32, np.int32)
+    ov = np.zeros(width * 32, np.int32)
+    st = lib.silk_schedule_bank_rows(ptr, cols, vals, width, slot0, oc, ov)
+    if st:
+        raise RuntimeError(_result(st).to_string())
+    return oc.reshape(width, 32), ov.reshape(width, 32)
 
 
 def assemble_cloth_host(cloth: ClothConfig, verts, faces, dt: float):
