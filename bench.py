@@ -118,6 +118,46 @@ def dist_env():
             int(os.environ.get("WORLD_SIZE", 1)))
 
 
+# Replicas plumbing (one process per GPU, no data-path collective): a process
+# group with a short timeout, a barrier and the max over ranks of each rank's
+# device time, and scenes sharded by rank.  The backend is "nccl" on GPUs and
+# "gloo" in the CPU tests of this plumbing.
+def dist_init(backend: str, timeout_s: int = 600) -> bool:
+    """Start the process group when WORLD_SIZE > 1; True if one runs."""
+    _, _, world_size = dist_env()
+    if world_size <= 1:
+        return False
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s))
+    return True
+
+
+def max_over_ranks(ms: float, device: str) -> float:
+    """Largest value over the ranks (every rank takes part), then a barrier."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return ms
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    return float(t.item())
+
+
+def shard(items, rank: int, world_size: int):
+    """Items of this rank: every world_size-th, starting at its rank."""
+    return items[rank::world_size]
+
+
+def weak_value(units_per_rank_step: float, world_size: int, steps: int, ms: float) -> float:
+    """Whole-job throughput: the units every rank processed over the slowest
+    rank's time."""
+    return units_per_rank_step * world_size * steps / (ms / 1e3)
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle sampling during the timed region."""
 
@@ -244,11 +284,7 @@ def run_ours(args) -> None:
 
     rank, local_rank, world_size = dist_env()
     torch.cuda.set_device(local_rank)
-    if world_size > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    dist_init("nccl")
     from silk_physics_b200 import native as N
 
     V, F, SV, SF = scene()
@@ -296,12 +332,8 @@ def run_ours(args) -> None:
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = float(sum(step_ms))
     prof = w.profile(reset=True)
-    if world_size > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-        torch.distributed.barrier()
-    value = world_size * args.steps / (total_ms / 1e3)
+    total_ms = max_over_ranks(total_ms, "cuda")
+    value = weak_value(1, world_size, args.steps, total_ms)
 
     # Learned warm start + BF16 MAS on the same scene, and the 100K-vertex
     # sheet (plain FP32 vs learned + BF16), each from its own fresh world.
@@ -502,9 +534,13 @@ def run_batched(args) -> None:
     minus the first start event (CUDA events)."""
     import torch
 
+    rank, local_rank, world_size = dist_env()
+    torch.cuda.set_device(local_rank)
+    dist_init("nccl")
     from silk_physics_b200 import native as N
 
-    scenes = scenes_c5(args.c5_scenes)
+    # Scenes are independent: each rank steps its share, no collective.
+    scenes = shard(scenes_c5(args.c5_scenes), rank, world_size)
     opts = N.SolverOptions(fixed_linear_rel_tol=args.cg_rel_tol, mas_bf16=args.bf16)
 
     def build():
@@ -540,20 +576,28 @@ def run_batched(args) -> None:
     # The same steps from the same state, concurrently and (on a second copy
     # of the worlds) one world after another.
     worlds, streams = build()
-    ms = timed(worlds, streams, args.c5_steps, 0)
+    ms = max_over_ranks(timed(worlds, streams, args.c5_steps, 0), "cuda")
+    contacts = int(sum(w.step_stats().contacts for w in worlds))
     seq_ms = None
     if args.c5_sequential:
         del worlds
         worlds, streams = build()
-        seq_ms = timed(worlds, streams, args.c5_steps, 1)
+        seq_ms = max_over_ranks(timed(worlds, streams, args.c5_steps, 1), "cuda")
+    if world_size > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank != 0:
+        return
     line = {
         "metric": "scene-steps/s (independent scenes stepped concurrently)",
-        "value": round(len(worlds) * args.c5_steps / (ms / 1e3), 4), "unit": "scene-steps/s",
-        "n_gpus": 1, "steps": args.c5_steps, "warmup": args.c5_prelude,
-        "contacts_last_step": int(sum(w.step_stats().contacts for w in worlds)),
+        "value": round(args.c5_scenes * args.c5_steps / (ms / 1e3), 4), "unit": "scene-steps/s",
+        "n_gpus": world_size, "steps": args.c5_steps, "warmup": args.c5_prelude,
+        "scaling": "strong", "contacts_last_step_rank0": contacts,
         "ms_per_step": round(ms / args.c5_steps, 3), "higher_is_better": True,
         "dtype": "f32", "data": "synthetic (seeded sheets + icospheres)",
-        "config": {"workload": C5_WORKLOAD, "scenes": len(worlds), "vertices": nverts,
+        "config": {"workload": C5_WORKLOAD, "scenes": args.c5_scenes,
+                   "scenes_rank0": len(worlds), "vertices_rank0": nverts,
                    "cg_rel_tol": args.cg_rel_tol, "mas": "bf16" if args.bf16 else "fp32",
                    "host_threads": "one per hardware thread"},
     }
