@@ -338,7 +338,8 @@ def run_ours(args) -> None:
     # Learned warm start + BF16 MAS on the same scene, and the 100K-vertex
     # sheet (plain FP32 vs learned + BF16), each from its own fresh world.
     variants = {}
-    if args.variants and MODEL.exists():
+    # Single-GPU diagnostics: not repeated on every replica.
+    if args.variants and MODEL.exists() and world_size == 1:
         for name, bf16, learned, extrap in (("c2_bf16", True, False, False),
                                             ("c2_learned_bf16", True, True, False),
                                             ("c2_extrapolated", False, False, True),
@@ -390,8 +391,10 @@ def run_ours(args) -> None:
         e2e_admm += we.step_stats().admm_iterations
         e2e_ccd += we.step_stats().ccd_queries
     e2e_prof = we.profile(reset=True)
-    e2e_val = n_e2e / (sum(e2e_ms) / 1e3) * world_size
-    value_same_steps = n_e2e / (sum(step_ms[:n_e2e]) / 1e3) * world_size
+    # Every rank takes both reductions, in this order.
+    e2e_val = weak_value(1, world_size, n_e2e, max_over_ranks(sum(e2e_ms), "cuda"))
+    value_same_steps = weak_value(1, world_size, n_e2e,
+                                  max_over_ranks(sum(step_ms[:n_e2e]), "cuda"))
     del we
 
     if rank != 0:
