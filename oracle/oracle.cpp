@@ -1803,10 +1803,21 @@ struct World {
         out[r] = s + lhs[r] * in[r];
       }
     };
+    // Fixed chunks summed in chunk order: the same value for any thread count
+    // (an OpenMP reduction adds the thread partials in the order they finish).
     auto dotp = [&](const std::vector<T>& a, const std::vector<T>& bb) {
+      constexpr int kChunk = 4096;
+      const int nch = (n + kChunk - 1) / kChunk;
+      std::vector<double> part(nch, 0.0);
+#pragma omp parallel for schedule(static)
+      for (int ch = 0; ch < nch; ++ch) {
+        double s = 0;
+        const int e = std::min(n, (ch + 1) * kChunk);
+        for (int i = ch * kChunk; i < e; ++i) s += (double)a[i] * (double)bb[i];
+        part[ch] = s;
+      }
       double s = 0;
-#pragma omp parallel for reduction(+ : s) schedule(static)
-      for (int i = 0; i < n; ++i) s += (double)a[i] * (double)bb[i];
+      for (double v : part) s += v;
       return s;
     };
     std::vector<T> r, z, p, Ap;

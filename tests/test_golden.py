@@ -1,0 +1,99 @@
+"""Golden fixtures (tests/golden/, made by tests/golden/make_golden.py from
+the CPU oracle): the oracle still reproduces them exactly (CPU), and the CUDA
+path matches them (GPU) - the C1 sheet within the FP32 parity tolerance, the
+CCD queries bit for bit."""
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from silk_physics_b200 import native as N
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+sys.path.insert(0, str(GOLDEN))
+
+import make_golden as G  # noqa: E402
+
+
+def _load(name):
+    return dict(np.load(GOLDEN / name))
+
+
+def test_host_partition_matches_golden():
+    g = _load("c1_sheet32.npz")
+    perm, offs = N.partition_mesh(g["verts"], g["faces"])
+    np.testing.assert_array_equal(perm, g["perm"])
+    np.testing.assert_array_equal(offs, g["part_offsets"])
+
+
+def test_oracle_reproduces_c1_golden(oracle):
+    """Deterministic oracle (fixed-order reductions): identical positions for
+    any number of OpenMP threads."""
+    g = _load("c1_sheet32.npz")
+    d = G.c1_sheet()
+    for k in g:
+        np.testing.assert_array_equal(np.asarray(d[k]), g[k], err_msg=k)
+
+
+@pytest.mark.parametrize("vf", [True, False])
+def test_oracle_reproduces_ccd_golden(oracle, vf):
+    g = _load("ccd_queries.npz")
+    tag = "vf" if vf else "ee"
+    x, ms, hit, toi, tup = G.ccd_queries(vf)
+    np.testing.assert_array_equal(x, g[f"{tag}_x"])
+    np.testing.assert_array_equal(hit, g[f"{tag}_hit"])
+    np.testing.assert_array_equal(toi, g[f"{tag}_toi"])
+    np.testing.assert_array_equal(tup, g[f"{tag}_tup"])
+
+
+@pytest.mark.gpu
+def test_gpu_c1_matches_golden():
+    """C1 setting (10 un-converged ADMM iterations, CG rel 1e-6): within 1e-4 m
+    of the FP32 oracle after 1 step and 2e-3 m after 10, and no further from
+    the FP64 oracle than 3x the FP32 oracle's own drift (floor 2e-5 m)."""
+    g = _load("c1_sheet32.npz")
+    V, F, P = g["verts"], g["faces"], g["pins"]
+    w = N.World()
+    assert w.init()
+    c = G.C1_CONFIG
+    assert w.set_global_config(N.GlobalConfig(max_inner_iteration=c["max_inner_iteration"],
+                                              admm_abs_tol=c["admm_abs_tol"],
+                                              admm_rel_tol=c["admm_rel_tol"]))
+    assert w.set_solver_options(N.SolverOptions(fixed_linear_rel_tol=c["fixed_linear_rel_tol"]))
+    r, h = w.add_cloth(N.ClothConfig(), N.CollisionConfig(is_collision_on=False,
+                                                          is_self_collision_on=False), V, F, P)
+    assert r, r.to_string()
+    perm, offs = w.cloth_partition(h, len(V))
+    np.testing.assert_array_equal(perm, g["perm"])
+    np.testing.assert_array_equal(offs, g["part_offsets"])
+    x = np.zeros(V.size, np.float32)
+    for k in range(1, max(G.C1_STEPS) + 1):
+        assert w.solver_step()
+        if k not in G.C1_STEPS:
+            continue
+        assert w.get_cloth_position(h, x)
+        xg = x.reshape(-1, 3).astype(np.float64)
+        x32, x64 = g[f"o32_step{k}"], g[f"o64_step{k}"]
+        e32 = np.abs(xg - x32).max()
+        eg64 = np.abs(xg - x64).max()
+        e3264 = np.abs(x32 - x64).max()
+        print(f"step {k}: |gpu-o32| {e32:.2e} |gpu-o64| {eg64:.2e} |o32-o64| {e3264:.2e}")
+        if k == 1:
+            assert e32 < 1e-4
+        if k == 10:
+            assert e32 < 2e-3
+        assert eg64 <= max(3.0 * e3264, 2e-5)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("vf", [True, False])
+def test_gpu_ccd_matches_golden(vf):
+    g = _load("ccd_queries.npz")
+    tag = "vf" if vf else "ee"
+    err = np.full(3, G.CCD_ERR[vf], np.float32)
+    hit, toi, tup = N.ccd_batch(vf, g[f"{tag}_x"], err, g[f"{tag}_ms"], 1e-6, 4096, 1.0)
+    np.testing.assert_array_equal(hit.astype(np.int32), g[f"{tag}_hit"])
+    m = g[f"{tag}_hit"] != 0
+    np.testing.assert_array_equal(np.float32(toi)[m], g[f"{tag}_toi"][m])
+    np.testing.assert_array_equal(np.float32(tup)[m], g[f"{tag}_tup"][m])
