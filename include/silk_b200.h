@@ -233,6 +233,14 @@ silk_status silk_debug_cloth_partition(const silk_world* w, uint32_t handle,
 /* Scalar system matrix L (H = L (x) I3) as dense row-major, solver order. */
 silk_status silk_debug_cloth_matrix(const silk_world* w, uint32_t handle,
                                     double* dense, int64_t n_len);
+/* Fine MAS level of the last factorisation (MASPreconditioner::factorize,
+ * mas_preconditioner.cu:903-965): the FP32 bank inverses (packed upper
+ * triangle, 528 floats per bank, banks in partition order, slot = solver
+ * index - first vertex of the bank) and the diagonal the ADMM adds to L
+ * (nv floats, solver order), the bank matrix being L + diag restricted to
+ * the bank. */
+silk_status silk_debug_mas_fine(const silk_world* w, uint32_t handle, float* inverses,
+                                int64_t inverses_len, float* diag, int64_t diag_len);
 /* Refit every collider to (t0 = current state, t1 = current + disp) where
  * disp is per cloth in original vertex order, concatenated. */
 silk_status silk_debug_refit(silk_world* w, const float* disp,

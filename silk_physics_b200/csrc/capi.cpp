@@ -276,6 +276,14 @@ silk_status silk_debug_cloth_matrix(const silk_world* w, uint32_t handle,
   });
 }
 
+silk_status silk_debug_mas_fine(const silk_world* w, uint32_t handle, float* inverses,
+                                int64_t inverses_len, float* diag, int64_t diag_len) {
+  if (!inverses || !diag) return SILK_ERR_INVALID_CONFIG;
+  return guard_init(const_cast<silk_world*>(w), [&](World& W) {
+    return W.debug_mas_fine(handle, inverses, inverses_len, diag, diag_len);
+  });
+}
+
 silk_status silk_debug_refit(silk_world* w, const float* disp, int64_t len) {
   return guard_init(w, [&](World& W) { return W.debug_refit(disp, len); });
 }

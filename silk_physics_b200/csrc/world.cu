@@ -1261,6 +1261,21 @@ silk_status World::debug_matrix(uint32_t h, double* dense, int64_t n) {
   return SILK_OK;
 }
 
+silk_status World::debug_mas_fine(uint32_t h, float* inv, int64_t ninv, float* diag,
+                                  int64_t ndiag) {
+  Cloth* c = find_cloth(h);
+  if (!c) return SILK_ERR_INVALID_HANDLE;
+  ensure_layout();
+  const ClothSetup& S = *c->setup;
+  const int64_t need = (int64_t)S.fine.nbank * BANK * (BANK + 1) / 2;
+  if (ninv != need || ndiag != S.nv || c->dev.fine.M.n < (size_t)need)
+    return SILK_ERR_INVALID_POSITION;
+  sync();
+  CUDA_CHECK(cudaMemcpy(inv, c->dev.fine.M.p, need * sizeof(float), cudaMemcpyDeviceToHost));
+  CUDA_CHECK(cudaMemcpy(diag, lhs.p + c->voff, S.nv * sizeof(float), cudaMemcpyDeviceToHost));
+  return SILK_OK;
+}
+
 silk_status World::debug_refit(const float* disp, int64_t n) {
   if (!initialized) return SILK_ERR_NOT_INITIALIZED;
   ensure_layout();

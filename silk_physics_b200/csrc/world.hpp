@@ -186,6 +186,7 @@ class World {
   silk_status debug_partition(uint32_t h, int* perm, int64_t perm_len,
                               int* offs, int64_t cap, int* nparts);
   silk_status debug_matrix(uint32_t h, double* dense, int64_t n);
+  silk_status debug_mas_fine(uint32_t h, float* inv, int64_t ninv, float* diag, int64_t ndiag);
   silk_status debug_refit(const float* disp, int64_t n);
   silk_status debug_candidates(int* out, int64_t cap, int* n);
   silk_status debug_dcd(float t, float dact, int* keys, int64_t cap, int* n);

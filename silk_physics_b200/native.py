@@ -273,6 +273,7 @@ def _load() -> C.CDLL:
         "silk_ccd_batch_noalloc": ([C.c_int32, C.c_void_p, C.c_int64, _F32P, C.c_void_p,
                                     C.c_float, C.c_int32, C.c_float, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)], C.c_int),
+        "silk_debug_mas_fine": ([_W, C.c_uint32, _F32P, C.c_int64, _F32P, C.c_int64], C.c_int),
         "silk_partition_mesh": ([_F32P, C.c_int64, _I32P, C.c_int64, _I32P, _I32P, C.c_int64,
                                  C.POINTER(C.c_int32)], C.c_int),
         "silk_schedule_bank_rows": ([_I32P, _I32P, _I32P, C.c_int32, C.c_int32, _I32P, _I32P],
@@ -446,6 +447,16 @@ class World:
         if st:
             raise RuntimeError(_result(st, self._w).to_string())
         return d.reshape(nv, nv)
+
+    def mas_fine(self, handle: int, nbank: int, nv: int) -> tuple[np.ndarray, np.ndarray]:
+        """(packed FP32 fine-bank inverses, nbank x 528; ADMM diagonal, nv)
+        of the last factorisation, solver order."""
+        inv = np.zeros(nbank * 528, np.float32)
+        diag = np.zeros(nv, np.float32)
+        st = lib.silk_debug_mas_fine(self._w, handle, inv, inv.size, diag, diag.size)
+        if st:
+            raise RuntimeError(_result(st, self._w).to_string())
+        return inv.reshape(nbank, 528), diag
 
     def debug_refit(self, disp=None) -> None:
         if disp is None:
