@@ -17,8 +17,9 @@
 //  * where the hierarchy allows it (every fine bank one coarse node, small
 //    upper levels) the solve runs in the resident form: one block per
 //    first-level coarse bank keeps its vertices' CG vectors in registers and
-//    its bank inverses in shared memory, three barriers per iteration, and
-//    BF16-stored inverses are applied with mma.sync (FP32 accumulation).
+//    its bank inverses in shared memory, two grid or cluster barriers per
+//    iteration, and BF16-stored inverses are applied with mma.sync (FP32
+//    accumulation).
 #include <cooperative_groups.h>
 #include <cuda/atomic>
 
@@ -549,18 +550,21 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel_cluster(CgArgs a) {
 // 32k+w, lane = slot).  Every vertex's x, r, p, Ap and its MAS output stay
 // in registers for the whole solve; the block's fine and first-level bank
 // inverses and the (few) banks of all higher levels are staged in shared
-// memory once per solve.  Only p crosses blocks (through a global exchange
-// buffer; neighbours inside the block are read from shared memory), plus the
+// memory once per solve.  What crosses blocks: each vertex's two-level z
+// (fine + first coarse level) for the blocks whose halo holds it, the
 // per-block partial sums and the residual restricted to the second coarse
-// level, which every block then solves redundantly.  That leaves three
-// barriers per iteration:
-//   A  totals, coarse levels >= 2, p = z + beta p, publish p      | barrier
-//   B  Ap = A p (sliced ELL, bank-aligned slices), p.Ap partial    | barrier
+// level, which every block then solves redundantly.  Each block computes p
+// at its halo vertices itself with the owner's operations (bit-identical),
+// so p needs no barrier of its own (when a block's halo overflows its
+// shared-memory slots, p is published through the grid as well):
+//   A  totals, coarse levels >= 2, p = z + beta p (own and halo)   | block barrier
+//   B  Ap = A p (bank-sliced ELL in a bank-group-conflict-free     |
+//      order, vertex and halo slots in shared memory), p.Ap partial | barrier
 //   C  alpha, x/r update, fine and first-level MAS, restriction,   | barrier
-//      r.z and r.r partials
-// The arithmetic of each vector entry is that of cg_kernel; only the order
-// of the FP64 block sums (and of the off-diagonal terms of a row: entries
-// from other blocks first) differs.
+//      two-level z published, r.z and r.r partials
+// The arithmetic of each vector entry is that of cg_kernel except the order
+// of the FP64 block sums, of the off-diagonal terms of a row (the scheduled
+// order) and of the upper-level bank solves (columns split over warps).
 // ---------------------------------------------------------------------------
 constexpr int kResWarps = kResThreads / 32;
 static_assert(kResCoarseBanks <= kResWarps, "one warp per upper coarse bank");
