@@ -1118,10 +1118,12 @@ __global__ void contact_gs_kernel(const ContactDev* contacts, const int* groups,
           unew = us;
         } else {
           float3 ut = sub3(us, sc3(un, k.normal));
-          float utn = sqrtf(dot3(ut, ut));
+          // Stick when |ut| <= radius (compared squared), else scale ut by
+          // 1 - radius / |ut| with one reciprocal square root.
+          float ut2 = dot3(ut, ut);
           float radius = -k.friction * un;
-          unew = utn <= radius ? make_float3(0.f, 0.f, 0.f)
-                               : sc3(1.0f - radius / utn, ut);
+          unew = ut2 <= radius * radius ? make_float3(0.f, 0.f, 0.f)
+                                        : sc3(1.0f - radius * rsqrtf(ut2), ut);
         }
         float3 du = sub3(unew, u);
         float3 nc = add3(old, du);
@@ -1264,9 +1266,12 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
         unew = us;
       } else {
         float3 ut = sub3(us, sc3(un, kc.normal));
-        float utn = sqrtf(dot3(ut, ut));
+        // Stick when |ut| <= radius (compared squared), else scale ut by
+        // 1 - radius / |ut| with one reciprocal square root.
+        float ut2 = dot3(ut, ut);
         float radius = -kc.friction * un;
-        unew = utn <= radius ? make_float3(0.f, 0.f, 0.f) : sc3(1.0f - radius / utn, ut);
+        unew = ut2 <= radius * radius ? make_float3(0.f, 0.f, 0.f)
+                                      : sc3(1.0f - radius * rsqrtf(ut2), ut);
       }
       float3 du = sub3(unew, u);
       float3 nc = add3(old, du);
@@ -1394,9 +1399,12 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
         unew = us;
       } else {
         float3 ut = sub3(us, sc3(un, kc.normal));
-        float utn = sqrtf(dot3(ut, ut));
+        // Stick when |ut| <= radius (compared squared), else scale ut by
+        // 1 - radius / |ut| with one reciprocal square root.
+        float ut2 = dot3(ut, ut);
         float radius = -kc.friction * un;
-        unew = utn <= radius ? make_float3(0.f, 0.f, 0.f) : sc3(1.0f - radius / utn, ut);
+        unew = ut2 <= radius * radius ? make_float3(0.f, 0.f, 0.f)
+                                      : sc3(1.0f - radius * rsqrtf(ut2), ut);
       }
       float3 du = sub3(unew, u);
       float3 nc = add3(old, du);
