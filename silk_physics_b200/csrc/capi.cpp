@@ -337,8 +337,10 @@ silk_status silk_partition_mesh(const float* verts, int64_t verts_len,
                                 const int32_t* faces, int64_t faces_len,
                                 int32_t* perm, int32_t* part_offsets,
                                 int64_t offsets_cap, int32_t* nparts) {
-  if (!verts || !faces || !perm || !part_offsets || !nparts)
+  if (!verts || !faces || !perm || !part_offsets || !nparts || verts_len < 0 || faces_len < 0)
     return SILK_ERR_INVALID_CONFIG;
+  if (!silkb::check_mesh_indices(verts, (long)verts_len, faces, (long)faces_len).empty())
+    return SILK_ERR_INVALID_MESH;
   try {
     std::vector<int> p, off;
     int nv = (int)(verts_len / 3), nf = (int)(faces_len / 3);

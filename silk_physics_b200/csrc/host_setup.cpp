@@ -48,6 +48,12 @@ std::string check_finite_and_index(const float* v, long nvf, const int* f,
 
 }  // namespace
 
+std::string check_mesh_indices(const float* v, long nvf, const int* f, long nfi) {
+  std::string r = check_schema(v, nvf, f, nfi, 0, 0);
+  if (!r.empty()) return r;
+  return check_finite_and_index(v, nvf, f, nfi);
+}
+
 std::string check_cloth_mesh(const float* v, long nvf, const int* f, long nfi) {
   std::string r = check_schema(v, nvf, f, nfi, 3, 1);
   if (!r.empty()) return r;

@@ -18,6 +18,10 @@ struct ClothParams {
 
 // Checks of common/mesh.cpp:231-276 (cloth) and :278-303 (obstacle).
 // Returns an empty string when valid, otherwise the reason.
+// Sizes, finite positions and face indices in range (the part of the mesh
+// checks every consumer of a face list needs); "" if valid.
+std::string check_mesh_indices(const float* verts, long nverts_floats, const int* faces,
+                               long nfaces_ints);
 std::string check_cloth_mesh(const float* verts, long nverts_floats,
                              const int* faces, long nfaces_ints);
 std::string check_obstacle_mesh(const float* verts, long nverts_floats,
