@@ -626,8 +626,18 @@ def run_reference(args) -> None:
     offs = np.unique(np.append(np.arange(0, nv, 32), nv)).astype(np.int32)
     h = ow.add_cloth(V, F, [], perm, offs)
     ow.add_obstacle(SV, SF)
+    # The oracle's own state after the default 24 prelude + 3 warm-up steps
+    # (oracle/make_reference_state.py) spares replaying them on the host
+    # cores; further untimed steps run from there when more are asked for.
+    state = ROOT / "oracle" / "reference_state_c2_step27.npz"
+    start = args.prelude + args.warmup
+    done = 0
+    if args.cg_rel_tol == 1e-5 and start >= 27 and state.exists():
+        st = np.load(state)
+        ow.set_state(h, st["x"], st["v"])
+        done = int(st["steps"])
     t_pre = time.perf_counter()
-    for _ in range(args.prelude + args.warmup):
+    for _ in range(start - done):
         ow.step()
     pre = time.perf_counter() - t_pre
     times = []
@@ -641,8 +651,10 @@ def run_reference(args) -> None:
         if time.perf_counter() - t0 > args.cpu_budget and len(times) >= 1:
             break
     value = len(times) / sum(times)
-    sample = (f"{len(times)} timed step(s) after {args.prelude + args.warmup} untimed "
-              f"({pre:.1f} s), {admm} ADMM iterations, OpenMP on {threads} threads")
+    origin = (f"from the oracle's stored state after {done} steps, "
+              f"{start - done} more untimed" if done else f"after {start} untimed steps")
+    sample = (f"{len(times)} timed step(s) {origin} ({pre:.1f} s), {admm} ADMM iterations, "
+              f"OpenMP on {threads} threads")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "steps/s",
         "n_gpus": world_size, "steps": len(times), "warmup": args.warmup,

@@ -2332,6 +2332,21 @@ int oracle_get_cloth_position(void* w, uint32_t h, float* out, int n) {
   return a->fp64 ? impl(*a->d) : impl(*a->f);
 }
 
+int oracle_get_cloth_velocity(void* w, uint32_t h, float* out, int n) {
+  AnyWorld* a = (AnyWorld*)w;
+  auto impl = [&](auto& W) {
+    for (auto& c : W.cloths)
+      if (c.id == h) {
+        if (n != 3 * c.nv) return 7;
+        for (int i = 0; i < c.nv; ++i)
+          for (int d = 0; d < 3; ++d) out[3 * i + d] = (float)c.v[3 * c.perm[i] + d];
+        return 0;
+      }
+    return 4;
+  };
+  return a->fp64 ? impl(*a->d) : impl(*a->f);
+}
+
 int oracle_get_cloth_position_f64(void* w, uint32_t h, double* out, int n) {
   AnyWorld* a = (AnyWorld*)w;
   auto impl = [&](auto& W) {

@@ -84,6 +84,8 @@ int oracle_set_cloth_state(void* w, uint32_t h, const float* x, const float* v,
                            int n);
 int oracle_get_cloth_position(void* w, uint32_t h, float* out, int n);
 int oracle_get_cloth_position_f64(void* w, uint32_t h, double* out, int n);
+/* Velocities (original vertex order). */
+int oracle_get_cloth_velocity(void* w, uint32_t h, float* out, int n);
 int oracle_get_stats(void* w, oracle_stats* s);
 
 /* Assembled static system of one cloth, solver order: the scalar V x V matrix

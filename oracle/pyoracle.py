@@ -146,6 +146,16 @@ class OracleWorld:
         return self.L.oracle_set_cloth_state(self.w, h, _p(xs, C.c_float), _p(vs, C.c_float),
                                              xs.size)
 
+    def position_f32(self, h) -> np.ndarray:
+        out = np.zeros(3 * self.nv[h], np.float32)
+        assert self.L.oracle_get_cloth_position(self.w, h, _p(out, C.c_float), out.size) == 0
+        return out.reshape(-1, 3)
+
+    def velocity(self, h) -> np.ndarray:
+        out = np.zeros(3 * self.nv[h], np.float32)
+        assert self.L.oracle_get_cloth_velocity(self.w, h, _p(out, C.c_float), out.size) == 0
+        return out.reshape(-1, 3)
+
     def position(self, h) -> np.ndarray:
         out = np.zeros(3 * self.nv[h], np.float64)
         assert self.L.oracle_get_cloth_position_f64(self.w, h, _p(out, C.c_double),

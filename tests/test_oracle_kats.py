@@ -118,3 +118,19 @@ def test_touching_boxes_are_candidates(oracle):
     ow.refit()
     c = ow.candidates()
     assert len(c) > 0
+
+
+def test_reference_arm_state_file():
+    """The stored oracle state the reference arm of bench.py starts from:
+    the 80x80 benchmark sheet after 27 steps, finite, in contact range of
+    the sphere (z of the lowest vertex near its top at 0.3 m)."""
+    from pathlib import Path
+
+    import numpy as np
+
+    st = np.load(Path(__file__).resolve().parent.parent / "oracle" /
+                 "reference_state_c2_step27.npz")
+    assert int(st["steps"]) == 27
+    assert st["x"].shape == (6400, 3) and st["v"].shape == (6400, 3)
+    assert np.isfinite(st["x"]).all() and np.isfinite(st["v"]).all()
+    assert 0.0 < st["x"][:, 2].min() < 0.6
