@@ -7,11 +7,24 @@
 #include <chrono>
 #include <cstring>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "collision.cuh"
 #include "world.hpp"
 #include "learned.cuh"
 
 namespace silkb {
+
+namespace {
+// Named host range for profiler timelines (nsys, ncu's NVTX filters); a
+// cheap no-op when no tool is attached.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+}  // namespace
 
 namespace {
 
@@ -976,6 +989,7 @@ silk_status World::get_cloth_velocity(uint32_t h, float* out, int64_t n) {
 }
 
 bool World::admm_solve() {
+  NvtxRange admm_range("ADMM solve");
   SolverView s = view();
   cudaStream_t st = stream;
   launch_compute_inertia(s, st);
@@ -1079,6 +1093,7 @@ bool World::admm_solve() {
 }
 
 silk_status World::solver_step() {
+  NvtxRange step_range("silk::solver_step");
   if (!initialized) return SILK_ERR_NOT_INITIALIZED;
   try {
     long long launches0 = g_launch_count;
@@ -1117,6 +1132,7 @@ silk_status World::solver_step() {
       float pad = coll_->scene_padding();
       ms = 0.2f * pad;
       dact = 1.0f * pad;
+      NvtxRange dcd_range("refit + DCD + contact rebuild");
       auto t0 = clk::now();
       coll_->refit(outer.p, outer.p);
       coll_->append_active(0.0f, dact);
@@ -1124,6 +1140,7 @@ silk_status World::solver_step() {
     }
     float remaining = 1.0f;
     for (int oit = 0; oit < g.max_outer_iteration; ++oit) {
+      NvtxRange outer_range("outer iteration");
       stats.outer_iterations += 1;
       launch_predict(nv, g.dt, make_float4(g.acceleration_x, g.acceleration_y, g.acceleration_z, 0.f),
                      outer.p, outer_v.p, x.p, st);
@@ -1149,6 +1166,7 @@ silk_status World::solver_step() {
       prof.admm_host_ms += ms_since(t_admm);
       float toi = remaining;
       if (collide) {
+        NvtxRange ccd_range("refit + CCD");
         auto t0 = clk::now();
         coll_->refit(x.p, outer.p);
         int nq = 0, nh = 0;
@@ -1167,6 +1185,7 @@ silk_status World::solver_step() {
       float frac = rollback / remaining;
       launch_mix(nv, frac, x.p, outer.p, st);
       remaining -= rollback;
+      NvtxRange dcd_range("refit + DCD + contact rebuild");
       auto t0 = clk::now();
       coll_->refit(outer.p, outer.p);
       coll_->append_active(1.0f - remaining, dact);
