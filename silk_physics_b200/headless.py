@@ -56,11 +56,13 @@ def _fan(poly):
 
 def _load_obj(path: Path):
     verts, faces = [], []
-    for line in path.read_text().splitlines():
+    for lineno, line in enumerate(path.read_text().splitlines(), 1):
         parts = line.split()
         if not parts:
             continue
-        if parts[0] == "v" and len(parts) >= 4:
+        if parts[0] == "v":
+            if len(parts) < 4:
+                raise ValueError(f"line {lineno}: a vertex needs three coordinates")
             verts.append([float(parts[1]), float(parts[2]), float(parts[3])])
         elif parts[0] == "f":
             idx = []
@@ -132,8 +134,7 @@ def _load_ply(path: Path):
                         row.append(float(toks[p]))
                         p += 1
                 if name == "vertex":
-                    names = [pr[-1] for pr in props]
-                    verts.append([row[names.index(a)] for a in ("x", "y", "z")])
+                    verts.append(_ply_xyz(row, props))
                 elif name == "face":
                     faces.extend(_fan(row[0]))
     else:
@@ -156,11 +157,19 @@ def _load_ply(path: Path):
                         p += struct.calcsize(t)
                         row.append(v)
                 if name == "vertex":
-                    names = [pr[-1] for pr in props]
-                    verts.append([row[names.index(a)] for a in ("x", "y", "z")])
+                    verts.append(_ply_xyz(row, props))
                 elif name == "face":
                     faces.extend(_fan(row[0]))
     return np.asarray(verts, np.float32), np.asarray(faces, np.int32)
+
+
+def _ply_xyz(row, props):
+    names = [pr[-1] for pr in props]
+    missing = [a for a in ("x", "y", "z") if a not in names]
+    if missing:
+        raise ValueError(f"vertex element without propert{'y' if len(missing) == 1 else 'ies'} "
+                         f"{', '.join(missing)}")
+    return [row[names.index(a)] for a in ("x", "y", "z")]
 
 
 def _load_stl(path: Path):
@@ -174,7 +183,12 @@ def _load_stl(path: Path):
                 vs.append([float(parts[1]), float(parts[2]), float(parts[3])])
         tris = np.asarray(vs, np.float32).reshape(-1, 3, 3)
     else:
+        if len(data) < 84:
+            raise ValueError("binary STL shorter than its 84-byte header")
         (n,) = struct.unpack_from("<I", data, 80)
+        if len(data) < 84 + 50 * n:
+            raise ValueError(f"binary STL declares {n} triangles but holds "
+                             f"{(len(data) - 84) // 50}")
         rec = np.frombuffer(data, dtype=np.dtype([("n", "<f4", 3), ("v", "<f4", (3, 3)),
                                                   ("a", "<u2")]), count=n, offset=84)
         tris = rec["v"].astype(np.float32)
@@ -189,9 +203,14 @@ def load_mesh(path: Path):
     loader = {".obj": _load_obj, ".off": _load_off, ".ply": _load_ply, ".stl": _load_stl}.get(ext)
     if loader is None:
         raise ValueError(f"{path}: unsupported mesh format {ext}")
-    V, F = loader(path)
+    try:
+        V, F = loader(path)
+    except (IndexError, KeyError, struct.error, UnicodeDecodeError, ValueError) as e:
+        raise ValueError(f"{path}: malformed {ext[1:].upper()} file ({e})") from e
     if len(V) == 0 or len(F) == 0:
         raise ValueError(f"{path}: empty mesh")
+    if F.min() < 0 or F.max() >= len(V):
+        raise ValueError(f"{path}: face index out of range ({len(V)} vertices)")
     return V, F
 
 
@@ -283,6 +302,9 @@ def load_scene(path: str | Path):
         if not mesh.is_absolute():
             cand = path.parent / mesh
             mesh = cand if cand.exists() else mesh
+        if not mesh.exists():
+            raise FileNotFoundError(f"{path}: mesh {o['mesh']!r} not found (looked beside the "
+                                    f"scene file and in the working directory)")
         V, F = load_mesh(mesh)
         V = apply_transform(V, o.get("transform"))
         kind = o["type"].lower()

@@ -91,6 +91,37 @@ def test_pin_selection_bbox():
     assert set(pins.tolist()) == {i for i, v in enumerate(V) if v[1] >= 0.4 and v[0] <= 0.6}
 
 
+def test_malformed_meshes_raise_clear_errors(tmp_path):
+    """Truncated or inconsistent mesh files fail with the file, the format
+    and the reason, not with an index or buffer error from the parser."""
+    cases = {
+        "short.obj": ("v 0 0\nf 1 2 3\n", "vertex needs three coordinates"),
+        "oob.obj": ("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 9\n", "face index out of range"),
+        "noy.ply": ("ply\nformat ascii 1.0\nelement vertex 1\nproperty float x\n"
+                    "end_header\n0\n", "without properties y, z"),
+        "bad.off": ("OFF\n3 1 0\n0 0 0\n1 0 0\n", "malformed OFF file"),
+    }
+    for name, (text, msg) in cases.items():
+        f = tmp_path / name
+        f.write_text(text)
+        with pytest.raises(ValueError, match=msg):
+            H.load_mesh(f)
+    stl = tmp_path / "short.stl"
+    stl.write_bytes(b"\0" * 80 + struct.pack("<I", 5))
+    with pytest.raises(ValueError, match="declares 5 triangles but holds 0"):
+        H.load_mesh(stl)
+    with pytest.raises(ValueError, match="unsupported mesh format"):
+        H.load_mesh(tmp_path / "x.xyz")
+
+
+def test_scene_with_missing_mesh_names_it(tmp_path):
+    scene = tmp_path / "scene.json"
+    scene.write_text(json.dumps({"global": {}, "objects": [
+        {"type": "cloth", "name": "a", "mesh": "nope.obj"}]}))
+    with pytest.raises(FileNotFoundError, match="'nope.obj' not found"):
+        H.load_scene(scene)
+
+
 def _scene_files(tmp_path, steps=3):
     V, F = S.grid_sheet(16, side=0.5, z=0.0, jitter=1e-4, seed=3)
     with open(tmp_path / "sheet.obj", "w") as f:
