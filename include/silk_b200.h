@@ -105,6 +105,13 @@ typedef struct {
                                  through the grid (applies when the solver
                                  layout is built: first step after a change of
                                  the cloths); 0: 1024 */
+  int32_t barrier_spin_limit; /* > 0: polls after which a CG grid-barrier wait
+                                 gives up (the step then returns
+                                 SILK_ERR_ITERATIVE_SOLVE_FAIL); 0: 2^22 */
+  int32_t debug_withhold_block; /* failure-detection tests: k > 0 makes block
+                                 k - 1 of a cooperative-grid CG launch skip its
+                                 barrier arrivals, so the other blocks' bounded
+                                 waits run out; 0: off */
 } silk_solver_options;
 
 /* CUDA-event timing of the persistent CG kernel over the steps since the
@@ -215,6 +222,15 @@ silk_status silk_get_profile(silk_world* w, silk_profile* p, int32_t reset);
 /* Vertex velocities of a cloth in mesh order (3 * vertex count floats). */
 silk_status silk_get_cloth_velocity(const silk_world* w, uint32_t handle,
                                     float* velocity, int64_t velocity_len);
+/* Restart a cloth from a stored state: positions and velocities in mesh
+ * order (3 * vertex count floats each; velocity NULL = at rest).  Positions
+ * and velocities are the whole state carried between steps (contacts are
+ * rebuilt by DCD and the ADMM variables reset when a step begins,
+ * main_loop.cu:140-176), so a step from here equals the step the stored
+ * simulation took next.  Non-finite values give SILK_ERR_INVALID_POSITION. */
+silk_status silk_set_cloth_state(silk_world* w, uint32_t handle, const float* position,
+                                 int64_t position_len, const float* velocity,
+                                 int64_t velocity_len);
 
 /* Phase trace of the last CG solve of a cloth, recorded when the solver
  * option profile is 2: [0],[1] globaltimer (ns) and clock64 at kernel entry,
@@ -298,6 +314,14 @@ silk_status silk_ccd_batch(int32_t is_vertex_face, const float* x, int64_t n,
                            const float* err3, const float* min_separation,
                            float tolerance, int32_t max_iter, float max_time,
                            int32_t* hit, float* toi, float* t_upper);
+/* The contact Gauss-Seidel's Coulomb projection run on the GPU for n
+ * (free displacement u, unit normal, friction coefficient) triples: the
+ * device function every contact projection of a step uses
+ * (solve_coulomb_contact, contact_constraints.cu:391-411); out receives n x 3
+ * projected displacements.  Inspection entry point for the known-answer
+ * tests of test/friction_contact_test.cu:23-92. */
+silk_status silk_debug_coulomb(const float* u, const float* normal, const float* friction,
+                               int64_t n, float* out);
 /* Contact colouring of n contacts given 4 vertex ids each (-1 = immovable)
  * and 64-bit priorities: greedy colouring in decreasing priority order. */
 silk_status silk_color_contacts(const int32_t* verts4, const uint64_t* prio,
@@ -363,7 +387,14 @@ silk_status silk_mlp_train(float* params, const float* features, const float* ta
  * 1 <= max_iter <= SILK_CCD_NOALLOC_MAX_ITER; outside them the call returns
  * SILK_ERR_INVALID_CONFIG before touching the device.  Host (non-device)
  * or misaligned buffers, NULL pointers and n < 0 also give
- * SILK_ERR_INVALID_CONFIG; a CUDA error gives SILK_ERR_UNKNOWN.
+ * SILK_ERR_INVALID_CONFIG, and so does a `stream` that is being captured
+ * (the call reads its counters back and synchronises the stream, so it
+ * refuses such a stream before queuing anything on it); a CUDA error gives
+ * SILK_ERR_UNKNOWN.  If a query's search ever needed more pending boxes than
+ * its second-pass storage region holds (not reachable within the limits:
+ * a search keeps at most max_iter + 2 pending boxes), that query is reported
+ * as a hit at time 0 with t_upper = max_time and the call returns
+ * SILK_ERR_UNKNOWN after writing every other query's result.
  *
  * The first call on each device (any n, 0 included) looks up the scratch
  * array's address, which loads the library's kernels onto that device; make
@@ -372,7 +403,10 @@ silk_status silk_mlp_train(float* params, const float* features, const float* ta
  * calls on one device share the one scratch array: overlapping calls would
  * race on it, so calls on the same device from several host threads are
  * serialised by a lock inside the library and each holds it until its work
- * on the device has finished. */
+ * on the device has finished, also when it returns an error after queuing
+ * work.  The scratch address is looked up once per device and kept for the
+ * life of the process: do not call this entry point again on a device after
+ * cudaDeviceReset has destroyed the context it was looked up in. */
 #define SILK_CCD_NOALLOC_MAX_QUERIES (1 << 20)
 #define SILK_CCD_NOALLOC_MAX_ITER 4096
 silk_status silk_ccd_batch_noalloc(int32_t is_vertex_face, const float* x,

@@ -13,10 +13,18 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "build" / "liboracle.so"
+# The reference's own CPU CCD (silk/src/backend/cpu/collision/ccd.cpp,
+# interval_root_finder.cpp, interval.cpp) compiled unchanged by `make ref`
+# where the reference checkout is present; the built library travels with
+# the tree.
+REF_LIB = HERE / "_ref" / "libref_ccd.so"
+REF_CHECKOUT = Path("/root/reference")
 
 
 def build() -> Path:
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    if (REF_CHECKOUT / "silk" / "src" / "backend" / "cpu" / "collision" / "ccd.cpp").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={REF_CHECKOUT}"], check=True)
     return LIB
 
 
@@ -238,3 +246,62 @@ def color_contacts(verts4, prio):
     out = np.zeros(p.size, np.int32)
     nc = L.oracle_color_contacts(_p(v, C.c_int), _p(p, C.c_uint64), p.size, _p(out, C.c_int))
     return out, nc
+
+
+_ref_lib = None
+
+
+def ref_available() -> bool:
+    return REF_LIB.exists()
+
+
+def ref_lib() -> C.CDLL:
+    """The reference's own CCD (oracle/_ref/libref_ccd.so)."""
+    global _ref_lib
+    if _ref_lib is None:
+        if not REF_LIB.exists():
+            raise FileNotFoundError(f"{REF_LIB} is not built (make -C oracle ref)")
+        _ref_lib = C.CDLL(str(REF_LIB))
+        _ref_lib.ref_ccd.restype = C.c_int
+        _ref_lib.ref_ccd.argtypes = [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                     C.c_float, C.c_float, C.c_long, C.c_int, C.c_float,
+                                     C.POINTER(C.c_float), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_float)]
+        _ref_lib.ref_numerical_error.restype = None
+    return _ref_lib
+
+
+def ref_ccd(is_vf: bool, x24, err3, ms, tol=1e-6, max_iter=4096, no_zero_toi=True,
+            max_time=1.0):
+    """silk::cpu::vertex_face_ccd / edge_edge_ccd of the reference itself:
+    (hit, t4 = [t_lo, t_hi, small_ms_t_lo, small_ms_t_hi], use_small_ms,
+    tolerance)."""
+    L = ref_lib()
+    x = np.ascontiguousarray(x24, np.float32).ravel()
+    e = np.ascontiguousarray(err3, np.float32).ravel()
+    t4 = np.zeros(4, np.float32)
+    small = C.c_int(0)
+    tolr = C.c_float(0.0)
+    hit = L.ref_ccd(int(is_vf), _p(x, C.c_float), _p(e, C.c_float), C.c_float(ms),
+                    C.c_float(tol), C.c_long(max_iter), int(no_zero_toi), C.c_float(max_time),
+                    _p(t4, C.c_float), C.byref(small), C.byref(tolr))
+    return bool(hit), t4, bool(small.value), float(tolr.value)
+
+
+def ref_ccd_toi(is_vf, x24, err3, ms, tol=1e-6, max_iter=4096, max_time=1.0):
+    """The reference's answer as the solver step consumes it: (hit, toi,
+    t_upper) from the accepted interval, or from the refined-separation
+    interval when the first starts at 0 (ccd.cpp:150-180 with
+    narrowphase.cu:66)."""
+    hit, t4, small, _ = ref_ccd(is_vf, x24, err3, ms, tol, max_iter, True, max_time)
+    if not hit:
+        return False, max_time, max_time
+    return True, float(t4[2] if small else t4[0]), float(t4[3] if small else t4[1])
+
+
+def ref_numerical_error(absmax3, is_vf: bool) -> np.ndarray:
+    L = ref_lib()
+    a = np.ascontiguousarray(absmax3, np.float32).ravel()
+    out = np.zeros(3, np.float32)
+    L.ref_numerical_error(_p(a, C.c_float), int(is_vf), _p(out, C.c_float))
+    return out

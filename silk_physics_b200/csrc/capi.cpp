@@ -243,6 +243,14 @@ silk_status silk_get_profile(silk_world* w, silk_profile* p, int32_t reset) {
   return guard(w, [&](World& W) { return W.get_profile(p, reset != 0); });
 }
 
+silk_status silk_set_cloth_state(silk_world* w, uint32_t handle, const float* position,
+                                 int64_t position_len, const float* velocity,
+                                 int64_t velocity_len) {
+  return guard_init(w, [&](World& x) {
+    return x.set_cloth_state(handle, position, position_len, velocity, velocity_len);
+  });
+}
+
 silk_status silk_get_cloth_velocity(const silk_world* w, uint32_t handle,
                                     float* velocity, int64_t velocity_len) {
   if (!velocity && velocity_len != 0) return SILK_ERR_INVALID_POSITION;
@@ -404,6 +412,17 @@ silk_status silk_ccd_batch(int32_t is_vertex_face, const float* x, int64_t n,
   try {
     silkb::ccd_batch_host(is_vertex_face != 0, x, n, err3, min_separation,
                           tolerance, max_iter, max_time, hit, toi, t_upper);
+    return SILK_OK;
+  } catch (...) {
+    return SILK_ERR_UNKNOWN;
+  }
+}
+
+silk_status silk_debug_coulomb(const float* u, const float* normal, const float* friction,
+                              int64_t n, float* out) {
+  if (n < 0 || (n > 0 && (!u || !normal || !friction || !out))) return SILK_ERR_INVALID_CONFIG;
+  try {
+    silkb::coulomb_debug_host(u, normal, friction, n, out);
     return SILK_OK;
   } catch (...) {
     return SILK_ERR_UNKNOWN;

@@ -361,6 +361,24 @@ __device__ __forceinline__ float3 sc3(float s, float3 a) {
 __device__ __forceinline__ float dot3(float3 a, float3 b) {
   return a.x * b.x + a.y * b.y + a.z * b.z;
 }
+
+// Exact Signorini-Coulomb projection of one contact's free displacement us
+// onto the friction cone of unit normal n and coefficient mu: separating
+// displacements (us.n >= 0) stay, sticking ones (tangential part inside the
+// cone) become zero, sliding ones keep the tangential part shortened by the
+// cone radius (solve_coulomb_contact, contact_constraints.cu:391-411).  The
+// stick test compares squared lengths and the slide scales by
+// 1 - radius * rsqrt(|u_t|^2): one reciprocal square root instead of a square
+// root and a division.
+__device__ __forceinline__ float3 coulomb_project(float3 us, float3 n, float mu) {
+  float un = dot3(us, n);
+  if (un >= 0.0f) return us;
+  float3 ut = sub3(us, sc3(un, n));
+  float ut2 = dot3(ut, ut);
+  float radius = -mu * un;
+  return ut2 <= radius * radius ? make_float3(0.f, 0.f, 0.f)
+                                : sc3(1.0f - radius * rsqrtf(ut2), ut);
+}
 __device__ __forceinline__ float3 axpby3(float a, float3 x, float b, float3 y) {
   return make_float3(a * x.x + b * y.x, a * x.y + b * y.y, a * x.z + b * y.z);
 }
@@ -1111,20 +1129,7 @@ __global__ void contact_gs_kernel(const ContactDev* contacts, const int* groups,
         float4 o = corr[ci];
         float3 old = make_float3(o.x, o.y, o.z);
         float3 us = sub3(u, old);
-        // solve_coulomb_contact (contact_constraints.cu:391-411).
-        float un = dot3(us, k.normal);
-        float3 unew;
-        if (un >= 0.0f) {
-          unew = us;
-        } else {
-          float3 ut = sub3(us, sc3(un, k.normal));
-          // Stick when |ut| <= radius (compared squared), else scale ut by
-          // 1 - radius / |ut| with one reciprocal square root.
-          float ut2 = dot3(ut, ut);
-          float radius = -k.friction * un;
-          unew = ut2 <= radius * radius ? make_float3(0.f, 0.f, 0.f)
-                                        : sc3(1.0f - radius * rsqrtf(ut2), ut);
-        }
+        float3 unew = coulomb_project(us, k.normal, k.friction);
         float3 du = sub3(unew, u);
         float3 nc = add3(old, du);
         corr[ci] = make_float4(nc.x, nc.y, nc.z, 0.f);
@@ -1260,19 +1265,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
         }
       float3 old = make_float3(o.x, o.y, o.z);
       float3 us = sub3(u, old);
-      float un = dot3(us, kc.normal);
-      float3 unew;
-      if (un >= 0.0f) {
-        unew = us;
-      } else {
-        float3 ut = sub3(us, sc3(un, kc.normal));
-        // Stick when |ut| <= radius (compared squared), else scale ut by
-        // 1 - radius / |ut| with one reciprocal square root.
-        float ut2 = dot3(ut, ut);
-        float radius = -kc.friction * un;
-        unew = ut2 <= radius * radius ? make_float3(0.f, 0.f, 0.f)
-                                      : sc3(1.0f - radius * rsqrtf(ut2), ut);
-      }
+      float3 unew = coulomb_project(us, kc.normal, kc.friction);
       float3 du = sub3(unew, u);
       float3 nc = add3(old, du);
       ccorr[cur] = make_float4(nc.x, nc.y, nc.z, 0.f);
@@ -1393,19 +1386,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
         }
       float3 old = make_float3(o.x, o.y, o.z);
       float3 us = sub3(u, old);
-      float un = dot3(us, kc.normal);
-      float3 unew;
-      if (un >= 0.0f) {
-        unew = us;
-      } else {
-        float3 ut = sub3(us, sc3(un, kc.normal));
-        // Stick when |ut| <= radius (compared squared), else scale ut by
-        // 1 - radius / |ut| with one reciprocal square root.
-        float ut2 = dot3(ut, ut);
-        float radius = -kc.friction * un;
-        unew = ut2 <= radius * radius ? make_float3(0.f, 0.f, 0.f)
-                                      : sc3(1.0f - radius * rsqrtf(ut2), ut);
-      }
+      float3 unew = coulomb_project(us, kc.normal, kc.friction);
       float3 du = sub3(unew, u);
       float3 nc = add3(old, du);
       sc[cur] = make_float4(nc.x, nc.y, nc.z, 0.f);
@@ -2365,6 +2346,36 @@ __global__ void color_explicit_round(const int4* v4, const unsigned long long* p
 }
 }  // namespace
 
+namespace {
+__global__ void coulomb_debug_kernel(int n, const float* u, const float* nrm, const float* mu,
+                                     float* out) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  float3 r = coulomb_project(make_float3(u[3 * q], u[3 * q + 1], u[3 * q + 2]),
+                             make_float3(nrm[3 * q], nrm[3 * q + 1], nrm[3 * q + 2]), mu[q]);
+  out[3 * q] = r.x;
+  out[3 * q + 1] = r.y;
+  out[3 * q + 2] = r.z;
+}
+}  // namespace
+
+void coulomb_debug_host(const float* u, const float* nrm, const float* mu, int64_t n,
+                        float* out) {
+  if (n == 0) return;
+  DevBuf<float> ud, nd, md, od;
+  ud.alloc(3 * n);
+  nd.alloc(3 * n);
+  md.alloc(n);
+  od.alloc(3 * n);
+  CUDA_CHECK(cudaMemcpy(ud.p, u, 3 * n * sizeof(float), cudaMemcpyHostToDevice));
+  CUDA_CHECK(cudaMemcpy(nd.p, nrm, 3 * n * sizeof(float), cudaMemcpyHostToDevice));
+  CUDA_CHECK(cudaMemcpy(md.p, mu, n * sizeof(float), cudaMemcpyHostToDevice));
+  coulomb_debug_kernel<<<div_up((int)n, 256), 256>>>((int)n, ud.p, nd.p, md.p, od.p);
+  SILK_LAUNCHED();
+  CUDA_CHECK(cudaGetLastError());
+  CUDA_CHECK(cudaMemcpy(out, od.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost));
+}
+
 int color_contacts_host(const int* verts4, const uint64_t* prio, int64_t n, int* colors) {
   if (n == 0) return 0;
   int maxv = -1;
@@ -2460,7 +2471,11 @@ __global__ void __launch_bounds__(kNoAllocSpillSlots) ccd_batch_spill_kernel(
     float t = max_time, u = max_time;
     int s = ccd_query(vf, Pt, e, ms[q], tol, max_iter, max_time, t, u, st);
     if (s == 2) {
+      // Storage ran out: report the conservative answer (a hit at time 0).
       atomicAdd(&counters[1], 1);
+      hit[q] = 1;
+      toi[q] = 0.0f;
+      if (tup) tup[q] = max_time;
       continue;
     }
     hit[q] = s != 0 ? 1 : 0;
@@ -2492,6 +2507,15 @@ NoAllocStatus ccd_batch_noalloc(bool vf, const float* x, int64_t n, const float*
   if (n < 0 || !err3) return NoAllocStatus::kBadArgument;
   if (n > kNoAllocMaxQueries || max_iter < 1 || max_iter > kNoAllocMaxIter)
     return NoAllocStatus::kBeyondLimits;
+  // A stream under capture is refused before anything is queued on it: the
+  // call reads results back and synchronises, which would invalidate the
+  // caller's capture.
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &capture) != cudaSuccess ||
+      capture != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return NoAllocStatus::kBadArgument;
+  }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
     cudaGetLastError();
@@ -2519,19 +2543,30 @@ NoAllocStatus ccd_batch_noalloc(bool vf, const float* x, int64_t n, const float*
   int* list = reinterpret_cast<int*>(base + kNoAllocListOffset);
   IBox* spill = reinterpret_cast<IBox*>(base + kNoAllocSpillOffset);
   const float3 e3 = make_float3(err3[0], err3[1], err3[2]);
-  if (cudaMemsetAsync(counters, 0, 4 * sizeof(int), stream) != cudaSuccess)
+  // Any failure after work was queued waits for that work before returning,
+  // so the lock is released only once the scratch array is idle.
+  auto fail_after_queue = [&]() {
+    cudaGetLastError();
+    cudaStreamSynchronize(stream);
+    cudaGetLastError();
     return NoAllocStatus::kCudaError;
+  };
+  cudaGetLastError();  // an earlier, unrelated error is not this call's
+  if (cudaMemsetAsync(counters, 0, 4 * sizeof(int), stream) != cudaSuccess)
+    return fail_after_queue();
   CcdSpill first{nullptr, 0, nullptr, list, counters};
   ccd_batch_kernel<<<div_up((int)n, kCollThreads), kCollThreads, 0, stream>>>(
       vf, x, (int)n, e3, ms, tol, max_iter, max_time, hit, toi, t_upper, counters + 1, first);
   SILK_LAUNCHED();
+  if (cudaGetLastError() != cudaSuccess) return fail_after_queue();
   ccd_batch_spill_kernel<<<1, kNoAllocSpillSlots, 0, stream>>>(
       vf, x, e3, ms, tol, max_iter, max_time, hit, toi, t_upper, counters, list, spill);
   SILK_LAUNCHED();
-  if (cudaGetLastError() != cudaSuccess) return NoAllocStatus::kCudaError;
+  if (cudaGetLastError() != cudaSuccess) return fail_after_queue();
   int h[4] = {0, 0, 0, 0};
-  if (cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-      cudaStreamSynchronize(stream) != cudaSuccess) {
+  if (cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+    return fail_after_queue();
+  if (cudaStreamSynchronize(stream) != cudaSuccess) {
     cudaGetLastError();
     return NoAllocStatus::kCudaError;
   }

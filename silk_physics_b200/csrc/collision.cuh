@@ -58,6 +58,10 @@ void ccd_batch_host(bool vf, const float* x, int64_t n, const float* err3,
                     int* hit, float* toi, float* t_upper);
 int color_contacts_host(const int* verts4, const uint64_t* prio, int64_t n,
                         int* colors);
+// The contact Gauss-Seidel's Coulomb projection (coulomb_project) on n
+// (free displacement, unit normal, friction) triples.
+void coulomb_debug_host(const float* u, const float* nrm, const float* mu, int64_t n,
+                        float* out);
 
 // CCD batch on caller-owned device buffers of the current device that
 // allocates no memory: all working memory is a static device array.

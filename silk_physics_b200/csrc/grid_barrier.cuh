@@ -18,6 +18,10 @@ struct GridBarrier {
   unsigned* unused;
   unsigned nblocks;
   unsigned epoch = 0;  // barriers passed by this block
+  long long limit = kBarrierSpinLimit;  // polls before the wait gives up
+  // Failure-detection tests only: this block never arrives, so the others'
+  // waits run out (it waits, bounded by the same limit, for their error).
+  unsigned withhold = 0xffffffffu;
 
   __device__ bool sync() {
     __shared__ int s_ok;
@@ -32,6 +36,11 @@ struct GridBarrier {
       int ok = 1;
       if (e.load(cuda::memory_order_relaxed) != 0u) {
         ok = 0;
+      } else if (blockIdx.x == withhold) {
+        long long spins = 0;
+        while (e.load(cuda::memory_order_relaxed) == 0u && ++spins <= limit) __nanosleep(32);
+        e.store(1u, cuda::memory_order_relaxed);
+        ok = 0;
       } else {
         const unsigned target = epoch * nblocks;
         unsigned arrived = c.fetch_add(1u, cuda::memory_order_acq_rel) + 1u;
@@ -41,7 +50,7 @@ struct GridBarrier {
             ok = 0;
             break;
           }
-          if (++spins > kBarrierSpinLimit) {
+          if (++spins > limit) {
             e.store(1u, cuda::memory_order_relaxed);
             ok = 0;
             break;

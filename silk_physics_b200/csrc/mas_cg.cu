@@ -46,10 +46,14 @@ __global__ void galerkin_fill_kernel(GalerkinDev g, const double* src_vals,
 
 // Fill one 32x32 bank matrix in FP64 and invert it in place with symmetric
 // pivot sweeps (no pivoting; the bank matrices are SPD principal blocks of a
-// Galerkin operator, virtual slots are identity).
+// Galerkin operator, virtual slots are identity).  A zero or non-finite pivot,
+// or a non-finite inverse entry, sets kFailMasPivot in *fail and leaves the
+// bank's inverse zero, as batched_invert_upper rejects such a bank
+// (mas_preconditioner.cu:766-830, reported as a failed factorisation at
+// :854-858).
 __global__ void __launch_bounds__(256) bank_invert_kernel(
     MasLevelDev lv, int fine, const int* part_off, const double* src_vals,
-    const float* dyn) {
+    const float* dyn, int* fail) {
   __shared__ double A[BANK][BANK + 1];
   __shared__ double col[BANK], row[BANK];
   int bank = blockIdx.x;
@@ -74,6 +78,14 @@ __global__ void __launch_bounds__(256) bank_invert_kernel(
     }
     __syncthreads();
     double p = col[k];
+    if (!isfinite(p) || p == 0.0) {  // uniform: every thread reads the same pivot
+      if (threadIdx.x == 0 && fail) atomicOr(fail, kFailMasPivot);
+      for (int idx = threadIdx.x; idx < kPacked; idx += blockDim.x) {
+        if (lv.M) lv.M[(size_t)bank * kPacked + idx] = 0.0f;
+        if (lv.Mb) lv.Mb[(size_t)bank * kPacked + idx] = __float2bfloat16_rn(0.0f);
+      }
+      return;
+    }
     double inv = 1.0 / p;
     for (int e = threadIdx.x; e < BANK * BANK; e += blockDim.x) {
       int i = e / BANK, j = e % BANK;
@@ -95,6 +107,10 @@ __global__ void __launch_bounds__(256) bank_invert_kernel(
     }
     int j = i + rem;
     double v = A[i][j];
+    if (!isfinite((float)v)) {
+      if (fail) atomicOr(fail, kFailMasPivot);
+      v = 0.0;
+    }
     if (lv.M) lv.M[(size_t)bank * kPacked + idx] = (float)v;
     if (lv.Mb) lv.Mb[(size_t)bank * kPacked + idx] = __float2bfloat16_rn((float)v);
   }
@@ -401,7 +417,7 @@ __device__ __forceinline__ double blend_weight(double rr, double r_ra, double ra
 }
 
 __device__ __forceinline__ void mark_fail(const CgArgs& a) {
-  if (threadIdx.x == 0 && a.fail) atomicExch(a.fail, 1);
+  if (threadIdx.x == 0 && a.fail) atomicOr(a.fail, kFailBarrier);
 }
 
 template <class Barrier>
@@ -535,6 +551,8 @@ __device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm
 __global__ void __launch_bounds__(kCgThreads) cg_kernel(CgArgs a) {
   extern __shared__ float sm_all[];
   GridBarrier bar{a.barrier, a.barrier + 1, a.barrier + 2, gridDim.x};
+  if (a.barrier_spin_limit > 0) bar.limit = a.barrier_spin_limit;
+  if (a.withhold_block >= 0) bar.withhold = (unsigned)a.withhold_block;
   cg_body(a, bar, sm_all);
 }
 
@@ -739,7 +757,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
   int iter = -1;  // -1 while setting up (not traced)
   double* part = a.partials + 4 * k;
   auto fail = [&]() {
-    if (tid == 0 && a.fail) atomicExch(a.fail, 1);
+    if (tid == 0 && a.fail) atomicOr(a.fail, kFailBarrier);
   };
 
   // ---- one-time staging ----------------------------------------------------
@@ -1178,6 +1196,8 @@ __global__ void __launch_bounds__(kResThreads, 1) cg_resident_kernel(CgArgs a) {
   extern __shared__ __align__(16) unsigned char res_smem[];
   ResShared& s = *reinterpret_cast<ResShared*>(res_smem);
   GridBarrier bar{a.barrier, a.barrier + 1, a.barrier + 2, gridDim.x};
+  if (a.barrier_spin_limit > 0) bar.limit = a.barrier_spin_limit;
+  if (a.withhold_block >= 0) bar.withhold = (unsigned)a.withhold_block;
   res_body(a, bar, s);
 }
 
@@ -1226,11 +1246,11 @@ void launch_galerkin_fill(const GalerkinDev& g, const double* src_vals,
 }
 
 void launch_bank_invert(const MasLevelDev& lv, bool fine, const int* part_off,
-                        const double* src_vals, const float* dyn,
+                        const double* src_vals, const float* dyn, int* fail,
                         cudaStream_t st) {
   if (lv.nbank == 0) return;
   bank_invert_kernel<<<lv.nbank, 256, 0, st>>>(lv, fine ? 1 : 0, part_off,
-                                               src_vals, dyn);
+                                               src_vals, dyn, fail);
   SILK_LAUNCHED();
 }
 

@@ -8,6 +8,11 @@
 
 namespace silkb {
 
+// Bits of the solver failure word (World::cg_fail), read by the ADMM
+// convergence test and reported as IterativeSolveFail.
+constexpr int kFailBarrier = 1;   // a grid-barrier wait of a CG kernel gave up
+constexpr int kFailMasPivot = 2;  // a MAS bank had a zero or non-finite pivot
+
 constexpr int kPacked = BANK * (BANK + 1) / 2;  // 528 packed upper entries
 
 struct MasLevelDev {
@@ -84,7 +89,9 @@ struct CgArgs {
   const int* halo_off = nullptr;  // per block: first entry of its halo in halo_col
   const int* halo_col = nullptr;  // halo vertices (outside the block, read by its rows)
   int halo_full = 0;  // every off-block column of the resident rows is in its block's halo
-  int* fail = nullptr;          // set to 1 when a barrier wait gives up
+  int* fail = nullptr;          // kFail* bits: a barrier wait gave up
+  long long barrier_spin_limit = 0;  // > 0: grid-barrier polls before giving up
+  int withhold_block = -1;      // >= 0: that block skips its barrier arrivals (tests)
   // Optional phase trace of block 0 (null = off): [0] globaltimer and [1]
   // clock64 at entry, [2] and [3] at exit, [4] traced iterations, [5] kernel
   // form (0 streaming, 1 resident), then for each of the first kCgTraceIters
@@ -120,7 +127,7 @@ void launch_galerkin_fill(const GalerkinDev& g, const double* src_vals,
                           const float* dyn, cudaStream_t st);
 // mode 0: fine level (fill from L, add dynamic diagonal via part offsets).
 void launch_bank_invert(const MasLevelDev& lv, bool fine, const int* part_off,
-                        const double* src_vals, const float* dyn,
+                        const double* src_vals, const float* dyn, int* fail,
                         cudaStream_t st);
 int cg_grid_size(int nslices, int nbank0);
 void launch_cg(const CgArgs& a, int grid, cudaStream_t st);

@@ -254,6 +254,46 @@ silk_status World::get_cloth_position(uint32_t h, float* out, int64_t n) {
   return SILK_OK;
 }
 
+// Restart a cloth from a stored state.  The state between steps is exactly
+// the positions and velocities: contacts are rebuilt by DCD and the ADMM
+// variables reset at the start of every step (main_loop.cu:140-176).  The
+// warm-start feature history becomes the positions one and two steps back
+// along the given velocity.
+silk_status World::set_cloth_state(uint32_t h, const float* xin, int64_t nx,
+                                   const float* vin, int64_t nvel) {
+  Cloth* c = find_cloth(h);
+  if (!c) return SILK_ERR_INVALID_HANDLE;
+  const int nv = c->nv();
+  if (!xin || nx != 3 * (int64_t)nv || (vin && nvel != 3 * (int64_t)nv))
+    return SILK_ERR_INVALID_POSITION;
+  for (int64_t i = 0; i < nx; ++i)
+    if (!std::isfinite(xin[i]) || (vin && !std::isfinite(vin[i]))) {
+      last_error = "non-finite state";
+      return SILK_ERR_INVALID_POSITION;
+    }
+  ensure_layout();
+  std::vector<float4> xs(nv), vs(nv), h1(nv), h2(nv);
+  const auto& perm = c->setup->perm;
+  const float dt = g.dt;
+  for (int i = 0; i < nv; ++i) {
+    float px = xin[3 * i], py = xin[3 * i + 1], pz = xin[3 * i + 2];
+    float vx = vin ? vin[3 * i] : 0.f, vy = vin ? vin[3 * i + 1] : 0.f,
+          vz = vin ? vin[3 * i + 2] : 0.f;
+    int s = perm[i];
+    xs[s] = make_float4(px, py, pz, 0.f);
+    vs[s] = make_float4(vx, vy, vz, 0.f);
+    h1[s] = make_float4(px - dt * vx, py - dt * vy, pz - dt * vz, 0.f);
+    h2[s] = make_float4(px - 2.f * dt * vx, py - 2.f * dt * vy, pz - 2.f * dt * vz, 0.f);
+  }
+  const size_t bytes = nv * sizeof(float4);
+  CUDA_CHECK(cudaMemcpyAsync(sx.p + c->voff, xs.data(), bytes, cudaMemcpyHostToDevice, stream));
+  CUDA_CHECK(cudaMemcpyAsync(sv.p + c->voff, vs.data(), bytes, cudaMemcpyHostToDevice, stream));
+  CUDA_CHECK(cudaMemcpyAsync(hist1.p + c->voff, h1.data(), bytes, cudaMemcpyHostToDevice, stream));
+  CUDA_CHECK(cudaMemcpyAsync(hist2.p + c->voff, h2.data(), bytes, cudaMemcpyHostToDevice, stream));
+  sync();
+  return SILK_OK;
+}
+
 silk_status World::set_cloth_config(uint32_t h, const silk_cloth_config& cfg) {
   Cloth* c = find_cloth(h);
   if (!c) return SILK_ERR_INVALID_HANDLE;
@@ -845,10 +885,10 @@ void World::factorize(Cloth& c, cudaStream_t st) {
     gd.vals = d.gal[k].vals.p;
     launch_galerkin_fill(gd, k == 0 ? d.Lvals.p : d.gal[k - 1].vals.p, dyn, st);
   }
-  launch_bank_invert(d.cg.fine, true, d.part_off.p, d.Lvals.p, dyn, st);
+  launch_bank_invert(d.cg.fine, true, d.part_off.p, d.Lvals.p, dyn, cg_fail.p, st);
   for (int l = 1; l <= S.levels; ++l)
     launch_bank_invert(d.cg.coarse[l - 1], false, nullptr, d.gal[l - 1].vals.p,
-                       nullptr, st);
+                       nullptr, cg_fail.p, st);
 }
 
 float World::warm_sigma() const {
@@ -880,6 +920,8 @@ void World::cg_solve(Cloth& c, float rel_tol, bool first, cudaStream_t st) {
     a.trace = c.dev.cg_trace.p;
   }
   a.fail = cg_fail.p;
+  a.barrier_spin_limit = opt.barrier_spin_limit;
+  a.withhold_block = opt.debug_withhold_block - 1;
   const bool resident = c.dev.res_grid != 0 && opt.cg_form != 1;
   if (resident) stats.cg_resident_solves += 1;
   auto launch = [&]() {
@@ -1159,7 +1201,9 @@ silk_status World::solver_step() {
       if (!admm_solve()) {
         int f = 0;
         CUDA_CHECK(cudaMemcpy(&f, cg_fail.p, sizeof(int), cudaMemcpyDeviceToHost));
-        last_error = f ? "CG barrier wait gave up" : "solver diverged";
+        last_error = (f & kFailMasPivot) ? "MAS bank inverse failed: zero or non-finite pivot"
+                     : (f & kFailBarrier) ? "CG barrier wait gave up"
+                                          : "solver diverged";
         if (f) cg_fail.zero(st);
         return SILK_ERR_ITERATIVE_SOLVE_FAIL;
       }

@@ -178,6 +178,8 @@ class World {
   silk_status get_profile(silk_profile* p, bool reset);
   silk_status debug_cg_trace(uint32_t h, int64_t* out, int64_t cap, int32_t* n);
   silk_status get_cloth_velocity(uint32_t h, float* out, int64_t n);
+  silk_status set_cloth_state(uint32_t h, const float* x, int64_t nx, const float* v,
+                              int64_t nvel);
   silk_status set_warm_start_model(const float* params, int64_t n);
   silk_status get_warm_start_samples(uint32_t h, float* feat, float* target, int64_t nv,
                                      int* valid);

@@ -78,7 +78,8 @@ class _SolverOptionsC(C.Structure):
                 ("mas_bf16", C.c_int32), ("profile", C.c_int32), ("cg_form", C.c_int32),
                 ("learned_warm_start", C.c_int32), ("capture_samples", C.c_int32),
                 ("contact_gs_form", C.c_int32), ("admm_extrapolated_start", C.c_int32),
-                ("resident_halo_limit", C.c_int32)]
+                ("resident_halo_limit", C.c_int32), ("barrier_spin_limit", C.c_int32),
+                ("debug_withhold_block", C.c_int32)]
 
 
 class _ProfileC(C.Structure):
@@ -165,6 +166,8 @@ class SolverOptions:
     contact_gs_form: int = 0          # 0: single-block Gauss-Seidel where possible; 1: grid
     admm_extrapolated_start: bool = False  # offer 2 x_k - x_(k-1) as later CG starts
     resident_halo_limit: int = 0  # > 0: fewer halo slots per resident-CG block (0: 1024)
+    barrier_spin_limit: int = 0  # > 0: polls before a CG grid-barrier wait gives up
+    debug_withhold_block: int = 0  # k > 0: block k - 1 of a cooperative CG grid never arrives
 
     def to_c(self) -> _SolverOptionsC:
         o = _SolverOptionsC()
@@ -178,6 +181,8 @@ class SolverOptions:
         o.contact_gs_form = int(self.contact_gs_form)
         o.admm_extrapolated_start = int(self.admm_extrapolated_start)
         o.resident_halo_limit = int(self.resident_halo_limit)
+        o.barrier_spin_limit = int(self.barrier_spin_limit)
+        o.debug_withhold_block = int(self.debug_withhold_block)
         return o
 
 
@@ -246,6 +251,9 @@ def _load() -> C.CDLL:
         "silk_set_stream": ([_W, C.c_void_p], C.c_int),
         "silk_get_profile": ([_W, C.POINTER(_ProfileC), C.c_int32], C.c_int),
         "silk_get_cloth_velocity": ([_W, C.c_uint32, _F32P, C.c_int64], C.c_int),
+        "silk_set_cloth_state": ([_W, C.c_uint32, _F32P, C.c_int64, C.c_void_p, C.c_int64],
+                                 C.c_int),
+        "silk_debug_coulomb": ([_F32P, _F32P, _F32P, C.c_int64, _F32P], C.c_int),
         "silk_debug_cloth_partition": ([_W, C.c_uint32, _I32P, C.c_int64, _I32P, C.c_int64,
                                         C.POINTER(C.c_int32)], C.c_int),
         "silk_debug_cloth_matrix": ([_W, C.c_uint32, _F64P, C.c_int64], C.c_int),
@@ -425,6 +433,17 @@ class World:
         p = _ProfileC()
         lib.silk_get_profile(self._w, C.byref(p), int(reset))
         return {n: getattr(p, n) for n, _ in _ProfileC._fields_ if n != "reserved"}
+
+    def set_cloth_state(self, handle: int, position, velocity=None) -> Result:
+        """Restart a cloth from stored positions (and velocities; None = at
+        rest), mesh order."""
+        x = _f32(position)
+        if velocity is None:
+            return _result(lib.silk_set_cloth_state(self._w, handle, x, x.size, None, 0),
+                           self._w)
+        v = _f32(velocity)
+        return _result(lib.silk_set_cloth_state(self._w, handle, x, x.size, v.ctypes.data,
+                                                v.size), self._w)
 
     def get_cloth_velocity(self, handle: int, velocity: np.ndarray) -> Result:
         return _result(lib.silk_get_cloth_velocity(self._w, handle, velocity.reshape(-1),
@@ -658,6 +677,22 @@ def assemble_cloth_host(cloth: ClothConfig, verts, faces, dt: float):
     if st:
         raise RuntimeError(_result(st).to_string())
     return L.reshape(nv, nv), m, w, b
+
+
+def debug_coulomb(u, normal, friction) -> np.ndarray:
+    """The GPU contact Gauss-Seidel's Coulomb projection of n (u, normal,
+    friction) triples (n x 3 results)."""
+    u = _f32(u).reshape(-1)
+    nn = _f32(normal).reshape(-1)
+    mu = _f32(friction).reshape(-1)
+    n = mu.size
+    if u.size != 3 * n or nn.size != 3 * n:
+        raise ValueError("u and normal need 3 floats per friction coefficient")
+    out = np.zeros(3 * n, np.float32)
+    st = lib.silk_debug_coulomb(u, nn, mu, n, out)
+    if st:
+        raise RuntimeError(_result(st).to_string())
+    return out.reshape(n, 3)
 
 
 def color_contacts(verts4: np.ndarray, prio: np.ndarray) -> tuple[np.ndarray, int]:

@@ -77,3 +77,41 @@ CONFIGS = {
     "c3_sheet316_sphere": dict(side_count=316, side=2.0, z=1.0, jitter=1e-4, pins=False,
                                sphere=0.6, steps=200, max_inner=100),
 }
+
+
+def c2_scene(seed: int = 1236):
+    """6.4K-vertex sheet on a sphere: 80 x 80 grid (12,482 triangles), side
+    1 m, jitter N(0, 1e-4) m, at z = 1 above an icosphere of subdivision 4
+    and radius 0.3 m at the origin.  Returns (V, F, SV, SF)."""
+    V, F = grid_sheet(80, side=1.0, z=1.0, jitter=1e-4, seed=seed)
+    SV, SF = icosphere(4, radius=0.3)
+    return V, F, SV, SF
+
+
+def c3_scene(seed: int = 1237):
+    """100K-vertex drape: 316 x 316 grid (99,856 vertices, 198,450
+    triangles), side 2 m, jitter N(0, 1e-4) m, at z = 0.7, 0.1 m above an
+    icosphere of subdivision 4 and radius 0.6 m at the origin.  Returns
+    (V, F, SV, SF)."""
+    V, F = grid_sheet(316, side=2.0, z=0.7, jitter=1e-4, seed=seed)
+    SV, SF = icosphere(4, radius=0.6)
+    return V, F, SV, SF
+
+
+def free_fall_state(V, steps: int, dt: float = 1.0 / 60.0, g: float = -9.81,
+                    damping: float = 0.01):
+    """Positions and velocities of an unpinned, unstressed sheet after
+    `steps` steps of free fall from rest (each step damps the velocity by
+    1 - damping, adds g dt and moves by v dt, main_loop.cu:24-120).  Returns
+    float32 (x, v) in mesh order."""
+    vz = 0.0
+    dz = 0.0
+    for _ in range(steps):
+        vz = (1.0 - damping) * vz + g * dt
+        dz += vz * dt
+    x = np.asarray(V, np.float64).copy()
+    x[:, 2] += dz
+    v = np.zeros_like(x)
+    v[:, 2] = vz
+    return x.astype(np.float32), v.astype(np.float32)
+
