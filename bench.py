@@ -3,24 +3,28 @@
 
 Workload (N = 1): the 6.4K-vertex sheet of the benchmark's second
 configuration -- an 80 x 80 grid (12,482 triangles, side 1 m, jitter
-N(0, 1e-4) m from a fixed seed) dropped from z = 1 onto a static icosphere
-(subdivision 4, radius 0.3 m), self-collision and obstacle CCD on, float32,
-dt = 1/60, gravity -9.81.  A step is one solver_step.  The sheet first falls
-freely for `--prelude` untimed steps so that the timed steps run with active
-contacts (the regime the reference's "6K cloth with active collision" claim
-describes); then `--warmup` untimed and `--steps` timed steps follow.
+N(0, 1e-4) m from a fixed seed) on a static icosphere (subdivision 4, radius
+0.3 m), self-collision and obstacle CCD on, float32, dt = 1/60, gravity
+-9.81, CG relative tolerance fixed at 1e-5 -- in the contact regime: both arms
+start from the CPU oracle's own state after 27 steps (24 of free fall, 3 in
+contact; oracle/reference_state_c2_step27.npz, which also holds the MAS
+partition both arms use), so they time the same steps (28, 29, ...) from the
+same state.  A step is one solver_step.
 
-Metric: steps/s (higher is better).  `value` is device time (CUDA events on
-the world's stream) with inputs resident; `e2e` drives the public API with
-host buffers each step (obstacle position upload + solver_step + position
-readback).  Between timed steps a 256 MiB buffer is written to flush L2.
+Metric: steps/s (higher is better).  `value`: K steps timed with CUDA events
+on the world's stream, inputs resident, a 256 MiB write flushing L2 before
+each step (outside the events).  `e2e`: the same K steps again from the same
+state through the public API with host buffers (obstacle position from
+pinned memory + solver_step + cloth position into pinned memory, inside the
+timed region).  The W warm-up steps run from the stored state before the
+world is set back to it.
 
 Multi-GPU: scenes are independent, so --gpus N runs N replicas (one process
 per GPU, no collective on the data path; barrier + max over ranks only).
 
 `--impl reference` times the CPU restatement of the reference algorithm
-(oracle/, the reference itself cannot be built here) on all host cores on the
-same scene and steps.
+(oracle/; the reference itself cannot be built here) on all host cores from
+the same stored state, as many of the same steps as fit the CPU budget.
 """
 from __future__ import annotations
 
@@ -31,6 +35,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -39,83 +44,59 @@ sys.path.insert(0, str(ROOT))
 
 import numpy as np  # noqa: E402
 
-WORKLOAD = "c2_sheet80_on_icosphere_r0.3"
+WORKLOAD = "c2_sheet80_on_icosphere_r0.3_contact"
 METRIC = "steps/s (6.4K-vertex sheet on sphere, active contact)"
-
-
-def scene(seed=1236):
-    from silk_physics_b200 import scenes as S
-
-    V, F = S.grid_sheet(80, side=1.0, z=1.0, jitter=1e-4, seed=seed)
-    SV, SF = S.icosphere(4, radius=0.3)
-    return V, F, SV, SF
-
-
-C3_WORKLOAD = "c3_sheet316_on_icosphere_r0.6"
+C3_WORKLOAD = "c3_sheet316_on_icosphere_r0.6_first_contact"
+STATE = ROOT / "oracle" / "reference_state_c2_step27.npz"
 MODEL = ROOT / "silk_physics_b200" / "models" / "warm_start.npy"
+TRAFFIC = ROOT / "profiles" / "cg_resident_c2_contact.json"
+SCENES = ROOT / "tests" / "golden" / "reference_scenes.npz"
+C3_START_STEPS = 8  # free-fall steps before the drape's first contact step
 
 
-def scene_c3(seed=1237):
+def scene():
     from silk_physics_b200 import scenes as S
 
-    V, F = S.grid_sheet(316, side=2.0, z=0.7, jitter=1e-4, seed=seed)
-    SV, SF = S.icosphere(4, radius=0.6)
-    return V, F, SV, SF
+    return S.c2_scene()
 
 
-def timed_variant(N, torch, stream, flush, V, F, SV, SF, cg_rel_tol, bf16, learned,
-                  prelude, steps, extrap=False):
-    """Steps/s and CG statistics of one solver variant on one scene: `prelude`
-    untimed steps, then `steps` steps timed with CUDA events (L2 flushed
-    between steps)."""
-    opts = N.SolverOptions(fixed_linear_rel_tol=cg_rel_tol, profile=True, mas_bf16=bf16,
-                           learned_warm_start=learned, admm_extrapolated_start=extrap)
-    w, h, _ = make_world(stream.cuda_stream, opts, V, F, SV, SF)
-    if learned:
-        from silk_physics_b200 import learned as L
+def scene_c3():
+    from silk_physics_b200 import scenes as S
 
-        r = w.set_warm_start_model(L.load(str(MODEL)))
-        assert r, r.to_string()
-    for _ in range(prelude):
-        r = w.solver_step()
-        assert r, r.to_string()
-    w.profile(reset=True)
-    ms, admm, cg, solves, first, taken, outer, ext = 0.0, 0, 0, 0, 0, 0, 0, 0
-    for k in range(steps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
-            flush.fill_(k & 0xff)
-            a.record(stream)
-        r = w.solver_step()
-        b.record(stream)
-        b.synchronize()
-        assert r, r.to_string()
-        ms += a.elapsed_time(b)
-        st = w.step_stats()
-        admm += st.admm_iterations
-        cg += st.cg_iterations
-        solves += st.cg_solves
-        first += st.cg_first_solve_iterations
-        taken += st.learned_starts
-        ext += st.extrapolated_starts
-        outer += st.outer_iterations
-    prof = w.profile(reset=True)
-    return {"value": round(steps / (ms / 1e3), 4), "ms_per_step": round(ms / steps, 3),
-            "cg_kernel_ms_per_step": round(prof["cg_time_ms"] / steps, 2),
-            "other_admm_kernels_ms_per_step": round(prof["admm_other_ms"] / steps, 2),
-            "contact_gs_ms_per_step": round(prof["contact_gs_ms"] / steps, 2),
-            "ccd_host_ms_per_step": round(prof["ccd_host_ms"] / steps, 2),
-            "dcd_host_ms_per_step": round(prof["dcd_host_ms"] / steps, 2),
-            "admm_iterations_per_step": admm / steps,
-            "cg_iterations_per_solve": round(cg / max(solves, 1), 2),
-            "first_solve_cg_iterations_per_outer": round(first / max(outer, 1), 2),
-            "learned_starts_taken": taken, "extrapolated_starts_taken": ext,
-            "outer_iterations": outer}
+    return S.c3_scene()
+
+
+def stored_state():
+    """(x, v, steps, perm, part_offsets) of the stored C2 contact state."""
+    d = np.load(STATE)
+    return (d["x"].reshape(-1), d["v"].reshape(-1), int(d["steps"]), d["perm"],
+            d["part_offsets"])
+
+
+def c3_start(V):
+    """The drape's free-fall state right before its first contact step."""
+    from silk_physics_b200 import scenes as S
+
+    x, v = S.free_fall_state(V, C3_START_STEPS)
+    return x.reshape(-1), v.reshape(-1)
+
+
+def bench_config(args, V, F, SV, world_size: int) -> dict:
+    """The workload description, identical in both arms."""
+    return {"workload": WORKLOAD, "vertices": int(len(V)), "faces": int(len(F)),
+            "obstacle_vertices": int(len(SV)),
+            "start": "CPU oracle state after 27 steps (in contact), timed steps 28 on",
+            "cg_rel_tol": args.cg_rel_tol if args.cg_rel_tol > 0 else "adaptive (reference)",
+            "mas": "bf16" if args.bf16 else "fp32",
+            "mas_partition": "host partition stored with the state",
+            "l2": "flushed between timed steps (256 MiB write)",
+            "parallelism": f"replicas x{world_size}"}
 
 
 def dist_env():
     return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
             int(os.environ.get("WORLD_SIZE", 1)))
+
 
 
 # Replicas plumbing (one process per GPU, no data-path collective): a process
@@ -210,6 +191,8 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+
+
 def peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -219,20 +202,16 @@ def peaks() -> dict:
 
 
 def traffic_per_launch():
-    """DRAM bytes per CG launch from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / "cg_resident_c2.md"
-    if not p.exists():
+    """DRAM bytes per CG launch of a contact-regime solve, from the committed
+    ncu summary (profiles/cg_resident_c2_contact.json), or None."""
+    if not TRAFFIC.exists():
         return None
-    for line in p.read_text().splitlines():
-        if line.strip().startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1].strip())
-            except ValueError:
-                return None
-    return None
+    d = json.loads(TRAFFIC.read_text())
+    return {"bytes": d["dram_bytes_per_launch"], "source": TRAFFIC.name,
+            "captured": d.get("captured")}
 
 
-def make_world(stream_handle, opts, V, F, SV, SF):
+def make_world(stream_handle, opts, V, F, SV, SF, model=False):
     from silk_physics_b200 import native as N
 
     w = N.World()
@@ -247,36 +226,143 @@ def make_world(stream_handle, opts, V, F, SV, SF):
     assert r, r.to_string()
     r, hs = w.add_obstacle(N.CollisionConfig(), SV, SF)
     assert r, r.to_string()
+    if model:
+        from silk_physics_b200 import learned as L
+
+        r = w.set_warm_start_model(L.load(str(MODEL)))
+        assert r, r.to_string()
     return w, h, hs
 
 
-def cpu_oracle_sample(x0, v0, V, F, SV, SF, cg_rel_tol, budget_s=20.0):
-    """Time the CPU restatement from the same state on all host cores.
-
-    Contact steps of this algorithm take minutes on a CPU, so the sample is
-    the steps that fit in ~budget_s (at least one); the result is steps/s."""
+def oracle_steps(x0, v0, perm, offs, V, F, SV, SF, cg_rel_tol, max_steps, budget_s):
+    """The CPU restatement stepped from (x0, v0) on all host cores: per-step
+    wall seconds of up to max_steps steps, stopping once budget_s is spent
+    (at least one step), and their ADMM iterations."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import pyoracle
 
     ow = pyoracle.OracleWorld(config=dict(acceleration=(0.0, 0.0, -9.81),
                                           fixed_linear_rel_tol=cg_rel_tol))
-    nv = len(V)
-    perm = np.arange(nv, dtype=np.int32)
-    offs = np.unique(np.append(np.arange(0, nv, 32), nv)).astype(np.int32)
     h = ow.add_cloth(V, F, [], perm, offs)
     ow.add_obstacle(SV, SF)
     ow.set_state(h, x0, v0)
+    times, admm = [], 0
     t0 = time.perf_counter()
-    steps = 0
-    admm = 0
-    while True:
-        ow.step()
-        steps += 1
+    for _ in range(max_steps):
+        a = time.perf_counter()
+        assert ow.step() == 0
+        times.append(time.perf_counter() - a)
         admm += ow.stats()["admm_iterations"]
         if time.perf_counter() - t0 > budget_s:
             break
-    el = time.perf_counter() - t0
-    return steps / el, steps, el, admm
+    return times, admm
+
+
+def replay_variant(N, torch, stream, flush, V, F, SV, SF, x0, v0, cg_rel_tol, bf16, learned,
+                   extrap, reps):
+    """Controlled A/B: `reps` times the same step from the same state (the
+    world is set back to (x0, v0) before each), CUDA events around each
+    step, L2 flushed before it."""
+    opts = N.SolverOptions(fixed_linear_rel_tol=cg_rel_tol, profile=True, mas_bf16=bf16,
+                           learned_warm_start=learned, admm_extrapolated_start=extrap)
+    w, h, _ = make_world(stream.cuda_stream, opts, V, F, SV, SF, model=learned)
+    assert w.set_cloth_state(h, x0, v0)
+    assert w.solver_step()  # untimed: first-use setup of the world
+    w.profile(reset=True)
+    ms, keys = [], set()
+    for k in range(reps):
+        assert w.set_cloth_state(h, x0, v0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 0xff)
+            a.record(stream)
+        r = w.solver_step()
+        b.record(stream)
+        b.synchronize()
+        assert r, r.to_string()
+        ms.append(a.elapsed_time(b))
+        s = w.step_stats()
+        keys.add((s.admm_iterations, s.cg_iterations, s.contacts, s.outer_iterations))
+    s = w.step_stats()
+    prof = w.profile(reset=True)
+    med = statistics.median(ms)
+    return {"ms_per_step_median": round(med, 2), "ms_per_step": [round(t, 2) for t in ms],
+            "value": round(1e3 / med, 4),
+            "admm_iterations_per_step": s.admm_iterations,
+            "outer_iterations": s.outer_iterations,
+            "cg_iterations_per_step": s.cg_iterations,
+            "cg_iterations_per_solve": round(s.cg_iterations / max(s.cg_solves, 1), 2),
+            "first_solve_cg_iterations": s.cg_first_solve_iterations,
+            "ms_per_admm_iteration": round(med / max(s.admm_iterations, 1), 4),
+            "cg_kernel_ms_per_step": round(prof["cg_time_ms"] / reps, 2),
+            "contact_gs_ms_per_step": round(prof["contact_gs_ms"] / reps, 2),
+            "ccd_host_ms_per_step": round(prof["ccd_host_ms"] / reps, 2),
+            "contacts": s.contacts, "replays_identical": len(keys) == 1,
+            "learned_starts_taken": s.learned_starts,
+            "extrapolated_starts_taken": s.extrapolated_starts}
+
+
+def variants_ab(N, torch, stream, flush, args):
+    """Plain FP32 MAS, BF16 MAS and the learned warm start, each replaying
+    the same contact step from the same state: C2 from the stored oracle
+    state, C3 from the drape's free-fall state before its first contact."""
+    out = {}
+    forms = (("plain_fp32", False, False, False), ("bf16", True, False, False),
+             ("learned_bf16", True, True, False), ("extrapolated_fp32", False, False, True),
+             ("learned_extrapolated_bf16", True, True, True))
+    V, F, SV, SF = scene()
+    x0, v0, s0, _, _ = stored_state()
+    c2 = {"workload": WORKLOAD, "replayed_step": s0 + 1, "replays": args.variant_reps}
+    for name, bf16, learned, extrap in forms:
+        if learned and not MODEL.exists():
+            continue
+        c2[name] = replay_variant(N, torch, stream, flush, V, F, SV, SF, x0, v0,
+                                  args.cg_rel_tol, bf16, learned, extrap, args.variant_reps)
+    out["c2"] = c2
+    V3, F3, SV3, SF3 = scene_c3()
+    x3, v3 = c3_start(V3)
+    c3 = {"workload": C3_WORKLOAD, "vertices": int(len(V3)), "faces": int(len(F3)),
+          "replayed_step": C3_START_STEPS + 1, "replays": args.variant_reps}
+    for name, bf16, learned, extrap in forms:
+        if learned and not MODEL.exists():
+            continue
+        c3[name] = replay_variant(N, torch, stream, flush, V3, F3, SV3, SF3, x3, v3,
+                                  args.cg_rel_tol, bf16, learned, extrap, args.variant_reps)
+    for d in (c2, c3):
+        for name in ("bf16", "learned_bf16", "extrapolated_fp32", "learned_extrapolated_bf16"):
+            if name in d:
+                d[name + "_over_plain"] = round(
+                    d["plain_fp32"]["ms_per_step_median"] / d[name]["ms_per_step_median"], 3)
+    out["c3"] = c3
+    return out
+
+
+def reference_scenes(N, steps_cloth_ball: int):
+    """The reference's own example scenes (packaged in tests/golden/) through
+    the headless driver with the reference's default solver settings
+    (adaptive CG tolerance): dense_sheet.json (the README's 6K sheet, its 10
+    steps) and cloth_ball.json (the same sheet on a ground plane and a
+    sphere, first steps_cloth_ball steps).  Host wall time of solver_step."""
+    from silk_physics_b200 import headless as H
+
+    d = dict(np.load(SCENES))
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, steps in (("dense_sheet", None), ("cloth_ball", steps_cloth_ball)):
+            text = bytes(d[f"{name}/json"]).decode()
+            meshes = {o["mesh"]: (d[f"mesh/{o['mesh']}/verts"], d[f"mesh/{o['mesh']}/faces"])
+                      for o in json.loads(text)["objects"]}
+            path = H.write_scene(Path(tmp) / name, name, text, meshes)
+            g = json.loads(text)["global"]
+            _, wall = H.run(path, steps=steps, bench=True, log=None)
+            n = len(wall)
+            out[name] = {"steps": n, "dt": g["dt"], "value": round(n / (sum(wall) / 1e3), 3),
+                         "unit": "steps/s", "ms_per_step": round(sum(wall) / n, 2),
+                         "max_inner_iteration": g["max_inner_iteration"],
+                         "cg_tolerance": "adaptive (reference default)"}
+    out["note"] = ("README.md:7 of the reference: 'maintain 40 FPS' on a 6K cloth mesh with "
+                   "active collision, hardware, backend and settings unstated")
+    return out
 
 
 def run_ours(args) -> None:
@@ -288,26 +374,25 @@ def run_ours(args) -> None:
     from silk_physics_b200 import native as N
 
     V, F, SV, SF = scene()
+    x0, v0, s0, perm_s, offs_s = stored_state()
     stream = torch.cuda.Stream()
     opts = N.SolverOptions(fixed_linear_rel_tol=args.cg_rel_tol, profile=True,
                            mas_bf16=args.bf16)
     w, h, hs = make_world(stream.cuda_stream, opts, V, F, SV, SF)
+    perm, offs = w.cloth_partition(h, len(V))
+    assert np.array_equal(perm, perm_s) and np.array_equal(offs, offs_s), \
+        "the stored state's partition is not the one this build computes"
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    x = np.zeros(V.size, np.float32)
-    for _ in range(args.prelude):
-        r = w.solver_step()
-        assert r, r.to_string()
+    assert w.set_cloth_state(h, x0, v0)
     for _ in range(args.warmup):
         r = w.solver_step()
         assert r, r.to_string()
-    state_x = np.zeros(V.size, np.float32)
-    state_v = np.zeros(V.size, np.float32)
-    w.get_cloth_position(h, state_x)
-    w.get_cloth_velocity(h, state_v)
+    assert w.set_cloth_state(h, x0, v0)
     w.profile(reset=True)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
-    launches = admm = cg = solves = contacts = admm_first = ccd_first = 0
+    launches = admm = cg = solves = contacts = 0
+    per_step_admm = []
     if world_size > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -322,9 +407,7 @@ def run_ours(args) -> None:
             st = w.step_stats()
             launches += st.kernel_launches
             admm += st.admm_iterations
-            if k < args.e2e_steps:
-                admm_first += st.admm_iterations
-                ccd_first += st.ccd_queries
+            per_step_admm.append(st.admm_iterations)
             cg += st.cg_iterations
             solves += st.cg_solves
             contacts = st.contacts
@@ -335,67 +418,35 @@ def run_ours(args) -> None:
     total_ms = max_over_ranks(total_ms, "cuda")
     value = weak_value(1, world_size, args.steps, total_ms)
 
-    # Learned warm start + BF16 MAS on the same scene, and the 100K-vertex
-    # sheet (plain FP32 vs learned + BF16), each from its own fresh world.
-    variants = {}
-    # Single-GPU diagnostics: not repeated on every replica.
-    if args.variants and MODEL.exists() and world_size == 1:
-        for name, bf16, learned, extrap in (("c2_bf16", True, False, False),
-                                            ("c2_learned_bf16", True, True, False),
-                                            ("c2_extrapolated", False, False, True),
-                                            ("c2_learned_extrapolated_bf16", True, True, True)):
-            variants[name] = timed_variant(N, torch, stream, flush, V, F, SV, SF,
-                                           args.cg_rel_tol, bf16, learned,
-                                           args.prelude + args.warmup, args.variant_steps,
-                                           extrap)
-        V3, F3, SV3, SF3 = scene_c3()
-        c3 = {"workload": C3_WORKLOAD, "vertices": int(len(V3)), "faces": int(len(F3)),
-              "prelude_steps": args.c3_prelude, "steps": args.c3_steps}
-        for name, bf16, learned, extrap in (("plain_fp32", False, False, False),
-                                            ("bf16", True, False, False),
-                                            ("learned_bf16", True, True, False),
-                                            ("learned_extrapolated_bf16", True, True, True)):
-            c3[name] = timed_variant(N, torch, stream, flush, V3, F3, SV3, SF3, args.cg_rel_tol,
-                                     bf16, learned, args.c3_prelude, args.c3_steps, extrap)
-        for name in ("learned_bf16", "learned_extrapolated_bf16"):
-            c3[name + "_over_plain"] = round(c3[name]["value"] / c3["plain_fp32"]["value"], 3)
-        variants["c3"] = c3
-
-    # End to end through the public API with host buffers, on the same steps:
-    # a fresh world replays the prelude and warm-up (the step is
-    # deterministic), then the first e2e_steps timed steps run with the
-    # obstacle position uploaded from pinned host memory and the cloth
-    # position read back to it inside the timed region.
-    we, he, hse = make_world(stream.cuda_stream, opts, V, F, SV, SF)
-    for _ in range(args.prelude + args.warmup):
-        r = we.solver_step()
-        assert r, r.to_string()
+    # End to end through the public API with host buffers, the same K steps
+    # from the same state.
+    assert w.set_cloth_state(h, x0, v0)
     pin_obs = torch.from_numpy(SV.ravel().copy()).pin_memory().numpy()
     pin_out = torch.empty(V.size, dtype=torch.float32).pin_memory().numpy()
-    e2e_ms = []
-    e2e_admm = e2e_ccd = 0
-    we.profile(reset=True)
-    n_e2e = min(args.e2e_steps, args.steps)
-    for k in range(n_e2e):
+    e2e_ms, e2e_admm = [], []
+    w.profile(reset=True)
+    torch.cuda.synchronize()
+    for k in range(args.steps):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(stream):
             flush.fill_(k & 0xff)
         a.record(stream)
-        we.set_obstacle_position(hse, pin_obs)
-        r = we.solver_step()
-        we.get_cloth_position(he, pin_out)
+        w.set_obstacle_position(hs, pin_obs)
+        r = w.solver_step()
+        w.get_cloth_position(h, pin_out)
         b.record(stream)
         b.synchronize()
         assert r, r.to_string()
         e2e_ms.append(a.elapsed_time(b))
-        e2e_admm += we.step_stats().admm_iterations
-        e2e_ccd += we.step_stats().ccd_queries
-    e2e_prof = we.profile(reset=True)
-    # Every rank takes both reductions, in this order.
-    e2e_val = weak_value(1, world_size, n_e2e, max_over_ranks(sum(e2e_ms), "cuda"))
-    value_same_steps = weak_value(1, world_size, n_e2e,
-                                  max_over_ranks(sum(step_ms[:n_e2e]), "cuda"))
-    del we
+        e2e_admm.append(w.step_stats().admm_iterations)
+    e2e_prof = w.profile(reset=True)
+    e2e_val = weak_value(1, world_size, args.steps, max_over_ranks(sum(e2e_ms), "cuda"))
+
+    # Single-GPU diagnostics: not repeated on every replica.
+    variants, ref_scenes = {}, None
+    if args.variants and world_size == 1:
+        variants = variants_ab(N, torch, stream, flush, args)
+        ref_scenes = reference_scenes(N, args.scene_steps)
 
     if rank != 0:
         if world_size > 1:
@@ -405,55 +456,52 @@ def run_ours(args) -> None:
     cg_launch_ms = prof["cg_time_ms"] / max(prof["cg_launches"], 1)
     bytes_per_launch = prof["cg_algorithmic_bytes"] / max(prof["cg_launches"], 1)
     achieved = bytes_per_launch / (cg_launch_ms / 1e3) / 1e9 if cg_launch_ms > 0 else 0.0
+    tr = traffic_per_launch()
     roofline = {"bound": "hbm", "kernel": "cg_resident_cluster_kernel (persistent MAS-PCG)",
                 "achieved": round(achieved, 2), "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved / pk["hbm_gbs"], 5), "peak_source": pk["source"],
-                "traffic": traffic_per_launch(),
+                "traffic": tr["bytes"] if tr else None,
+                "traffic_source": (f"{tr['source']}: {tr['captured']}" if tr else None),
                 "algorithmic_bytes_per_launch": round(bytes_per_launch),
                 "avg_launch_ms": round(cg_launch_ms, 5),
+                "cg_iterations_per_launch": round(prof["cg_iterations"] /
+                                                  max(prof["cg_launches"], 1), 2),
                 "cg_share_of_step": round(prof["cg_time_ms"] / total_ms, 4) if total_ms else None}
     cpu = None
     if world_size == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        sps, n, el, cadmm = cpu_oracle_sample(state_x, state_v, V, F, SV, SF,
-                                               args.cg_rel_tol, args.cpu_budget)
-        cpu = {"value": round(sps, 6), "unit": "steps/s", "cores": threads, "kind": "port",
-               "sample": f"{n} step(s) of the same scene from the GPU state after "
-                         f"{args.prelude + args.warmup} steps, {el:.1f} s wall, "
-                         f"{cadmm} ADMM iterations, OpenMP on all host threads"}
+        times, cadmm = oracle_steps(x0, v0, perm_s, offs_s, V, F, SV, SF, args.cg_rel_tol,
+                                    args.steps, args.cpu_budget)
+        cpu = {"value": round(len(times) / sum(times), 6), "unit": "steps/s", "cores": threads,
+               "kind": "port",
+               "sample": f"the first {len(times)} of the same timed steps from the same stored "
+                         f"state ({sum(times):.1f} s wall, {cadmm} ADMM iterations; the GPU "
+                         f"ran {sum(per_step_admm[:len(times)])} on them), OpenMP on all host "
+                         f"threads"}
     clocks = clk.summary()
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": "steps/s", "n_gpus": world_size,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded grid sheet + icosphere)",
-        "config": {"workload": WORKLOAD, "vertices": int(len(V)), "faces": int(len(F)),
-                   "obstacle_vertices": int(len(SV)), "prelude_steps": args.prelude,
-                   "cg_rel_tol": args.cg_rel_tol if args.cg_rel_tol > 0 else "adaptive (reference)",
-                   "mas": "bf16" if args.bf16 else "fp32",
-                   "l2": "flushed between timed steps (256 MiB write)",
-                   "admm_iterations_per_step": admm / args.steps,
-                   "cg_iterations_per_solve": round(cg / max(solves, 1), 2),
-                   "contacts_last_step": contacts,
-                   "parallelism": f"replicas x{world_size}"},
+        "config": bench_config(args, V, F, SV, world_size),
+        "stats": {"admm_iterations_per_step": admm / args.steps,
+                  "admm_iterations_per_timed_step": per_step_admm,
+                  "cg_iterations_per_solve": round(cg / max(solves, 1), 2),
+                  "contacts_last_step": contacts},
         "roofline": roofline, "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_val, 4), "unit": "steps/s",
                 "h2d_bytes_per_step": int(SV.nbytes), "d2h_bytes_per_step": int(V.nbytes),
-                "steps": n_e2e, "device_value_same_steps": round(value_same_steps, 4),
-                "admm_iterations": e2e_admm, "device_admm_iterations_same_steps": admm_first,
-                # set_obstacle_position marks the obstacle as moving (as the
-                # reference does), so the e2e steps run the moving-obstacle
-                # collision path: its CCD queries beside the device run's.
-                "ccd_queries": e2e_ccd, "device_ccd_queries_same_steps": ccd_first,
+                "steps": args.steps, "admm_iterations_per_step": e2e_admm,
                 "ms_per_step": [round(t, 1) for t in e2e_ms],
-                "device_ms_per_step": [round(t, 1) for t in step_ms[:n_e2e]],
+                "device_ms_per_step": [round(t, 1) for t in step_ms],
                 "phases_ms_per_step": {
-                    "cg_kernel_events": round(e2e_prof["cg_time_ms"] / n_e2e, 2),
-                    "other_admm_kernels_events": round(e2e_prof["admm_other_ms"] / n_e2e, 2),
-                    "admm_host_wall": round(e2e_prof["admm_host_ms"] / n_e2e, 2),
-                    "ccd_host_wall": round(e2e_prof["ccd_host_ms"] / n_e2e, 2),
-                    "dcd_host_wall": round(e2e_prof["dcd_host_ms"] / n_e2e, 2),
-                    "step_host_wall": round(e2e_prof["step_host_ms"] / n_e2e, 2)}},
+                    "cg_kernel_events": round(e2e_prof["cg_time_ms"] / args.steps, 2),
+                    "other_admm_kernels_events": round(e2e_prof["admm_other_ms"] / args.steps, 2),
+                    "admm_host_wall": round(e2e_prof["admm_host_ms"] / args.steps, 2),
+                    "ccd_host_wall": round(e2e_prof["ccd_host_ms"] / args.steps, 2),
+                    "dcd_host_wall": round(e2e_prof["dcd_host_ms"] / args.steps, 2),
+                    "step_host_wall": round(e2e_prof["step_host_ms"] / args.steps, 2)}},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "phases_ms_per_step": {
@@ -465,6 +513,7 @@ def run_ours(args) -> None:
             "dcd_host_wall": round(prof["dcd_host_ms"] / args.steps, 2),
             "step_host_wall": round(prof["step_host_ms"] / args.steps, 2)},
         "variants": variants,
+        "reference_scenes": ref_scenes,
     }
     print(json.dumps(line), flush=True)
     if world_size > 1:
@@ -481,18 +530,23 @@ STREAMING_PHASES = ["prolongation", "barrier 1", "SpMV", "barrier 2", "fine MAS"
 
 
 def run_trace(args) -> None:
-    """Median per-phase time of one CG iteration (block 0, clock64 stamps)."""
+    """Median per-phase time of one CG iteration (block 0, clock64 stamps),
+    over the last CG solve of one contact step from the stored state (C2) or
+    of the drape's first contact step (C3)."""
     import torch
 
     from silk_physics_b200 import native as N
 
     c3 = args.trace_workload == "c3"
     V, F, SV, SF = scene_c3() if c3 else scene()
+    x0, v0 = c3_start(V) if c3 else stored_state()[:2]
     stream = torch.cuda.Stream()
     opts = N.SolverOptions(fixed_linear_rel_tol=args.cg_rel_tol, profile=1, mas_bf16=args.bf16)
     w, h, _ = make_world(stream.cuda_stream, opts, V, F, SV, SF)
-    for _ in range(args.prelude + args.warmup):
+    assert w.set_cloth_state(h, x0, v0)
+    for _ in range(args.warmup):
         assert w.solver_step()
+    assert w.set_cloth_state(h, x0, v0)
     opts.profile = 2
     assert w.set_solver_options(opts)
     assert w.solver_step()
@@ -502,11 +556,13 @@ def run_trace(args) -> None:
     med = np.median(t["phase_cycles"], axis=0)[:len(names)] / ghz / 1e3
     print(json.dumps({"cg_trace": {
         "workload": C3_WORKLOAD if c3 else WORKLOAD,
-        "steps_before": args.prelude + args.warmup,
         "form": "resident" if t["form"] == 1 else "streaming",
         "mas": "bf16" if args.bf16 else "fp32", "traced_iterations": t["iters"],
         "sm_ghz": round(ghz, 3), "phase_us": {n: round(float(m), 2) for n, m in zip(names, med)},
         "iteration_us": round(float(med.sum()), 2)}}), flush=True)
+
+
+
 
 
 C5_WORKLOAD = "c5_batched_sheets_on_spheres"
@@ -615,55 +671,25 @@ def run_reference(args) -> None:
         return
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import pyoracle
-
     V, F, SV, SF = scene()
-    ow = pyoracle.OracleWorld(config=dict(acceleration=(0.0, 0.0, -9.81),
-                                          fixed_linear_rel_tol=args.cg_rel_tol))
-    nv = len(V)
-    perm = np.arange(nv, dtype=np.int32)
-    offs = np.unique(np.append(np.arange(0, nv, 32), nv)).astype(np.int32)
-    h = ow.add_cloth(V, F, [], perm, offs)
-    ow.add_obstacle(SV, SF)
-    # The oracle's own state after the default 24 prelude + 3 warm-up steps
-    # (oracle/make_reference_state.py) spares replaying them on the host
-    # cores; further untimed steps run from there when more are asked for.
-    state = ROOT / "oracle" / "reference_state_c2_step27.npz"
-    start = args.prelude + args.warmup
-    done = 0
-    if args.cg_rel_tol == 1e-5 and start >= 27 and state.exists():
-        st = np.load(state)
-        ow.set_state(h, st["x"], st["v"])
-        done = int(st["steps"])
-    t_pre = time.perf_counter()
-    for _ in range(start - done):
-        ow.step()
-    pre = time.perf_counter() - t_pre
-    times = []
-    admm = 0
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        a = time.perf_counter()
-        ow.step()
-        times.append(time.perf_counter() - a)
-        admm += ow.stats()["admm_iterations"]
-        if time.perf_counter() - t0 > args.cpu_budget and len(times) >= 1:
-            break
+    x0, v0, s0, perm, offs = stored_state()
+    times, admm = oracle_steps(x0, v0, perm, offs, V, F, SV, SF, args.cg_rel_tol, args.steps,
+                               args.cpu_budget)
     value = len(times) / sum(times)
-    origin = (f"from the oracle's stored state after {done} steps, "
-              f"{start - done} more untimed" if done else f"after {start} untimed steps")
-    sample = (f"{len(times)} timed step(s) {origin} ({pre:.1f} s), {admm} ADMM iterations, "
-              f"OpenMP on {threads} threads")
+    sample = (f"steps {s0 + 1}-{s0 + len(times)} (the first {len(times)} of the {args.steps} "
+              f"timed steps of the GPU arm) from the same stored oracle state, "
+              f"{admm} ADMM iterations, OpenMP on {threads} threads; more steps than fit "
+              f"{args.cpu_budget:.0f} s of CPU time are not run")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "steps/s",
-        "n_gpus": world_size, "steps": len(times), "warmup": args.warmup,
+        "n_gpus": world_size, "steps": len(times), "warmup": 0,
         "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded grid sheet + icosphere)",
-        "config": {"workload": WORKLOAD, "vertices": int(nv), "prelude_steps": args.prelude,
-                   "implementation": "CPU restatement of the reference algorithm (oracle/); "
-                                     "the reference cannot be built offline"},
+        "config": bench_config(args, V, F, SV, world_size),
+        "implementation": "CPU restatement of the reference algorithm (oracle/); the reference "
+                          "cannot be built offline",
+        "ms_per_timed_step": [round(1e3 * t, 1) for t in times],
         "cpu_baseline": {"value": round(value, 6), "unit": "steps/s", "cores": threads,
                          "kind": "port", "sample": sample},
         "e2e": {"value": round(value, 6), "unit": "steps/s", "h2d_bytes_per_step": 0,
@@ -676,8 +702,6 @@ def main() -> None:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--prelude", type=int, default=24)
-    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cg-rel-tol", type=float, default=1e-5,
                     help="fixed CG relative tolerance (0 = the reference's adaptive rule)")
@@ -685,11 +709,11 @@ def main() -> None:
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", type=int, default=1,
-                    help="also time learned + BF16 MAS at 6.4K and plain vs learned + BF16 "
-                         "at 100K vertices (needs the trained model file)")
-    ap.add_argument("--variant-steps", type=int, default=5)
-    ap.add_argument("--c3-prelude", type=int, default=8)
-    ap.add_argument("--c3-steps", type=int, default=2)
+                    help="also the controlled A/B of the solver forms at 6.4K and 100K "
+                         "vertices and the reference's example scenes")
+    ap.add_argument("--variant-reps", type=int, default=5)
+    ap.add_argument("--scene-steps", type=int, default=60,
+                    help="steps of the cloth_ball reference scene")
     ap.add_argument("--trace-workload", choices=["c2", "c3"], default="c2")
     ap.add_argument("--batched", action="store_true",
                     help="time independent scenes stepped concurrently instead of the bench line")
@@ -698,8 +722,8 @@ def main() -> None:
     ap.add_argument("--c5-steps", type=int, default=2)
     ap.add_argument("--c5-sequential", type=int, default=1)
     ap.add_argument("--cg-trace", action="store_true",
-                    help="print the CG phase breakdown of one step (after prelude and warm-up) "
-                         "instead of the bench line")
+                    help="print the CG phase breakdown of one contact step instead of the "
+                         "bench line")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -269,6 +269,12 @@ silk_status silk_debug_candidates(silk_world* w, int32_t* out, int64_t cap,
  * sorted; count in *n. */
 silk_status silk_debug_dcd(silk_world* w, float t, float activation,
                            int32_t* keys, int64_t cap, int32_t* n);
+/* Active contact set of the last solver_step (the contacts DCD activated at
+ * the start of the step and after each rollback, deduplicated by the
+ * reference's canonical key, contact_constraints.cu:440-453): rows of
+ * (type, obj_a, obj_b, i0..i3) in canonical order; *n = total count (rows
+ * beyond cap are not written). */
+silk_status silk_debug_contacts(silk_world* w, int32_t* keys, int64_t cap, int32_t* n);
 /* Minimum time of impact over the current refit.  prune = 1 lets searches
  * stop once they cannot lower the minimum (the solver step's mode: same
  * minimum, n_hits then counts completed searches only). */

@@ -308,6 +308,11 @@ silk_status silk_debug_dcd(silk_world* w, float t, float activation,
   });
 }
 
+silk_status silk_debug_contacts(silk_world* w, int32_t* keys, int64_t cap, int32_t* n) {
+  if (!n || (cap > 0 && !keys)) return SILK_ERR_INVALID_CONFIG;
+  return guard_init(w, [&](World& W) { return W.debug_contacts(keys, cap, n); });
+}
+
 silk_status silk_debug_min_toi(silk_world* w, float time_start, float max_time,
                                float min_separation, int32_t prune, float* toi,
                                int32_t* n_queries, int32_t* n_hits) {

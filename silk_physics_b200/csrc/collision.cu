@@ -2229,6 +2229,21 @@ int CollisionSystem::debug_candidates(int* out, int64_t cap) {
   return n;
 }
 
+int CollisionSystem::debug_contacts(int* keys, int64_t cap) {
+  const CollisionImpl& I = *impl_;
+  int i = 0;
+  for (const Key& k : I.keys) {  // std::set: canonical key order
+    if (i < cap) {
+      keys[7 * i] = k.type;
+      keys[7 * i + 1] = (int)k.oa;
+      keys[7 * i + 2] = (int)k.ob;
+      for (int q = 0; q < 4; ++q) keys[7 * i + 3 + q] = k.idx[q];
+    }
+    ++i;
+  }
+  return i;
+}
+
 int CollisionSystem::debug_dcd(float t, float dact, int* keys, int64_t cap) {
   CollisionImpl& I = *impl_;
   cudaStream_t st = w_.stream;

@@ -46,6 +46,8 @@ class CollisionSystem {
   // Inspection.
   int debug_candidates(int* out, int64_t cap);
   int debug_dcd(float t, float dact, int* keys, int64_t cap);
+  // Active contact set of the last step (keys in canonical order).
+  int debug_contacts(int* keys, int64_t cap);
 
  private:
   World& w_;

@@ -1378,6 +1378,11 @@ silk_status World::debug_dcd(float t, float dact, int* keys, int64_t cap, int* n
   return SILK_OK;
 }
 
+silk_status World::debug_contacts(int* keys, int64_t cap, int* n) {
+  *n = coll_ ? coll_->debug_contacts(keys, cap) : 0;
+  return SILK_OK;
+}
+
 silk_status World::debug_min_toi(float ts, float mt, float ms, bool prune,
                                  float* toi, int* nq, int* nh) {
   *toi = coll_->min_toi(ts, mt, ms, nq, nh, prune);

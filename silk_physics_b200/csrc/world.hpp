@@ -192,6 +192,7 @@ class World {
   silk_status debug_refit(const float* disp, int64_t n);
   silk_status debug_candidates(int* out, int64_t cap, int* n);
   silk_status debug_dcd(float t, float dact, int* keys, int64_t cap, int* n);
+  silk_status debug_contacts(int* keys, int64_t cap, int* n);
   silk_status debug_min_toi(float ts, float mt, float ms, bool prune, float* toi,
                             int* nq, int* nh);
 

@@ -325,6 +325,33 @@ def load_scene(path: str | Path):
     return cfg.get("global", {}), objects
 
 
+def write_obj(path: Path, V: np.ndarray, F: np.ndarray) -> None:
+    """Triangle mesh as Wavefront OBJ; nine significant digits keep every
+    float32 coordinate exact through load_mesh."""
+    path.parent.mkdir(parents=True, exist_ok=True)
+    lines = [f"v {x:.9g} {y:.9g} {z:.9g}" for x, y, z in np.asarray(V, np.float32).tolist()]
+    lines += [f"f {a + 1} {b + 1} {c + 1}" for a, b, c in np.asarray(F, np.int64).tolist()]
+    path.write_text("\n".join(lines) + "\n")
+
+
+def write_scene(directory: str | Path, name: str, scene_text: str,
+                meshes: dict) -> Path:
+    """Write a scene file and its meshes (mesh path as named in the scene ->
+    (vertices, triangles)) under `directory`; returns the scene file's path.
+    Meshes are written as OBJ at the named path (whatever its extension), so
+    run() loads the same vertices and triangles."""
+    d = Path(directory)
+    cfg = json.loads(scene_text)
+    for o in cfg.get("objects", []):
+        V, F = meshes[o["mesh"]]
+        obj = Path(o["mesh"]).with_suffix(".obj")
+        write_obj(d / obj, V, F)
+        o["mesh"] = str(obj)
+    path = d / f"{name}.json"
+    path.write_text(json.dumps(cfg, indent=2))
+    return path
+
+
 def run(scene: str | Path, out: str | None = None, steps: int | None = None,
         bench: bool = False, options: N.SolverOptions | None = None, log=print):
     """Run a scene; returns (objects with their frames, per-step wall ms)."""

@@ -263,6 +263,7 @@ def _load() -> C.CDLL:
                             C.POINTER(C.c_int32)], C.c_int),
         "silk_debug_cg_trace": ([_W, C.c_uint32, C.c_void_p, C.c_int64, C.POINTER(C.c_int32)],
                                 C.c_int),
+        "silk_debug_contacts": ([_W, _I32P, C.c_int64, C.POINTER(C.c_int32)], C.c_int),
         "silk_debug_min_toi": ([_W, C.c_float, C.c_float, C.c_float, C.c_int32,
                                 C.POINTER(C.c_float), C.POINTER(C.c_int32),
                                 C.POINTER(C.c_int32)], C.c_int),
@@ -498,6 +499,16 @@ class World:
         out = np.zeros(7 * cap, np.int32)
         n = C.c_int32(0)
         st = lib.silk_debug_dcd(self._w, t, activation, out, cap, C.byref(n))
+        if st:
+            raise RuntimeError(_result(st, self._w).to_string())
+        return out[: 7 * min(n.value, cap)].reshape(-1, 7)
+
+    def debug_contacts(self, cap: int = 1 << 20) -> np.ndarray:
+        """Active contact keys of the last step, rows (type, obj_a, obj_b,
+        i0..i3) in canonical order."""
+        out = np.zeros(7 * cap, np.int32)
+        n = C.c_int32(0)
+        st = lib.silk_debug_contacts(self._w, out, cap, C.byref(n))
         if st:
             raise RuntimeError(_result(st, self._w).to_string())
         return out[: 7 * min(n.value, cap)].reshape(-1, 7)

@@ -201,3 +201,66 @@ def test_headless_run_equals_direct_api(tmp_path):
         np.testing.assert_array_equal(res["ball/positions"][k + 1], V)
     # Pinned vertices stayed put.
     np.testing.assert_array_equal(res["sheet/positions"][-1][sheet.pins], sheet.verts[sheet.pins])
+
+
+REFERENCE = __import__("pathlib").Path("/root/reference")
+EXAMPLES = REFERENCE / "misc" / "example_config"
+FIXTURE = __import__("pathlib").Path(__file__).resolve().parent / "golden" / "reference_scenes.npz"
+
+
+def reference_scene(name, directory):
+    """Write one packaged reference scene (tests/golden/reference_scenes.npz)
+    into `directory`; returns the scene file path."""
+    d = dict(np.load(FIXTURE))
+    text = bytes(d[f"{name}/json"]).decode()
+    meshes = {o["mesh"]: (d[f"mesh/{o['mesh']}/verts"], d[f"mesh/{o['mesh']}/faces"])
+              for o in json.loads(text)["objects"]}
+    return H.write_scene(directory, name, text, meshes)
+
+
+@pytest.mark.skipif(not EXAMPLES.exists(), reason="reference checkout absent")
+def test_every_reference_example_scene_loads(monkeypatch):
+    """All seven scene files of misc/example_config parse with the reference's
+    meshes (paths relative to the reference root, as its demo resolves them):
+    objects and configs read, transforms applied, pins selected where a pin
+    box is given, and every cloth mesh passes the host mesh checks and
+    partitions into MAS banks."""
+    monkeypatch.chdir(REFERENCE)
+    files = sorted(EXAMPLES.glob("*.json"))
+    assert [p.stem for p in files] == ["bunny_and_cloth", "cloth_ball", "cloth_on_the_ground",
+                                       "default", "default_gpu", "dense_sheet", "simple_sheet"]
+    for p in files:
+        g, objs = H.load_scene(p)
+        cfg = json.loads(p.read_text())
+        gc = H.global_config(g)
+        assert gc.dt == pytest.approx(cfg["global"]["dt"])
+        assert gc.max_inner_iteration == cfg["global"]["max_inner_iteration"]
+        assert len(objs) == len(cfg["objects"])
+        for o, spec in zip(objs, cfg["objects"]):
+            assert o.kind == spec["type"] and len(o.verts) > 0 and len(o.faces) > 0
+            assert np.isfinite(o.verts).all()
+            if (spec.get("pin_selection") or {}).get("bbox"):
+                assert len(o.pins) > 0, (p.name, o.name)
+            if o.kind == "cloth":
+                perm, offs = N.partition_mesh(o.verts, o.faces)
+                assert sorted(perm.tolist()) == list(range(len(o.verts)))
+                assert offs[-1] == len(o.verts)
+
+
+def test_packaged_reference_scenes(tmp_path, monkeypatch):
+    """The packaged dense_sheet and cloth_ball scenes rebuild the reference's
+    objects exactly (compared with the original files where the checkout is
+    present)."""
+    for name, nobj in (("dense_sheet", 1), ("cloth_ball", 3)):
+        g, objs = H.load_scene(reference_scene(name, tmp_path / name))
+        assert len(objs) == nobj and objs[0].kind == "cloth" and len(objs[0].verts) == 6273
+        if name == "dense_sheet":
+            assert len(objs[0].pins) == 162
+        if EXAMPLES.exists():
+            monkeypatch.chdir(REFERENCE)
+            g2, ref = H.load_scene(EXAMPLES / f"{name}.json")
+            assert g == g2
+            for a, b in zip(objs, ref):
+                np.testing.assert_array_equal(a.verts, b.verts)
+                np.testing.assert_array_equal(a.faces, b.faces)
+                np.testing.assert_array_equal(a.pins, b.pins)
