@@ -527,6 +527,12 @@ RESIDENT_PHASES = ["A: p update", "barrier 1", "B: SpMV rows", "B: p.Ap block su
                    "A: upper bank solves", "A: rz sum"]
 STREAMING_PHASES = ["prolongation", "barrier 1", "SpMV", "barrier 2", "fine MAS", "barrier 3",
                     "coarse levels", "barrier 4"]
+CLUSTER_PHASES = ["A: p update (own and halo)", "CTA barrier", "B: SpMV rows",
+                  "B: p.Ap block sum + push", "cluster barrier 1", "C: pAp total",
+                  "C: x/r update + fine MAS", "C: first-level push + r.z/r.r sum + push",
+                  "cluster barrier 2", "A: halo z load + totals", "A: restriction chain",
+                  "A: coarse bank solves", "A: coarse r.z sum", "A: stopping test"]
+FORM_NAMES = {0: "streaming", 1: "resident", 2: "cluster (redundant coarse levels)"}
 
 
 def run_trace(args) -> None:
@@ -552,11 +558,11 @@ def run_trace(args) -> None:
     assert w.solver_step()
     t = w.debug_cg_trace(h)
     ghz = t["cycles"] / max(t["ns"], 1)
-    names = RESIDENT_PHASES if t["form"] == 1 else STREAMING_PHASES
+    names = {0: STREAMING_PHASES, 1: RESIDENT_PHASES, 2: CLUSTER_PHASES}[t["form"]]
     med = np.median(t["phase_cycles"], axis=0)[:len(names)] / ghz / 1e3
     print(json.dumps({"cg_trace": {
         "workload": C3_WORKLOAD if c3 else WORKLOAD,
-        "form": "resident" if t["form"] == 1 else "streaming",
+        "form": FORM_NAMES[t["form"]],
         "mas": "bf16" if args.bf16 else "fp32", "traced_iterations": t["iters"],
         "sm_ghz": round(ghz, 3), "phase_us": {n: round(float(m), 2) for n, m in zip(names, med)},
         "iteration_us": round(float(med.sum()), 2)}}), flush=True)

@@ -87,8 +87,13 @@ typedef struct {
   int32_t mas_bf16;           /* 0: FP32 bank inverses; 1: BF16 storage */
   int32_t profile;            /* 1: time the CG kernel with CUDA events;
                                  2: also record the CG phase trace */
-  int32_t cg_form;            /* 0: resident CG kernel where the system fits
-                                 it, else streaming; 1: streaming always */
+  int32_t cg_form;            /* 0: the cluster form with redundant coarse
+                                 levels where the system fits one cluster of
+                                 CTAs of 8 or 16 fine banks, else the resident
+                                 form where it fits, else streaming;
+                                 2: resident where it fits, else streaming;
+                                 1: streaming always (applies when the solver
+                                 layout is built; changing it rebuilds it) */
   int32_t learned_warm_start; /* 1: offer the loaded model's prediction as the
                                  start of each outer iteration's first CG solve */
   int32_t capture_samples;    /* 1: record warm-start training samples */
@@ -150,7 +155,11 @@ typedef struct {
                                         first CG solve, summed */
   int32_t learned_starts;      /* first solves that started from the model */
   int32_t extrapolated_starts; /* solves that started from the extrapolation */
-  int32_t reserved[2];
+  int32_t cg_cluster_solves;   /* of the resident solves, those in the cluster form
+                                  with redundant coarse levels (CTAs of 8 or 16
+                                  fine banks exchanging through distributed
+                                  shared memory) */
+  int32_t reserved[1];
 } silk_step_stats;
 
 /* --- World lifetime (silk.hpp:92-100) ---------------------------------- */

@@ -1236,6 +1236,511 @@ int max_cluster_size() {
   return size;
 }
 
+
+// ---------------------------------------------------------------------------
+// Cluster CG with redundant coarse levels, for systems whose fine banks fit
+// one thread-block cluster of at most 16 CTAs of F fine banks each (F = 8 or
+// 16; the 6.4K-vertex sheet: 213 fine banks on 14 CTAs of 16).  CTA q owns
+// fine banks qF .. qF+F-1, one thread per bank slot; every vector entry of
+// its vertices stays in registers for the whole solve.  Compared with the
+// resident form (one CTA per first-level coarse bank of 32 fine banks) the
+// same system spreads over twice the SMs, and the CTAs of the cluster
+// exchange through distributed shared memory instead of L2:
+//  * every per-CTA partial sum (p.Ap, r.z, r.r) is stored by its CTA into
+//    the shared memory of every CTA of the cluster before the cluster
+//    barrier, and each CTA sums the copies in its own shared memory in CTA
+//    order after it (identical totals everywhere, no global round trip);
+//  * the residual restricted to the first coarse level (one node per fine
+//    bank) is pushed the same way, so every CTA holds the whole first-level
+//    input and computes every coarse level (restriction chain and bank
+//    solves of all levels, at most kDsmCoarseBanks banks) redundantly, in
+//    the same order, with identical results;
+//  * p at a halo vertex is computed by the CTA itself from the owner's
+//    fine-level z (published through global memory before the barrier) and
+//    the coarse z every CTA holds, with the owner's operations.
+// Per iteration: p update | CTA barrier | SpMV + p.Ap | cluster barrier |
+// alpha, x/r update, fine MAS, pushes | cluster barrier | totals and coarse
+// levels.  Arithmetic per vector entry as in cg_resident_kernel except the
+// order of the FP64 sums and of the coarse bank solves.
+// ---------------------------------------------------------------------------
+constexpr int kDsmCoarseBanks = kDsmCoarseBankLimit;  // held by every CTA
+constexpr int kDsmMaxCtas = 16;
+constexpr int kDsmPartSlots = 8;     // 0 r.z, 1 r.r, 2 p.Ap, 3..5 alternative start
+
+template <int W>
+struct DsmShared {
+  float Mf[W][kPacked];                   // the CTA's fine bank inverses
+  float Mc[kDsmCoarseBanks][kPacked];     // every coarse bank of every level
+  float4 pl[2 * 32 * W];                  // own slots, then the halo (at most 32 W)
+  int4 hcm[32 * W];                       // coarse nodes of the halo vertices
+  float4 rc[kDsmCoarseBanks * BANK];      // coarse-level inputs (first level pushed)
+  float4 zc[kDsmCoarseBanks * BANK];      // coarse-level outputs
+  __nv_bfloat16 rb[W][8][BANK];           // BF16 apply: residual as B operand
+  float4 zs[W][BANK];                     // BF16 apply / split bank rows
+  double red[W][3];
+  double tot[3];
+  double part[kDsmMaxCtas][kDsmPartSlots];  // partials of every CTA (pushed)
+};
+
+// Off-diagonal row sum plus the diagonal term, every column in shared memory.
+__device__ __forceinline__ float3 dsm_row(const int2* e, int rw, const float4* pl, float d,
+                                          float3 pv) {
+  float yx = d * pv.x, yy = d * pv.y, yz = d * pv.z;
+#pragma unroll 4
+  for (int j = 0; j < rw; ++j) {
+    int2 q = e[j * BANK];
+    float val = __int_as_float(q.y);
+    float4 pj = pl[-1 - q.x];
+    yx += val * pj.x;
+    yy += val * pj.y;
+    yz += val * pj.z;
+  }
+  return make_float3(yx, yy, yz);
+}
+
+template <int F>
+__global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
+  constexpr int W = F, T = 32 * F;
+  extern __shared__ __align__(16) unsigned char dsm_smem[];
+  DsmShared<W>& s = *reinterpret_cast<DsmShared<W>*>(dsm_smem);
+  cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int q = blockIdx.x, nctas = gridDim.x;
+  const int fb = q * F + warp;
+  const bool bank_ok = fb < a.nbank0;
+  const int levels = a.levels;
+  const bool tc = a.bf16 != 0;
+  CgTrace tr(a.trace, 2);
+  int iter = -1;
+
+  // Bank offsets of the coarse levels in Mc / rc / zc.
+  int cbo[MAX_COARSE + 1];
+  cbo[0] = 0;
+#pragma unroll
+  for (int l = 0; l < MAX_COARSE; ++l) cbo[l + 1] = cbo[l] + (l < levels ? a.coarse[l].nbank : 0);
+  const int ncb = cbo[levels];
+  auto level_of = [&](int g) {
+    int l = 0;
+    while (l + 1 < levels && g >= cbo[l + 1]) ++l;
+    return l;
+  };
+  auto stage = [&](const MasLevelDev& lv, int bank, float* slot) {
+    if (tc)
+      stage_bank_frag(lv, bank, slot, lane);
+    else
+      stage_bank(lv, 0, bank, slot, lane);
+  };
+  // Store this CTA's N partial sums (s.tot after a block sum) into slots
+  // slot0.. of every CTA's s.part row q.
+  auto push_partials = [&](int slot0, int N) {
+    if (warp == 0 && lane < nctas) {
+      double* dst = cl.map_shared_rank(&s.part[q][slot0], lane);
+      for (int k = 0; k < N; ++k) dst[k] = s.tot[k];
+    }
+  };
+  auto total = [&](int slot) {
+    double t = 0.0;
+    for (int j = 0; j < nctas; ++j) t += s.part[j][slot];
+    return t;
+  };
+  // Block sum of N doubles per thread into s.tot (fixed order).
+  auto block_sum = [&](const double* v, int N) {
+    for (int k = 0; k < N; ++k) {
+      double x = warp_sum_d(v[k]);
+      if (lane == 0) s.red[warp][k] = x;
+    }
+    __syncthreads();
+    if (warp == 0)
+      for (int k = 0; k < N; ++k) {
+        double x = warp_sum_d(lane < W ? s.red[lane][k] : 0.0);
+        if (lane == 0) s.tot[k] = x;
+      }
+    __syncthreads();
+  };
+
+  // ---- one-time staging ----------------------------------------------------
+  for (int i = lane; i < 5 * BANK; i += 32) s.rb[warp][3 + i / BANK][i % BANK] = __float2bfloat16_rn(0.f);
+  int vbase = 0, vsize = 0, rptr = 0, rw = 0;
+  if (bank_ok) {
+    vbase = a.part_off[fb];
+    vsize = a.part_off[fb + 1] - vbase;
+    rptr = a.rb_ptr[fb];
+    rw = a.rb_w[fb];
+    stage(a.fine, fb, s.Mf[warp]);
+  }
+  for (int g = warp; g < ncb; g += W) {
+    const int l = level_of(g);
+    stage(a.coarse[l], g - cbo[l], s.Mc[g]);
+  }
+  for (int i = tid; i < kDsmCoarseBanks * BANK; i += T) {
+    s.rc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    s.zc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  const bool own = lane < vsize;
+  const int v = vbase + lane;
+  const int2* erow = a.rent + rptr + lane;
+  float d = 0.f;
+  float3 x = make_float3(0.f, 0.f, 0.f), b = x;
+  int cm[MAX_COARSE] = {0, 0, 0, 0};
+  if (own) {
+    d = a.Ldiag[v] + a.dyn[v];
+    float4 x4 = a.x[v], b4 = a.b[v];
+    x = make_float3(x4.x, x4.y, x4.z);
+    b = make_float3(b4.x, b4.y, b4.z);
+    int4 c = a.cmap[v];
+    cm[0] = c.x;
+    cm[1] = c.y;
+    cm[2] = c.z;
+    cm[3] = c.w;
+  }
+  int hcol = -1;
+  {
+    const int h0 = a.halo_off[q], nh = a.halo_off[q + 1] - h0;
+    if (tid < nh) {
+      hcol = a.halo_col[h0 + tid];
+      s.hcm[tid] = a.cmap[hcol];
+    }
+  }
+  auto gather_halo = [&](const float4* ex) {
+    if (hcol >= 0) s.pl[T + tid] = ldcg4(ex + hcol);
+    __syncthreads();
+  };
+  // z of a vertex: fine-level z plus the coarse z of its node at every level,
+  // in level order (the same operations for an own and a halo vertex).
+  auto full_z = [&](float3 z, int c0, int c1, int c2, int c3) {
+    const int c[MAX_COARSE] = {c0, c1, c2, c3};
+#pragma unroll
+    for (int l = 0; l < MAX_COARSE; ++l) {
+      if (l >= levels) break;
+      float4 qz = s.zc[cbo[l] * BANK + c[l]];
+      z.x += qz.x;
+      z.y += qz.y;
+      z.z += qz.z;
+    }
+    return z;
+  };
+
+  // Publish x for r = b - A x; the cluster barrier also guarantees that every
+  // CTA has finished staging before any CTA stores into its shared memory.
+  s.pl[tid] = make_float4(x.x, x.y, x.z, 0.f);
+  if (own) a.p[v] = make_float4(x.x, x.y, x.z, 0.f);
+  cl.sync();
+  gather_halo(a.p);
+  float3 r;
+  {
+    float3 y = dsm_row(erow, rw, s.pl, d, x);
+    r = own ? make_float3(b.x - y.x, b.y - y.y, b.z - y.z) : make_float3(0.f, 0.f, 0.f);
+  }
+  double rr_judge = -1.0;
+  if (a.x_alt) {
+    float3 xa = make_float3(0.f, 0.f, 0.f);
+    if (own) {
+      float4 qa = a.x_alt[v];
+      xa = make_float3(qa.x, qa.y, qa.z);
+    }
+    __syncthreads();
+    s.pl[tid] = make_float4(xa.x, xa.y, xa.z, 0.f);
+    if (own) a.Ap[v] = make_float4(xa.x, xa.y, xa.z, 0.f);
+    cl.sync();
+    gather_halo(a.Ap);
+    float3 ra;
+    {
+      float3 y = dsm_row(erow, rw, s.pl, d, xa);
+      ra = own ? make_float3(b.x - y.x, b.y - y.y, b.z - y.z) : make_float3(0.f, 0.f, 0.f);
+    }
+    const double v3[3] = {(double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z,
+                          (double)r.x * ra.x + (double)r.y * ra.y + (double)r.z * ra.z,
+                          (double)ra.x * ra.x + (double)ra.y * ra.y + (double)ra.z * ra.z};
+    block_sum(v3, 3);
+    push_partials(3, 3);
+    cl.sync();
+    const double rr_plain = total(3), r_pa = total(4), rr_alt = total(5);
+    rr_judge = rr_plain;
+    const float w = (float)blend_weight(rr_plain, r_pa, rr_alt);
+    if (w > 0.0f) {
+      x = make_float3(x.x + w * (xa.x - x.x), x.y + w * (xa.y - x.y), x.z + w * (xa.z - x.z));
+      r = make_float3(r.x + w * (ra.x - r.x), r.y + w * (ra.y - r.y), r.z + w * (ra.z - r.z));
+      if (q == 0 && tid == 0 && a.stats) atomicAdd(a.stats + a.alt_stat, 1);
+    }
+  }
+
+  // Phase C body: fine MAS of r, pushes of the first-level input and of the
+  // r.z / r.r partials, fine z published for the halos.
+  float3 z0 = make_float3(0.f, 0.f, 0.f), p = z0, Ap = z0;
+  float4 hz = make_float4(0.f, 0.f, 0.f, 0.f);
+  auto mas_fine = [&]() {
+    const double rr = own ? (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z : 0.0;
+    __syncwarp();
+    if (!bank_ok) {
+      z0 = make_float3(0.f, 0.f, 0.f);
+    } else if (tc) {
+      z0 = bank_apply_mma(s.Mf[warp], r, lane, s.rb[warp], s.zs[warp]);
+    } else {
+      // The warp's residuals go through its own slots of pl, which nothing
+      // reads between the SpMV and the next p update.
+      s.pl[tid] = make_float4(r.x, r.y, r.z, 0.f);
+      __syncwarp();
+      z0 = bank_apply_smem(s.Mf[warp], s.pl + warp * BANK, lane);
+    }
+    if (!own) z0 = make_float3(0.f, 0.f, 0.f);
+    const double rz = own ? (double)r.x * z0.x + (double)r.y * z0.y + (double)r.z * z0.z : 0.0;
+    tr.stamp(iter, 6);
+    if (levels > 0) {
+      const float sx = warp_sum(r.x), sy = warp_sum(r.y), sz = warp_sum(r.z);
+      if (bank_ok && lane < nctas) {
+        float4* dst = cl.map_shared_rank(&s.rc[fb], lane);
+        *dst = make_float4(sx, sy, sz, 0.f);
+      }
+    }
+    if (own) a.z0[v] = make_float4(z0.x, z0.y, z0.z, 0.f);
+    const double v2[2] = {rz, rr};
+    block_sum(v2, 2);
+    push_partials(0, 2);
+    tr.stamp(iter, 7);
+  };
+  // Phase A head: totals and every coarse level.
+  auto totals = [&](double& rz, double& rr) {
+    rz = total(0);
+    rr = total(1);
+    if (levels == 0) return;
+    tr.stamp(iter, 9);
+    // Restriction chain (warp sums per connected component of a bank).
+    for (int l = 0; l + 1 < levels; ++l) {
+      const MasLevelDev& lv = a.coarse[l];
+      for (int g = warp; g < lv.nbank; g += W) {
+        const bool valid = g * BANK + lane < lv.nnode;
+        float4 qv = s.rc[(cbo[l] + g) * BANK + lane];
+        float3 rl = valid ? make_float3(qv.x, qv.y, qv.z) : make_float3(0.f, 0.f, 0.f);
+        const int ncc = lv.ncco[g], base = lv.cco_base[g];
+        const int mine = lv.slot_cco[(size_t)g * BANK + lane];
+        for (int c = 0; c < ncc; ++c) {
+          float qx = warp_sum(mine == c ? rl.x : 0.f);
+          float qy = warp_sum(mine == c ? rl.y : 0.f);
+          float qz = warp_sum(mine == c ? rl.z : 0.f);
+          if (lane == 0) s.rc[cbo[l + 1] * BANK + base + c] = make_float4(qx, qy, qz, 0.f);
+        }
+      }
+      __syncthreads();
+    }
+    tr.stamp(iter, 10);
+    // Every coarse bank: BF16 one warp per bank on the tensor cores; FP32 the
+    // columns of a bank split over `split` warps, partial rows added by the
+    // bank's first warp in warp order.
+    double rzc = 0.0;
+    const int split = tc ? 1 : (ncb * 4 <= W ? 4 : (ncb * 2 <= W ? 2 : 1));
+    const int per_round = W / split;
+    for (int g0 = 0; g0 < ncb; g0 += per_round) {
+      const int g = g0 + warp / split, part = warp - (warp / split) * split;
+      const bool gok = g < ncb;
+      int l = 0, gl = 0;
+      bool gvalid = false;
+      if (gok) {
+        l = level_of(g);
+        gl = g - cbo[l];
+        gvalid = gl * BANK + lane < a.coarse[l].nnode;
+      }
+      const int slot = g * BANK + lane;
+      if (tc) {
+        if (gok) {
+          float4 qv = s.rc[slot];
+          float3 rl = gvalid ? make_float3(qv.x, qv.y, qv.z) : make_float3(0.f, 0.f, 0.f);
+          float3 zq = bank_apply_mma(s.Mc[g], rl, lane, s.rb[warp], s.zs[warp]);
+          if (!gvalid) zq = make_float3(0.f, 0.f, 0.f);
+          s.zc[slot] = make_float4(zq.x, zq.y, zq.z, 0.f);
+          rzc += (double)rl.x * zq.x + (double)rl.y * zq.y + (double)rl.z * zq.z;
+        }
+      } else {
+        if (gok) {
+          const int cols = BANK / split, k0 = part * cols;
+          const float* sm = s.Mc[g];
+          const float4* rs = s.rc + g * BANK;
+          float zx = 0.f, zy = 0.f, zz = 0.f;
+#pragma unroll 8
+          for (int kk = k0; kk < k0 + cols; ++kk) {
+            float m = sm[upper_index(BANK, lane, kk)];
+            float4 rk = rs[kk];
+            zx += m * rk.x;
+            zy += m * rk.y;
+            zz += m * rk.z;
+          }
+          s.zs[warp][lane] = make_float4(zx, zy, zz, 0.f);
+        }
+        __syncthreads();
+        if (gok && part == 0) {
+          float4 acc = s.zs[warp][lane];
+          for (int k = 1; k < split; ++k) {
+            float4 t = s.zs[warp + k][lane];
+            acc.x += t.x;
+            acc.y += t.y;
+            acc.z += t.z;
+          }
+          float4 qv = s.rc[slot];
+          float3 rl = gvalid ? make_float3(qv.x, qv.y, qv.z) : make_float3(0.f, 0.f, 0.f);
+          float3 zq = gvalid ? make_float3(acc.x, acc.y, acc.z) : make_float3(0.f, 0.f, 0.f);
+          s.zc[slot] = make_float4(zq.x, zq.y, zq.z, 0.f);
+          rzc += (double)rl.x * zq.x + (double)rl.y * zq.y + (double)rl.z * zq.z;
+        }
+        __syncthreads();
+      }
+    }
+    tr.stamp(iter, 11);
+    const double v1[1] = {rzc};
+    block_sum(v1, 1);
+    rz += s.tot[0];
+    tr.stamp(iter, 12);
+  };
+
+  __syncthreads();  // every warp has read pl in the residual rows
+  mas_fine();
+  cl.sync();
+  if (hcol >= 0) hz = ldcg4(a.z0 + hcol);
+  double rz, rr;
+  totals(rz, rr);
+  iter = 0;
+  if (!isfinite(rz)) {
+    if (q == 0 && tid == 0) {
+      a.result[0] = 0;
+      a.result[1] = kCgInvalidInitialResidual;
+      *a.result_rr = (float)rr;
+    }
+    return;  // every CTA takes the same decision; no store is in flight
+  }
+  const double rr0 = rr_judge >= 0.0 ? rr_judge : rr;
+  const double abs2 = (double)a.abs_tol * a.abs_tol;
+  const double rel2 = (double)a.rel_tol * a.rel_tol;
+  double beta = 0.0;
+  int status = kCgMaxIter;
+  while (true) {
+    {
+      const float bt = (float)beta;
+      float3 zt = full_z(z0, cm[0], cm[1], cm[2], cm[3]);
+      p = bt == 0.0f ? zt : make_float3(zt.x + bt * p.x, zt.y + bt * p.y, zt.z + bt * p.z);
+      if (!own) p = make_float3(0.f, 0.f, 0.f);
+      s.pl[tid] = make_float4(p.x, p.y, p.z, 0.f);
+      if (hcol >= 0) {
+        const int4 c4 = s.hcm[tid];
+        float3 zh = full_z(make_float3(hz.x, hz.y, hz.z), c4.x, c4.y, c4.z, c4.w);
+        float4 po = s.pl[T + tid];
+        float3 ph = bt == 0.0f ? zh
+                               : make_float3(zh.x + bt * po.x, zh.y + bt * po.y, zh.z + bt * po.z);
+        s.pl[T + tid] = make_float4(ph.x, ph.y, ph.z, 0.f);
+      }
+    }
+    tr.stamp(iter, 0);
+    __syncthreads();
+    tr.stamp(iter, 1);
+    {
+      Ap = dsm_row(erow, rw, s.pl, d, p);
+      if (!own) Ap = make_float3(0.f, 0.f, 0.f);
+      tr.stamp(iter, 2);
+      const double v1[1] = {own ? (double)p.x * Ap.x + (double)p.y * Ap.y + (double)p.z * Ap.z
+                                : 0.0};
+      block_sum(v1, 1);
+      push_partials(2, 1);
+    }
+    tr.stamp(iter, 3);
+    cl.sync();
+    tr.stamp(iter, 4);
+    {
+      const double pAp = total(2);
+      tr.stamp(iter, 5);
+      const float alpha = (float)(fabs(pAp) < 1e-20 ? 0.0 : rz / pAp);
+      x = make_float3(alpha * p.x + x.x, alpha * p.y + x.y, alpha * p.z + x.z);
+      r = make_float3(-alpha * Ap.x + r.x, -alpha * Ap.y + r.y, -alpha * Ap.z + r.z);
+      if (!own) r = make_float3(0.f, 0.f, 0.f);
+      mas_fine();
+    }
+    cl.sync();
+    tr.stamp(iter, 8);
+    if (hcol >= 0) hz = ldcg4(a.z0 + hcol);
+    const double rz_old = rz;
+    totals(rz, rr);
+    tr.stamp(iter, 13);
+    ++iter;
+    bool stop = false;
+    if (iter >= a.max_iter) {
+      status = kCgMaxIter;
+      stop = true;
+    } else if (rr <= abs2) {
+      status = kCgAbsTol;
+      stop = true;
+    } else if (rr <= rel2 * rr0) {
+      status = kCgRelTol;
+      stop = true;
+    }
+    beta = fabs(rz_old) < 1e-20 ? 0.0 : rz / rz_old;
+    if (stop) break;
+  }
+  if (own) a.x[v] = make_float4(x.x, x.y, x.z, 0.f);
+  tr.finish(iter);
+  if (q == 0 && tid == 0) {
+    a.result[0] = iter;
+    a.result[1] = status;
+    *a.result_rr = (float)rr;
+    if (a.stats) {
+      atomicAdd(a.stats, iter);
+      atomicAdd(a.stats + 1, 1);
+      if (a.first_solve) atomicAdd(a.stats + 2, iter);
+    }
+  }
+}
+
+template <int F>
+size_t dsm_smem_bytes() {
+  return sizeof(DsmShared<F>);
+}
+
+template <int F>
+int dsm_max_cluster() {
+  static const int n = [] {
+    const size_t smem = sizeof(DsmShared<F>);
+    if (cudaFuncSetAttribute(cg_dsm_cluster_kernel<F>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(cg_dsm_cluster_kernel<F>,
+                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kDsmMaxCtas);
+    cfg.blockDim = dim3(32 * F);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = kDsmMaxCtas;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int m = 0;
+    if (cudaOccupancyMaxPotentialClusterSize(&m, cg_dsm_cluster_kernel<F>, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      m = 0;
+    }
+    return m < kDsmMaxCtas ? m : kDsmMaxCtas;
+  }();
+  return n;
+}
+
+template <int F>
+void launch_dsm(const CgArgs& a, int nctas, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nctas);
+  cfg.blockDim = dim3(32 * F);
+  cfg.dynamicSmemBytes = sizeof(DsmShared<F>);
+  cfg.stream = st;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = nctas;
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  CUDA_CHECK(cudaLaunchKernelEx(&cfg, cg_dsm_cluster_kernel<F>, a));
+  SILK_LAUNCHED();
+}
+
 }  // namespace
 
 void launch_galerkin_fill(const GalerkinDev& g, const double* src_vals,
@@ -1371,6 +1876,20 @@ void launch_cg_resident(const CgArgs& a, int grid, cudaStream_t st) {
   CUDA_CHECK(cudaLaunchCooperativeKernel((const void*)cg_resident_kernel, dim3(grid),
                                          dim3(kResThreads), args, smem, st));
   SILK_LAUNCHED();
+}
+
+int cg_dsm_ctas(int nbank0, int f) {
+  if (nbank0 <= 0 || (f != 8 && f != 16)) return 0;
+  const int nctas = div_up(nbank0, f);
+  const int cap = f == 8 ? dsm_max_cluster<8>() : dsm_max_cluster<16>();
+  return nctas >= 2 && nctas <= cap ? nctas : 0;
+}
+
+void launch_cg_dsm(const CgArgs& a, int nctas, cudaStream_t st) {
+  if (a.dsm_f == 8)
+    launch_dsm<8>(a, nctas, st);
+  else
+    launch_dsm<16>(a, nctas, st);
 }
 
 }  // namespace silkb

@@ -92,6 +92,10 @@ struct CgArgs {
   int* fail = nullptr;          // kFail* bits: a barrier wait gave up
   long long barrier_spin_limit = 0;  // > 0: grid-barrier polls before giving up
   int withhold_block = -1;      // >= 0: that block skips its barrier arrivals (tests)
+  // Cluster form with redundant coarse levels (cg_dsm_cluster_kernel): fine
+  // banks per CTA (8 or 16; 0 = not this form).  It uses the rb_ptr / rb_w /
+  // rent / halo_off / halo_col layout built for blocks of dsm_f fine banks.
+  int dsm_f = 0;
   // Optional phase trace of block 0 (null = off): [0] globaltimer and [1]
   // clock64 at entry, [2] and [3] at exit, [4] traced iterations, [5] kernel
   // form (0 streaming, 1 resident), then for each of the first kCgTraceIters
@@ -132,5 +136,11 @@ void launch_bank_invert(const MasLevelDev& lv, bool fine, const int* part_off,
 int cg_grid_size(int nslices, int nbank0);
 void launch_cg(const CgArgs& a, int grid, cudaStream_t st);
 void launch_cg_resident(const CgArgs& a, int grid, cudaStream_t st);
+// Cluster form with redundant coarse levels: CTAs of f fine banks (8 or 16)
+// for nbank0 fine banks if they form one launchable cluster (at most 16
+// CTAs), else 0.
+constexpr int kDsmCoarseBankLimit = 16;  // banks of all coarse levels together
+int cg_dsm_ctas(int nbank0, int f);
+void launch_cg_dsm(const CgArgs& a, int nctas, cudaStream_t st);
 
 }  // namespace silkb

@@ -112,6 +112,9 @@ void World::clear() {
 }
 
 silk_status World::set_solver_options(const silk_solver_options& o) {
+  // The CG launch form is chosen when the solver layout is built.
+  if (o.cg_form != opt.cg_form || o.resident_halo_limit != opt.resident_halo_limit)
+    invalidate_layout();
   opt = o;
   if (opt.cg_max_iter <= 0) opt.cg_max_iter = 1000;
   return SILK_OK;
@@ -429,23 +432,25 @@ SolverView World::view() {
 // above fit the shared memory of a block.  The off-diagonal part of L is
 // re-sliced per fine bank; a column inside the block is stored as -1 - slot,
 // and the entries from other blocks come first in each row.
-void World::build_resident_layout(Cloth& c) {
-  const ClothSetup& S = *c.setup;
-  ClothDev& d = c.dev;
-  d.res_blocks = 0;
-  d.res_grid = 0;
+namespace {
+
+// Per-fine-bank ELL slices of the off-diagonal rows of L for CTAs of `bpb`
+// fine banks: a column inside the CTA is its shared-memory slot
+// (bank within the CTA * 32 + lane), a column outside it the next free halo
+// slot bpb * 32 + i (at most halo_cap halo vertices per CTA; further columns
+// stay global vertex indices and halo_full becomes false), entries ordered
+// by schedule_bank_rows.
+struct BlockLayout {
+  std::vector<int> ptr, width, halo_off, halo_col;
+  std::vector<int2> ent;
+  bool halo_full = true;
+};
+
+BlockLayout block_layout(const ClothSetup& S, int bpb, int halo_cap) {
+  BlockLayout L;
   const int nbank0 = S.fine.nbank;
-  const int nblocks = div_up(nbank0, BANK);
-  if (S.levels > 0) {
-    for (int b = 0; b < nbank0; ++b)
-      if (S.fine.bank_ncco[b] != 1 || S.fine.bank_cco_base[b] != b) return;
-    if (S.coarse[0].nbank != nblocks) return;
-    int upper = 0;
-    for (int l = 2; l <= S.levels; ++l) upper += S.coarse[l - 1].nbank;
-    if (upper > kResCoarseBanks) return;
-  }
-  int grid = cg_resident_grid(nblocks);
-  if (grid == 0) return;
+  const int nblocks = div_up(nbank0, bpb);
+  const int nthreads = bpb * BANK;
   const int nv = S.nv;
   std::vector<int> part_of(nv), lane_of(nv);
   for (int b = 0; b < nbank0; ++b)
@@ -453,50 +458,45 @@ void World::build_resident_layout(Cloth& c) {
       part_of[v] = b;
       lane_of[v] = v - S.part_offsets[b];
     }
-  std::vector<int> ptr(nbank0 + 1, 0), width(nbank0, 0);
+  L.ptr.assign(nbank0 + 1, 0);
+  L.width.assign(nbank0, 0);
   for (int b = 0; b < nbank0; ++b) {
     int w = 0;
     for (int v = S.part_offsets[b]; v < S.part_offsets[b + 1]; ++v)
       w = std::max(w, S.Lrows[v + 1] - S.Lrows[v] - 1);
-    width[b] = w;
-    ptr[b + 1] = ptr[b] + BANK * w;
+    L.width[b] = w;
+    L.ptr[b + 1] = L.ptr[b] + BANK * w;
   }
-  // Halo of each block: the vertices outside it that its rows read, gathered
-  // into shared memory once per product (at most kResHalo; any further ones
-  // are read from global memory by the rows themselves).
-  std::vector<int> halo_off(nblocks + 1, 0), halo_col;
+  L.halo_off.assign(nblocks + 1, 0);
   std::vector<int> halo_slot(nv, -1), halo_mark(nv, -1);
-  bool halo_overflow = false;
-  const int halo_cap = opt.resident_halo_limit > 0 ? std::min(opt.resident_halo_limit, kResHalo)
-                                                   : kResHalo;
   for (int k = 0; k < nblocks; ++k) {
-    halo_off[k] = (int)halo_col.size();
-    for (int bb = k * BANK; bb < std::min(nbank0, (k + 1) * BANK); ++bb)
+    L.halo_off[k] = (int)L.halo_col.size();
+    for (int bb = k * bpb; bb < std::min(nbank0, (k + 1) * bpb); ++bb)
       for (int v = S.part_offsets[bb]; v < S.part_offsets[bb + 1]; ++v)
         for (int q = S.Lrows[v]; q < S.Lrows[v + 1]; ++q) {
           int col = S.Lcols[q];
-          if (part_of[col] / BANK == k || halo_mark[col] == k) continue;
-          if ((int)halo_col.size() - halo_off[k] >= halo_cap) {
-            halo_overflow = true;
+          if (part_of[col] / bpb == k || halo_mark[col] == k) continue;
+          if ((int)L.halo_col.size() - L.halo_off[k] >= halo_cap) {
+            L.halo_full = false;
             continue;
           }
           halo_mark[col] = k;
-          halo_col.push_back(col);
+          L.halo_col.push_back(col);
         }
   }
-  halo_off[nblocks] = (int)halo_col.size();
-  std::vector<int2> ent(std::max(ptr[nbank0], 1));
+  L.halo_off[nblocks] = (int)L.halo_col.size();
+  L.ent.assign(std::max(L.ptr[nbank0], 1), make_int2(0, 0));
   std::vector<std::vector<std::pair<int, int>>> row(BANK);
   std::vector<std::pair<int, int>> sched;
   int halo_block = -1;
   for (int b = 0; b < nbank0; ++b) {
-    const int k = b / BANK;
+    const int k = b / bpb;
     if (k != halo_block) {
       if (halo_block >= 0)
-        for (int i = halo_off[halo_block]; i < halo_off[halo_block + 1]; ++i)
-          halo_slot[halo_col[i]] = -1;
-      for (int i = halo_off[k]; i < halo_off[k + 1]; ++i)
-        halo_slot[halo_col[i]] = kResThreads + i - halo_off[k];
+        for (int i = L.halo_off[halo_block]; i < L.halo_off[halo_block + 1]; ++i)
+          halo_slot[L.halo_col[i]] = -1;
+      for (int i = L.halo_off[k]; i < L.halo_off[k + 1]; ++i)
+        halo_slot[L.halo_col[i]] = nthreads + i - L.halo_off[k];
       halo_block = k;
     }
     for (int lane = 0; lane < BANK; ++lane) {
@@ -510,27 +510,81 @@ void World::build_resident_layout(Cloth& c) {
         int bits;
         std::memcpy(&bits, &val, 4);
         int cb = part_of[col];
-        if (cb / BANK == k)
-          row[lane].emplace_back(-1 - ((cb - k * BANK) * BANK + lane_of[col]), bits);
+        if (cb / bpb == k)
+          row[lane].emplace_back(-1 - ((cb - k * bpb) * BANK + lane_of[col]), bits);
         else if (halo_slot[col] >= 0)
           row[lane].emplace_back(-1 - halo_slot[col], bits);
         else
           row[lane].emplace_back(col, bits);
       }
     }
-    sched.resize((size_t)BANK * width[b]);
-    schedule_bank_rows(row, width[b], (b - k * BANK) * BANK, sched.data());
+    sched.resize((size_t)BANK * L.width[b]);
+    schedule_bank_rows(row, L.width[b], (b - k * bpb) * BANK, sched.data());
     for (size_t i = 0; i < sched.size(); ++i)
-      ent[ptr[b] + i] = make_int2(sched[i].first, sched[i].second);
+      L.ent[L.ptr[b] + i] = make_int2(sched[i].first, sched[i].second);
   }
+  if (L.halo_col.empty()) L.halo_col.push_back(0);
+  return L;
+}
+
+}  // namespace
+
+// Launch form of the cloth's CG solve, chosen when its layout is built:
+//  1. the cluster form with redundant coarse levels (CTAs of 8 or 16 fine
+//     banks, one cluster of at most 16 CTAs, every coarse bank held by every
+//     CTA, every off-CTA column in the CTA's halo);
+//  2. the resident form (one CTA per first-level coarse bank, a cluster of up
+//     to 16 or a cooperative grid);
+//  3. otherwise the streaming form.
+// Forms 1 and 2 need every fine bank to be one first-level coarse node.
+// solver option cg_form: 0 all forms, 2 forms 2 and 3, 1 form 3 only.
+void World::build_resident_layout(Cloth& c) {
+  const ClothSetup& S = *c.setup;
+  ClothDev& d = c.dev;
+  d.res_blocks = 0;
+  d.res_grid = 0;
+  d.dsm_ctas = 0;
+  d.dsm_f = 0;
+  const int nbank0 = S.fine.nbank;
+  const int nblocks = div_up(nbank0, BANK);
+  int upper = 0, all_coarse = 0;
+  if (S.levels > 0) {
+    for (int b = 0; b < nbank0; ++b)
+      if (S.fine.bank_ncco[b] != 1 || S.fine.bank_cco_base[b] != b) return;
+    if (S.coarse[0].nbank != nblocks) return;
+    for (int l = 1; l <= S.levels; ++l) {
+      all_coarse += S.coarse[l - 1].nbank;
+      if (l >= 2) upper += S.coarse[l - 1].nbank;
+    }
+  }
+  if (opt.cg_form == 1) return;
   cudaStream_t st = stream;
-  d.rb_ptr.upload(ptr, st);
-  d.rb_w.upload(width, st);
-  d.rent.upload(ent, st);
-  d.res_halo_off.upload(halo_off, st);
-  d.res_halo_full = !halo_overflow;
-  if (halo_col.empty()) halo_col.push_back(0);
-  d.res_halo_col.upload(halo_col, st);
+  auto upload = [&](const BlockLayout& L) {
+    d.rb_ptr.upload(L.ptr, st);
+    d.rb_w.upload(L.width, st);
+    d.rent.upload(L.ent, st);
+    d.res_halo_off.upload(L.halo_off, st);
+    d.res_halo_full = L.halo_full;
+    d.res_halo_col.upload(L.halo_col, st);
+  };
+  if (opt.cg_form == 0 && S.levels > 0 && all_coarse <= kDsmCoarseBankLimit) {
+    for (int f : {8, 16}) {
+      const int n = cg_dsm_ctas(nbank0, f);
+      if (n == 0) continue;
+      BlockLayout L = block_layout(S, f, BANK * f);
+      if (!L.halo_full) continue;
+      upload(L);
+      d.dsm_ctas = n;
+      d.dsm_f = f;
+      return;
+    }
+  }
+  if (S.levels > 0 && upper > kResCoarseBanks) return;
+  int grid = cg_resident_grid(nblocks);
+  if (grid == 0) return;
+  const int halo_cap = opt.resident_halo_limit > 0 ? std::min(opt.resident_halo_limit, kResHalo)
+                                                   : kResHalo;
+  upload(block_layout(S, BANK, halo_cap));
   d.res_blocks = nblocks;
   d.res_grid = grid;
 }
@@ -694,6 +748,15 @@ void World::build_cloth_device(Cloth& c) {
     float4* rin = l == 1 ? d.fine.rout.p : d.coarse[l - 2].rout.p;
     a.coarse[l - 1] = lv_dev(S.coarse[l - 1], d.coarse[l - 1],
                              S.galerkin[l - 1].n, rin);
+  }
+  if (d.dsm_ctas > 0) {
+    a.dsm_f = d.dsm_f;
+    a.rb_ptr = d.rb_ptr.p;
+    a.rb_w = d.rb_w.p;
+    a.rent = d.rent.p;
+    a.halo_off = d.res_halo_off.p;
+    a.halo_col = d.res_halo_col.p;
+    a.halo_full = 1;
   }
   if (d.res_grid != 0) {
     a.res_blocks = d.res_blocks;
@@ -922,10 +985,14 @@ void World::cg_solve(Cloth& c, float rel_tol, bool first, cudaStream_t st) {
   a.fail = cg_fail.p;
   a.barrier_spin_limit = opt.barrier_spin_limit;
   a.withhold_block = opt.debug_withhold_block - 1;
-  const bool resident = c.dev.res_grid != 0 && opt.cg_form != 1;
-  if (resident) stats.cg_resident_solves += 1;
+  const bool dsm = c.dev.dsm_ctas > 0;
+  const bool resident = !dsm && c.dev.res_grid != 0;
+  if (dsm || resident) stats.cg_resident_solves += 1;
+  if (dsm) stats.cg_cluster_solves += 1;
   auto launch = [&]() {
-    if (resident)
+    if (dsm)
+      launch_cg_dsm(a, c.dev.dsm_ctas, st);
+    else if (resident)
       launch_cg_resident(a, c.dev.res_grid, st);
     else
       launch_cg(a, c.dev.cg_grid, st);
@@ -1078,8 +1145,9 @@ bool World::admm_solve() {
       std::vector<int> forked;
       for (int k = 0; k < (int)cloths.size(); ++k) {
         const ClothDev& d = cloths[k]->dev;
-        const bool resident = d.res_grid != 0 && opt.cg_form != 1;
-        if (cloths.size() > 1 && (resident ? d.res_grid < 0 : d.cg_grid < 0)) forked.push_back(k);
+        const bool resident = d.res_grid != 0;
+        const bool cluster = d.dsm_ctas > 0 || (resident ? d.res_grid < 0 : d.cg_grid < 0);
+        if (cloths.size() > 1 && cluster) forked.push_back(k);
       }
       if (!forked.empty()) {
         ensure_cloth_streams(cloths.size());

@@ -104,6 +104,8 @@ struct ClothDev {
   bool res_halo_full = false;              // every off-block column is in a halo
   int res_blocks = 0;         // resident form: blocks (0 = streaming form only)
   int res_grid = 0;           // cg_resident_grid(res_blocks)
+  int dsm_ctas = 0;           // cluster form with redundant coarse levels: CTAs (0 = not used)
+  int dsm_f = 0;              // its fine banks per CTA
   CgArgs cg;
   int cg_grid = 1;
   double bytes_per_iter_fp32 = 0.0;  // algorithmic DRAM bytes per CG iteration

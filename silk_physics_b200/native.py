@@ -99,7 +99,8 @@ class _StepStatsC(C.Structure):
                 ("min_toi", C.c_float), ("broadphase_candidates", C.c_int32),
                 ("kernel_launches", C.c_int64), ("cg_resident_solves", C.c_int32),
                 ("cg_first_solve_iterations", C.c_int32), ("learned_starts", C.c_int32),
-                ("extrapolated_starts", C.c_int32), ("reserved", C.c_int32 * 2)]
+                ("extrapolated_starts", C.c_int32), ("cg_cluster_solves", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 @dataclass
@@ -160,7 +161,7 @@ class SolverOptions:
     cg_max_iter: int = 1000
     mas_bf16: bool = False
     profile: int = 0  # 1: CUDA-event kernel timing; 2: also the CG phase trace
-    cg_form: int = 0  # 0: resident CG kernel where possible; 1: streaming form
+    cg_form: int = 0  # 0: cluster form, else resident, else streaming; 2: no cluster form; 1: streaming
     learned_warm_start: bool = False  # offer the loaded model's first-solve start
     capture_samples: bool = False     # record warm-start training samples
     contact_gs_form: int = 0          # 0: single-block Gauss-Seidel where possible; 1: grid
@@ -203,6 +204,7 @@ class StepStats:
     cg_first_solve_iterations: int = 0
     learned_starts: int = 0
     extrapolated_starts: int = 0
+    cg_cluster_solves: int = 0
 
 
 _F32P = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")

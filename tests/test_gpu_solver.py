@@ -161,33 +161,46 @@ def _gpu_run(s, steps, form, tol=1e-5, jitter=1e-4):
     return iters, resident
 
 
-# 32: one 2-block cluster; 80: a 7-block cluster; 128: a cooperative grid of
-# 17 blocks.
+# Form 0 (default): 32 -> the cluster form with redundant coarse levels on 5
+# CTAs of 8 fine banks; 80 -> the same on 14 CTAs of 16; 128 -> too many fine
+# banks for one such cluster: the resident form, a cooperative grid of 17
+# blocks.  Form 2 (resident): 32 a 2-block cluster, 80 a 7-block cluster,
+# 128 the grid.  Form 1: streaming.
 @pytest.mark.parametrize("s", [32, 80, 128])
 def test_resident_and_streaming_forms_against_oracle(oracle, s):
-    """The resident CG kernel (one block per first-level coarse bank) and the
-    streaming kernel run the same preconditioned iteration and differ only in
-    the order of FP64 block sums and of the off-diagonal terms of a row.  In
-    the well-conditioned, converged setting each form must be as close to
-    the FP64 oracle as 3x the FP32 oracle's own drift (floor 2e-6 m; the
-    drift grows with the mesh: about 1e-6 m at 32x32, 6e-6 m at 128x128);
-    in the default setting their CG iteration counts agree within 5 %."""
+    """The cluster form with redundant coarse levels, the resident CG kernel
+    (one block per first-level coarse bank) and the streaming kernel run the
+    same preconditioned iteration and differ only in the order of FP64 sums,
+    of the off-diagonal terms of a row and of the coarse bank solves.  In the
+    well-conditioned, converged setting each form must be as close to the
+    FP64 oracle as 3x the FP32 oracle's own drift (floor 2e-6 m; the drift
+    grows with the mesh: about 1e-6 m at 32x32, 6e-6 m at 128x128); in the
+    default setting their CG iteration counts agree within 5 %."""
     cloth = N.ClothConfig(elastic_stiffness=10.0, bending_stiffness=1e-4, density=5.0,
                           damping=0.01)
     kw = dict(inner=50, admm_tol=1e-6, cg_rel=1e-6, cloth=cloth, jitter=1e-4)
     _, _, _, o32, _ = _pair(oracle, s, 1, **kw)
     _, _, _, o64, _ = _pair(oracle, s, 1, fp64=True, **kw)
     e3264 = np.abs(o32[0][2] - o64[0][2]).max()
-    for form in (0, 1):
-        _, _, _, og, _ = _pair(oracle, s, 1, form=form, **kw)
+    for form in (0, 2, 1):
+        w, _, _, og, _ = _pair(oracle, s, 1, form=form, **kw)
+        st = w.step_stats()
         eg64 = np.abs(og[0][1] - o64[0][2]).max()
-        print(f"s={s} form={form}: |gpu-o64| {eg64:.2e} |o32-o64| {e3264:.2e}")
+        print(f"s={s} form={form}: |gpu-o64| {eg64:.2e} |o32-o64| {e3264:.2e}, "
+              f"cluster solves {st.cg_cluster_solves} resident {st.cg_resident_solves} "
+              f"of {st.cg_solves}")
         assert eg64 <= max(3.0 * e3264, 2e-6)
-    ir, nres = _gpu_run(s, 3, 0)
+        if form == 0:
+            assert (st.cg_cluster_solves == st.cg_solves) == (s <= 80)
+        else:
+            assert st.cg_cluster_solves == 0
+    ic, ncl = _gpu_run(s, 3, 0)
+    ir, nres = _gpu_run(s, 3, 2)
     is_, nstr = _gpu_run(s, 3, 1)
-    print(f"s={s}: CG iterations resident {ir} streaming {is_}, resident solves {nres}")
+    print(f"s={s}: CG iterations default {ic} resident {ir} streaming {is_}")
     assert nres > 0 and nstr == 0
     assert all(abs(a - b) <= 0.05 * b for a, b in zip(ir, is_))
+    assert all(abs(a - b) <= 0.05 * b for a, b in zip(ic, is_))
 
 
 @pytest.mark.parametrize("form", [0, 1])
@@ -269,14 +282,15 @@ def test_resident_halo_overflow_against_oracle(oracle, s):
     through the cluster or grid and the overflow columns are read from
     global memory.  Same parity bound as the full-halo form: within 3x the
     FP32 oracle's drift of the FP64 oracle (floor 2e-6 m), resident form in
-    use (80: a 7-block cluster; 128: a 17-block cooperative grid)."""
+    use (cg_form 2; 80: a 7-block cluster; 128: a 17-block cooperative
+    grid)."""
     cloth = N.ClothConfig(elastic_stiffness=10.0, bending_stiffness=1e-4, density=5.0,
                           damping=0.01)
     kw = dict(inner=50, admm_tol=1e-6, cg_rel=1e-6, cloth=cloth, jitter=1e-4)
     _, _, _, o32, _ = _pair(oracle, s, 1, **kw)
     _, _, _, o64, _ = _pair(oracle, s, 1, fp64=True, **kw)
     e3264 = np.abs(o32[0][2] - o64[0][2]).max()
-    w, _, _, og, _ = _pair(oracle, s, 1, halo_limit=16, **kw)
+    w, _, _, og, _ = _pair(oracle, s, 1, halo_limit=16, form=2, **kw)
     st = w.step_stats()
     eg64 = np.abs(og[0][1] - o64[0][2]).max()
     print(f"s={s} halo limit 16: |gpu-o64| {eg64:.2e} |o32-o64| {e3264:.2e}, "
