@@ -94,9 +94,16 @@ typedef struct {
                                  2: resident where it fits, else streaming;
                                  1: streaming always (applies when the solver
                                  layout is built; changing it rebuilds it) */
-  int32_t learned_warm_start; /* 1: offer the loaded model's prediction as the
-                                 start of each outer iteration's first CG solve */
-  int32_t capture_samples;    /* 1: record warm-start training samples */
+  int32_t learned_warm_start; /* 1: offer the loaded first-solve model's
+                                 prediction as the start of each outer
+                                 iteration's first CG solve and, when an
+                                 iterate model is loaded, its prediction of
+                                 the next ADMM iterate as the start of every
+                                 later CG solve (from the third of an ADMM
+                                 solve on) */
+  int32_t capture_samples;    /* bit 1: record first-solve training samples;
+                                 bit 2: record iterate-model training samples
+                                 (256 vertices per ADMM iteration) */
   int32_t contact_gs_form;    /* 0: single-block contact Gauss-Seidel where the
                                  contacts fit it, else grid; 1: grid always */
   int32_t admm_extrapolated_start; /* 1: offer 2 x_k - x_(k-1) (the last two ADMM
@@ -159,7 +166,8 @@ typedef struct {
                                   with redundant coarse levels (CTAs of 8 or 16
                                   fine banks exchanging through distributed
                                   shared memory) */
-  int32_t reserved[1];
+  int32_t learned_iterate_starts; /* later CG solves of an ADMM solve that started
+                                  from the iterate model's prediction */
 } silk_step_stats;
 
 /* --- World lifetime (silk.hpp:92-100) ---------------------------------- */
@@ -354,9 +362,22 @@ silk_status silk_color_contacts(const int32_t* verts4, const uint64_t* prio,
  * W4 (64x8), b4 (8), feature mean (16), feature std (16), output scale (8);
  * weights row-major (input, output). */
 #define SILK_MLP_PARAMS 9968
-/* Load a trained model into the world (NULL disables it); used when the
- * solver option learned_warm_start is 1. */
+/* Load trained models into the world (NULL disables them); used when the
+ * solver option learned_warm_start is 1.  n = SILK_MLP_PARAMS: the
+ * first-solve model; n = 2 * SILK_MLP_PARAMS: the first-solve model followed
+ * by the iterate model, the same network over 13 features of the last three
+ * ADMM iterates x_k, x_(k-1), x_(k-2) (x_k - x_(k-1), x_(k-1) - x_(k-2), the
+ * 1-ring means of both, the pin flag, all over sigma = the RMS of
+ * x_k - x_(k-1) over the vertices) that predicts (x_(k+1) - x_k) / sigma;
+ * x_k + sigma * prediction is offered to the solve for x_(k+1) like the
+ * first-solve start (taken only where it lowers the residual, the plain
+ * start's residual stays the stopping reference). */
 silk_status silk_set_warm_start_model(silk_world* w, const float* params, int64_t n);
+/* Iterate-model training samples of the last step (solver option
+ * capture_samples bit 2): up to cap rows of 16 features (13 used) and 4
+ * targets (3 used, (x_(k+1) - x_k) / sigma); *n = rows written. */
+silk_status silk_get_iterate_samples(silk_world* w, float* features, float* targets, int64_t cap,
+                                     int32_t* n);
 /* Training samples of the last step (solver option capture_samples = 1):
  * per vertex 16 features (13 used) and 4 targets (3 used: first CG solution
  * minus the inertial prediction, over the step scale dt^2 |g|), in the

@@ -461,6 +461,12 @@ silk_status silk_get_warm_start_samples(const silk_world* w, uint32_t handle,
   });
 }
 
+silk_status silk_get_iterate_samples(silk_world* w, float* features, float* targets,
+                                     int64_t cap, int32_t* n) {
+  if (!n || cap < 0 || (cap > 0 && (!features || !targets))) return SILK_ERR_INVALID_CONFIG;
+  return guard_init(w, [&](World& W) { return W.get_iterate_samples(features, targets, cap, n); });
+}
+
 silk_status silk_mlp_forward(const float* params, const float* features, int64_t n,
                              float* out) {
   if (!params || n < 0 || (n > 0 && (!features || !out))) return SILK_ERR_INVALID_CONFIG;

@@ -459,6 +459,108 @@ __global__ void warm_target_kernel(int n, const float4* __restrict__ x,
       make_float4((a.x - b.x) * inv_sigma, (a.y - b.y) * inv_sigma, (a.z - b.z) * inv_sigma, 0.f);
 }
 
+// Learned iterate start (CG solves of ADMM iterations >= 3): scale of the
+// last ADMM step, sigma = sqrt(mean |x_k - x_(k-1)|^2) over the vertices
+// (one block, FP64 sum in a fixed order), floored so the features stay finite.
+__global__ void __launch_bounds__(1024) iterate_scale_kernel(int n, const float4* __restrict__ x,
+                                                             const float4* __restrict__ h1,
+                                                             float* __restrict__ sigma) {
+  __shared__ double part[32];
+  double acc = 0.0;
+  for (int v = threadIdx.x; v < n; v += blockDim.x) {
+    float4 a = x[v], b = h1[v];
+    float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    acc += (double)dx * dx + (double)dy * dy + (double)dz * dz;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) *sigma = fmaxf((float)sqrt(t / (double)(n > 0 ? n : 1)), 1e-20f);
+  }
+}
+
+// Features of the iterate model: the last two ADMM steps x_k - x_(k-1) and
+// x_(k-1) - x_(k-2), their 1-ring means (all over sigma) and the pin flag.
+__global__ void iterate_features_kernel(int n, const float4* __restrict__ x,
+                                        const float4* __restrict__ h1,
+                                        const float4* __restrict__ h2,
+                                        const uint8_t* __restrict__ pin,
+                                        const int* __restrict__ ring_off,
+                                        const int* __restrict__ ring,
+                                        const float* __restrict__ sigma,
+                                        float* __restrict__ feat) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  const float is = 1.0f / *sigma;
+  float4 a = x[v], b = h1[v], c = h2[v];
+  float m1x = 0.f, m1y = 0.f, m1z = 0.f, m2x = 0.f, m2y = 0.f, m2z = 0.f;
+  int beg = ring_off[v], end = ring_off[v + 1];
+  for (int q = beg; q < end; ++q) {
+    int u = ring[q];
+    float4 ua = x[u], ub = h1[u], uc = h2[u];
+    m1x += ua.x - ub.x;
+    m1y += ua.y - ub.y;
+    m1z += ua.z - ub.z;
+    m2x += ub.x - uc.x;
+    m2y += ub.y - uc.y;
+    m2z += ub.z - uc.z;
+  }
+  const float ic = (end > beg ? 1.0f / (float)(end - beg) : 0.0f) * is;
+  float4* f = reinterpret_cast<float4*>(feat + (size_t)v * kMlpK);
+  f[0] = make_float4((a.x - b.x) * is, (a.y - b.y) * is, (a.z - b.z) * is, (b.x - c.x) * is);
+  f[1] = make_float4((b.y - c.y) * is, (b.z - c.z) * is, m1x * ic, m1y * ic);
+  f[2] = make_float4(m1z * ic, m2x * ic, m2y * ic, m2z * ic);
+  f[3] = make_float4(pin[v] ? 1.0f : 0.0f, 0.f, 0.f, 0.f);
+}
+
+// x_pred = x + sigma * out_scale * MLP output.
+__global__ void iterate_combine_kernel(int n, const float* __restrict__ o,
+                                       const float* __restrict__ params,
+                                       const float4* __restrict__ x,
+                                       const float* __restrict__ sigma,
+                                       float4* __restrict__ xp) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  const float sg = *sigma;
+  float4 b = x[v];
+  xp[v] = make_float4(b.x + sg * params[kOffOutScale] * o[3 * v],
+                      b.y + sg * params[kOffOutScale + 1] * o[3 * v + 1],
+                      b.z + sg * params[kOffOutScale + 2] * o[3 * v + 2], 0.f);
+}
+
+// Training samples of the iterate model: m vertices (a stride through the
+// mesh, shifted by `salt` from one iteration to the next) with their
+// features and target (x_new - x_old) / sigma, appended while the buffer has
+// room (the counter keeps counting).
+__global__ void iterate_sample_kernel(int m, int n, unsigned salt, const float* __restrict__ feat,
+                                      const float4* __restrict__ x_new,
+                                      const float4* __restrict__ x_old,
+                                      const float* __restrict__ sigma,
+                                      float* __restrict__ out_feat, float* __restrict__ out_tgt,
+                                      int* __restrict__ counter, int cap) {
+  __shared__ int base;
+  if (threadIdx.x == 0) base = atomicAdd(counter, m);
+  __syncthreads();
+  const float is = 1.0f / *sigma;
+  const unsigned stride = (unsigned)(n / m > 1 ? n / m : 1);
+  for (int j = threadIdx.x; j < m; j += blockDim.x) {
+    const int slot = base + j;
+    if (slot >= cap) return;
+    const int v = (int)((salt + (unsigned)j * stride) % (unsigned)n);
+    const float4* fs = reinterpret_cast<const float4*>(feat + (size_t)v * kMlpK);
+    float4* fd = reinterpret_cast<float4*>(out_feat + (size_t)slot * kMlpK);
+    for (int k = 0; k < kMlpK / 4; ++k) fd[k] = fs[k];
+    float4 a = x_new[v], b = x_old[v];
+    reinterpret_cast<float4*>(out_tgt)[slot] =
+        make_float4((a.x - b.x) * is, (a.y - b.y) * is, (a.z - b.z) * is, 0.f);
+  }
+}
+
 int fwd_grid(int n) {
   int tiles = (n + 15) / 16;
   int blocks = (tiles + kFwdWarps - 1) / kFwdWarps;
@@ -544,4 +646,29 @@ void warm_target(int n, const float4* x, const float4* y, float inv_sigma, float
   SILK_LAUNCHED();
 }
 
+void iterate_predict(const MlpDev& m, int n, const float4* x, const float4* h1, const float4* h2,
+                     const uint8_t* pin, const int* ring_off, const int* ring, float* sigma,
+                     float* feat, float* out_tmp, float4* x_pred, cudaStream_t st) {
+  if (n <= 0) return;
+  iterate_scale_kernel<<<1, 1024, 0, st>>>(n, x, h1, sigma);
+  SILK_LAUNCHED();
+  iterate_features_kernel<<<div_up(n, 256), 256, 0, st>>>(n, x, h1, h2, pin, ring_off, ring, sigma,
+                                                          feat);
+  SILK_LAUNCHED();
+  if (!m.params) return;  // features only (sample capture without a model)
+  mlp_forward(m, feat, n, out_tmp, st);
+  iterate_combine_kernel<<<div_up(n, 256), 256, 0, st>>>(n, out_tmp, m.params, x, sigma, x_pred);
+  SILK_LAUNCHED();
+}
+
+void iterate_samples(int m, int n, unsigned salt, const float* feat, const float4* x_new,
+                     const float4* x_old, const float* sigma, float* out_feat, float* out_tgt,
+                     int* counter, int cap, cudaStream_t st) {
+  if (n <= 0 || m <= 0) return;
+  iterate_sample_kernel<<<1, 256, 0, st>>>(m, n, salt, feat, x_new, x_old, sigma, out_feat,
+                                           out_tgt, counter, cap);
+  SILK_LAUNCHED();
+}
+
 }  // namespace silkb
+

@@ -71,6 +71,20 @@ void warm_predict(const MlpDev& m, int n, const float* feat, const float4* y, fl
 void warm_target(int n, const float4* x, const float4* y, float inv_sigma, float* t,
                  cudaStream_t st);
 
+// Learned iterate start: sigma (device scalar) = RMS of x - h1; features of
+// (x, h1 = x_(k-1), h2 = x_(k-2)) into feat (n x 16); with a model (m.params
+// not null) x_pred = x + sigma * out_scale * MLP(feat).
+void iterate_predict(const MlpDev& m, int n, const float4* x, const float4* h1, const float4* h2,
+                     const uint8_t* pin, const int* ring_off, const int* ring, float* sigma,
+                     float* feat, float* out_tmp, float4* x_pred, cudaStream_t st);
+// Append m samples (features from feat, target (x_new - x_old) / sigma) to
+// out_feat / out_tgt at the counter's position while below cap.
+void iterate_samples(int m, int n, unsigned salt, const float* feat, const float4* x_new,
+                     const float4* x_old, const float* sigma, float* out_feat, float* out_tgt,
+                     int* counter, int cap, cudaStream_t st);
+constexpr int kIterSamplesPerSolve = 256;   // vertices recorded per ADMM iteration
+constexpr int kIterSampleCap = 1 << 19;     // samples per step
+
 // Standalone entry points on host buffers (the trainer and the gradient
 // checks): forward outputs (n x 3), loss and gradient, Adam training.
 void mlp_forward_host(const float* params, const float* feat, int64_t n, float* out);

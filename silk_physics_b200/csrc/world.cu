@@ -966,6 +966,9 @@ void World::cg_solve(Cloth& c, float rel_tol, bool first, cudaStream_t st) {
   if (first && has_model && opt.learned_warm_start) {
     a.x_alt = xpred.p + c.voff;
     a.alt_stat = 3;
+  } else if (!first && iter_ready) {
+    a.x_alt = iter_pred.p + c.voff;
+    a.alt_stat = 5;
   } else if (!first && admm_ext_ready) {
     a.x_alt = admm_ext.p + c.voff;
     a.alt_stat = 4;
@@ -1031,14 +1034,18 @@ silk_status World::debug_cg_trace(uint32_t h, int64_t* out, int64_t cap, int32_t
   return SILK_OK;
 }
 
+// n = kMlpParams: the first-solve model; n = 2 kMlpParams: the first-solve
+// model followed by the iterate model.
 silk_status World::set_warm_start_model(const float* params, int64_t n) {
   if (!params) {
     has_model = false;
+    has_iter_model = false;
     return SILK_OK;
   }
-  if (n != kMlpParams) return SILK_ERR_INVALID_CONFIG;
-  for (int i = kOffStd; i < kOffStd + kMlpK; ++i)
-    if (!(params[i] > 0.0f)) return SILK_ERR_INVALID_CONFIG;
+  if (n != kMlpParams && n != 2 * (int64_t)kMlpParams) return SILK_ERR_INVALID_CONFIG;
+  for (int64_t m = 0; m < n; m += kMlpParams)
+    for (int i = kOffStd; i < kOffStd + kMlpK; ++i)
+      if (!(params[m + i] > 0.0f)) return SILK_ERR_INVALID_CONFIG;
   for (int64_t i = 0; i < n; ++i)
     if (!std::isfinite(params[i])) return SILK_ERR_INVALID_CONFIG;
   ensure_stream();
@@ -1047,8 +1054,33 @@ silk_status World::set_warm_start_model(const float* params, int64_t n) {
   CUDA_CHECK(cudaMemcpyAsync(mlp_params.p, params, kMlpParams * sizeof(float),
                              cudaMemcpyHostToDevice, stream));
   mlp_prepare(mlp_params.p, mlp_frag.p, stream);
+  has_iter_model = n == 2 * (int64_t)kMlpParams;
+  if (has_iter_model) {
+    mlp2_params.alloc(kMlpParams);
+    mlp2_frag.alloc(kMlpFragWords);
+    CUDA_CHECK(cudaMemcpyAsync(mlp2_params.p, params + kMlpParams, kMlpParams * sizeof(float),
+                               cudaMemcpyHostToDevice, stream));
+    mlp_prepare(mlp2_params.p, mlp2_frag.p, stream);
+  }
   sync();
   has_model = true;
+  return SILK_OK;
+}
+
+silk_status World::get_iterate_samples(float* feat, float* target, int64_t cap, int* n) {
+  *n = 0;
+  if (!iter_samp_n.p) return SILK_OK;
+  sync();
+  int total = 0;
+  CUDA_CHECK(cudaMemcpy(&total, iter_samp_n.p, sizeof(int), cudaMemcpyDeviceToHost));
+  const int64_t m = std::min<int64_t>(std::min(total, kIterSampleCap), cap);
+  if (m > 0) {
+    CUDA_CHECK(cudaMemcpy(feat, iter_samp_feat.p, (size_t)m * kMlpK * sizeof(float),
+                          cudaMemcpyDeviceToHost));
+    CUDA_CHECK(cudaMemcpy(target, iter_samp_tgt.p, (size_t)m * 4 * sizeof(float),
+                          cudaMemcpyDeviceToHost));
+  }
+  *n = (int)m;
   return SILK_OK;
 }
 
@@ -1125,7 +1157,33 @@ bool World::admm_solve() {
   fa.cg_fail = cg_fail.p;
   bool contacts = coll_ && coll_->contact_count() > 0;
   admm_ext_ready = false;
+  iter_ready = false;
+  // Learned iterate start and its sample capture (solver options
+  // learned_warm_start with an iterate model loaded, capture_samples bit 2).
+  const bool iter_model = has_iter_model && opt.learned_warm_start;
+  const bool iter_capture = (opt.capture_samples & 2) != 0;
+  if (iter_model || iter_capture) {
+    for (DevBuf<float4>* b : {&iter_hist0, &iter_hist1, &iter_hist2, &iter_pred})
+      if (b->n < (size_t)nv_total) b->alloc(nv_total);
+    if (iter_feat.n < (size_t)kMlpK * nv_total) iter_feat.alloc((size_t)kMlpK * nv_total);
+    if (iter_out.n < (size_t)kMlpOut * nv_total) iter_out.alloc((size_t)kMlpOut * nv_total);
+    if (!iter_sigma.p) iter_sigma.alloc(1);
+  }
+  DevBuf<float4>* iter_ring[3] = {&iter_hist0, &iter_hist1, &iter_hist2};
   for (int it = 0; it < g.max_inner_iteration; ++it) {
+    if (it != 0 && (iter_model || iter_capture)) {
+      // x holds x_(it-1); slots (it-1) % 3 and (it-2) % 3 hold x_(it-2) and
+      // x_(it-3) from the previous iterations.
+      if (it >= 3) {
+        MlpDev m{iter_model ? mlp2_params.p : nullptr, mlp2_frag.p};
+        iterate_predict(m, nv_total, x.p, iter_ring[(it - 1) % 3]->p, iter_ring[(it - 2) % 3]->p,
+                        pin_flag.p, ring_off.p, ring.p, iter_sigma.p, iter_feat.p, iter_out.p,
+                        iter_pred.p, st);
+      }
+      CUDA_CHECK(cudaMemcpyAsync(iter_ring[it % 3]->p, x.p, nv_total * sizeof(float4),
+                                 cudaMemcpyDeviceToDevice, st));
+      iter_ready = iter_model && it >= 3;
+    }
     if (it != 0) {
       // Extrapolated start: from the third solve on, 2 x_k - x_(k-1) of the
       // last two iterates of this ADMM solve (the first solve starts from the
@@ -1169,10 +1227,14 @@ bool World::admm_solve() {
         }
       }
       for (int k : forked) CUDA_CHECK(cudaStreamWaitEvent(st, cloth_done_[k], 0));
-      if (it == 1 && opt.capture_samples && warm_first_) {
+      if (it == 1 && (opt.capture_samples & 1) && warm_first_) {
         warm_target(nv_total, x.p, ypred.p, 1.0f / warm_sigma(), warm_tgt.p, st);
         samples_valid = true;
       }
+      if (iter_capture && it >= 3)
+        iterate_samples(kIterSamplesPerSolve, nv_total, (unsigned)(it * 7919 + stats.admm_iterations),
+                        iter_feat.p, x.p, iter_ring[it % 3]->p, iter_sigma.p, iter_samp_feat.p,
+                        iter_samp_tgt.p, iter_samp_n.p, kIterSampleCap, st);
     }
     std::pair<cudaEvent_t, cudaEvent_t>* oe = opt.profile ? next_event_pair(events_other, events_other_used) : nullptr;
     if (oe) CUDA_CHECK(cudaEventRecord(oe->first, st));
@@ -1226,7 +1288,15 @@ silk_status World::solver_step() {
     events_other_used = 0;
     events_gs_used = 0;
     CUDA_CHECK(cudaMemcpyAsync(step_start.p, sx.p, nv * sizeof(float4), cudaMemcpyDeviceToDevice, st));
-    if (opt.capture_samples) samples_valid = false;
+    if (opt.capture_samples & 1) samples_valid = false;
+    if (opt.capture_samples & 2) {
+      if (!iter_samp_n.p) {
+        iter_samp_n.alloc(1);
+        iter_samp_feat.alloc((size_t)kIterSampleCap * kMlpK);
+        iter_samp_tgt.alloc((size_t)kIterSampleCap * 4);
+      }
+      iter_samp_n.zero(st);
+    }
     // init (main_loop.cu:24-76): damped velocity, fresh ADMM aux variables.
     launch_damp(nv, damp.p, sv.p, prev_v.p, st);
     zu.zero(st);
@@ -1321,6 +1391,7 @@ silk_status World::solver_step() {
       stats.cg_first_solve_iterations += q[2];
       stats.learned_starts += q[3];
       stats.extrapolated_starts += q[4];
+      stats.learned_iterate_starts += q[5];
       if (opt.profile) {
         double bpi = opt.mas_bf16 ? cloths[k]->dev.bytes_per_iter_bf16
                                   : cloths[k]->dev.bytes_per_iter_fp32;

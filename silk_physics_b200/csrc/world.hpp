@@ -185,6 +185,7 @@ class World {
   silk_status set_warm_start_model(const float* params, int64_t n);
   silk_status get_warm_start_samples(uint32_t h, float* feat, float* target, int64_t nv,
                                      int* valid);
+  silk_status get_iterate_samples(float* feat, float* target, int64_t cap, int* n);
 
   // Inspection.
   silk_status debug_partition(uint32_t h, int* perm, int64_t perm_len,
@@ -228,6 +229,15 @@ class World {
   DevBuf<float4> admm_prev, admm_ext;
   bool admm_ext_ready = false;
   DevBuf<int> ring_off, ring;
+  // Learned iterate start: second model, the last ADMM iterates (a ring of
+  // three: at iteration k, slot k % 3 receives x_(k-1) before the solve),
+  // scale, features, prediction and the step's training samples.
+  DevBuf<float> mlp2_params, iter_feat, iter_out, iter_sigma, iter_samp_feat, iter_samp_tgt;
+  DevBuf<uint32_t> mlp2_frag;
+  DevBuf<float4> iter_hist0, iter_hist1, iter_hist2, iter_pred;
+  DevBuf<int> iter_samp_n;
+  bool has_iter_model = false;
+  bool iter_ready = false;  // iter_pred holds a prediction for the coming solve
   bool has_model = false;
   bool samples_valid = false;
   bool warm_first_ = false;  // the current outer iteration is the step's first
@@ -261,7 +271,9 @@ class World {
   std::vector<cudaStream_t> cloth_streams_;  // per-cloth CG streams (multi-cloth worlds)
   std::vector<cudaEvent_t> cloth_done_;
   cudaEvent_t fork_ev_ = nullptr;
-  bool warm_active() const { return (has_model && opt.learned_warm_start) || opt.capture_samples; }
+  bool warm_active() const {
+    return (has_model && opt.learned_warm_start) || (opt.capture_samples & 1);
+  }
   float warm_sigma() const;
   bool admm_solve();  // false on divergence
   void sync();

@@ -100,7 +100,7 @@ class _StepStatsC(C.Structure):
                 ("kernel_launches", C.c_int64), ("cg_resident_solves", C.c_int32),
                 ("cg_first_solve_iterations", C.c_int32), ("learned_starts", C.c_int32),
                 ("extrapolated_starts", C.c_int32), ("cg_cluster_solves", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("learned_iterate_starts", C.c_int32)]
 
 
 @dataclass
@@ -163,7 +163,7 @@ class SolverOptions:
     profile: int = 0  # 1: CUDA-event kernel timing; 2: also the CG phase trace
     cg_form: int = 0  # 0: cluster form, else resident, else streaming; 2: no cluster form; 1: streaming
     learned_warm_start: bool = False  # offer the loaded model's first-solve start
-    capture_samples: bool = False     # record warm-start training samples
+    capture_samples: int = 0  # bit 1: first-solve samples, bit 2: iterate-model samples
     contact_gs_form: int = 0          # 0: single-block Gauss-Seidel where possible; 1: grid
     admm_extrapolated_start: bool = False  # offer 2 x_k - x_(k-1) as later CG starts
     resident_halo_limit: int = 0  # > 0: fewer halo slots per resident-CG block (0: 1024)
@@ -205,6 +205,7 @@ class StepStats:
     learned_starts: int = 0
     extrapolated_starts: int = 0
     cg_cluster_solves: int = 0
+    learned_iterate_starts: int = 0
 
 
 _F32P = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -274,6 +275,8 @@ def _load() -> C.CDLL:
         "silk_color_contacts": ([_I32P, _U64P, C.c_int64, _I32P, C.POINTER(C.c_int32)],
                                 C.c_int),
         "silk_set_warm_start_model": ([_W, C.c_void_p, C.c_int64], C.c_int),
+        "silk_get_iterate_samples": ([_W, _F32P, _F32P, C.c_int64, C.POINTER(C.c_int32)],
+                                     C.c_int),
         "silk_get_warm_start_samples": ([_W, C.c_uint32, _F32P, _F32P, C.c_int64,
                                          C.POINTER(C.c_int32)], C.c_int),
         "silk_mlp_forward": ([_F32P, _F32P, C.c_int64, _F32P], C.c_int),
@@ -541,6 +544,17 @@ class World:
         if st:
             raise RuntimeError(_result(st, self._w).to_string())
         return (f, t) if valid.value else None
+
+    def iterate_samples(self, cap: int = 1 << 19):
+        """Iterate-model samples of the last step (capture_samples bit 2):
+        (features n x 16, targets n x 4)."""
+        f = np.zeros((cap, 16), np.float32)
+        t = np.zeros((cap, 4), np.float32)
+        n = C.c_int32(0)
+        st = lib.silk_get_iterate_samples(self._w, f.reshape(-1), t.reshape(-1), cap, C.byref(n))
+        if st:
+            raise RuntimeError(_result(st, self._w).to_string())
+        return f[: n.value], t[: n.value]
 
     def debug_cg_trace(self, handle: int) -> dict | None:
         """Phase trace of the last CG solve (solver option profile = 2):

@@ -198,3 +198,66 @@ def test_learned_warm_start_in_the_solver():
     assert taken_bad == 0
     assert worse == plain
     np.testing.assert_array_equal(xb, xp)
+
+
+MODEL = Path(__file__).resolve().parents[1] / "silk_physics_b200" / "models" / "warm_start.npy"
+# Held-out gain required of the committed iterate model: CG iterations per
+# solve of the learned run at most this fraction of the plain run's.
+HELD_OUT_GAIN = 0.97
+
+
+def _held_out_run(params, learned, extrap=False, steps=2):
+    """A scene outside the training mix (seeds, size and radius of its own):
+    a 70 x 70 sheet of side 1.2 m over a sphere of radius 0.45 m, from its
+    free-fall state one step before contact; default settings, CG relative
+    tolerance 1e-5."""
+    V, F = S.grid_sheet(70, side=1.2, z=0.55, jitter=1e-4, seed=4242)
+    SV, SF = S.icosphere(4, 0.45, center=(0.05, -0.03, 0.0))
+    x0, v0 = S.free_fall_state(V, 7)
+    w = N.World()
+    assert w.init()
+    assert w.set_global_config(N.GlobalConfig(acceleration_z=-9.81))
+    assert w.set_solver_options(N.SolverOptions(fixed_linear_rel_tol=1e-5,
+                                                learned_warm_start=learned,
+                                                admm_extrapolated_start=extrap))
+    r, h = w.add_cloth(N.ClothConfig(), N.CollisionConfig(), V, F, [])
+    assert r
+    r, _ = w.add_obstacle(N.CollisionConfig(), SV, SF)
+    assert r
+    if params is not None:
+        assert w.set_warm_start_model(params)
+    assert w.set_cloth_state(h, x0, v0)
+    cg = solves = iter_starts = contacts = 0
+    for _ in range(steps):
+        r = w.solver_step()
+        assert r, r.to_string()
+        st = w.step_stats()
+        cg += st.cg_iterations
+        solves += st.cg_solves
+        iter_starts += st.learned_iterate_starts
+        contacts = st.contacts
+    x = np.zeros(V.size, np.float32)
+    assert w.get_cloth_position(h, x)
+    return cg / max(solves, 1), iter_starts, contacts, x
+
+
+@pytest.mark.gpu
+def test_trained_model_gains_on_held_out_scene():
+    """The committed model file (both networks, trained by
+    python -m silk_physics_b200.learned on solver samples of the training mix)
+    on a held-out contact scene: the iterate model's starts are taken and the
+    CG needs fewer iterations per solve than from the plain start (the
+    reference's warm start, the previous ADMM iterate), by at least
+    1 - HELD_OUT_GAIN; positions stay within the contact tolerance of the
+    plain run.  The ADMM-extrapolated start (2 x_k - x_(k-1)) is printed
+    beside them."""
+    params = L.load(str(MODEL))
+    assert params.size == 2 * L.N_PARAMS
+    plain, s0, c0, xp = _held_out_run(None, False)
+    learned, s1, c1, xl = _held_out_run(params, True)
+    extrap, _, _, _ = _held_out_run(None, False, extrap=True)
+    print(f"CG iterations per solve: plain {plain:.2f}, learned {learned:.2f} "
+          f"({s1} iterate-model starts), extrapolated {extrap:.2f}; contacts {c0} / {c1}")
+    assert s0 == 0 and s1 > 0 and c0 > 0
+    assert learned <= HELD_OUT_GAIN * plain
+    assert np.abs(xl - xp).max() < 1e-3
