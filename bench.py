@@ -530,7 +530,7 @@ STREAMING_PHASES = ["prolongation", "barrier 1", "SpMV", "barrier 2", "fine MAS"
 CLUSTER_PHASES = ["A: p update (own and halo)", "CTA barrier", "B: SpMV rows",
                   "B: p.Ap block sum + push", "cluster barrier 1", "C: pAp total",
                   "C: x/r update + fine MAS", "C: first-level push + r.z/r.r sum + push",
-                  "cluster barrier 2", "A: halo z load + totals", "A: restriction chain",
+                  "cluster barrier 2", "A: halo z + totals", "A: restriction chain",
                   "A: coarse bank solves", "A: coarse r.z sum", "A: stopping test"]
 FORM_NAMES = {0: "streaming", 1: "resident", 2: "cluster (redundant coarse levels)"}
 

@@ -1256,8 +1256,9 @@ int max_cluster_size() {
 //    solves of all levels, at most kDsmCoarseBanks banks) redundantly, in
 //    the same order, with identical results;
 //  * p at a halo vertex is computed by the CTA itself from the owner's
-//    fine-level z (published through global memory before the barrier) and
-//    the coarse z every CTA holds, with the owner's operations.
+//    fine-level z (stored by the owner into the CTA's shared memory before
+//    the barrier) and the coarse z every CTA holds, with the owner's
+//    operations.
 // Per iteration: p update | CTA barrier | SpMV + p.Ap | cluster barrier |
 // alpha, x/r update, fine MAS, pushes | cluster barrier | totals and coarse
 // levels.  Arithmetic per vector entry as in cg_resident_kernel except the
@@ -1267,10 +1268,16 @@ constexpr int kDsmCoarseBanks = kDsmCoarseBankLimit;  // held by every CTA
 constexpr int kDsmMaxCtas = 16;
 constexpr int kDsmPartSlots = 8;     // 0 r.z, 1 r.r, 2 p.Ap, 3..5 alternative start
 
+// Bank inverses in shared memory: FP32 as the full symmetric 32 x 32 matrix,
+// column-major (entry (row i, column k) at k * 32 + i), so that the 32 lanes
+// of a bank apply read one column in one conflict-free pass; BF16 as the
+// mma.m16n8k16 A fragments (the first 2 KB of the slot).
+constexpr int kDsmBankFloats = BANK * BANK;
+
 template <int W>
 struct DsmShared {
-  float Mf[W][kPacked];                   // the CTA's fine bank inverses
-  float Mc[kDsmCoarseBanks][kPacked];     // every coarse bank of every level
+  float Mf[W][kDsmBankFloats];                // the CTA's fine bank inverses
+  float Mc[kDsmCoarseBanks][kDsmBankFloats];  // every coarse bank of every level
   float4 pl[2 * 32 * W];                  // own slots, then the halo (at most 32 W)
   int4 hcm[32 * W];                       // coarse nodes of the halo vertices
   float4 rc[kDsmCoarseBanks * BANK];      // coarse-level inputs (first level pushed)
@@ -1280,7 +1287,35 @@ struct DsmShared {
   double red[W][3];
   double tot[3];
   double part[kDsmMaxCtas][kDsmPartSlots];  // partials of every CTA (pushed)
+  float4 zown[32 * W];                    // fine-level z of the own slots
+  float4 hzs[32 * W];                     // fine-level z of the halo (pushed by the owners)
+  int push[kDsmPushPerThread * 32 * W];   // this CTA's pushes (own slot, CTA, halo index)
 };
+
+__device__ __forceinline__ void stage_bank_full(const MasLevelDev& lv, int bank, float* slot,
+                                                int lane) {
+  const float* src = lv.M + (size_t)bank * kPacked;
+  for (int e = lane; e < kDsmBankFloats; e += 32)
+    slot[e] = src[upper_index(BANK, e & (BANK - 1), e >> 5)];
+  __syncwarp();
+}
+
+// z (lane row) = M r over columns [k0, k1) of a full column-major bank, with
+// the residuals read as shared-memory broadcasts: the products of
+// bank_apply_smem summed in the same order.
+__device__ __forceinline__ float3 bank_apply_full(const float* M, const float4* rs, int lane,
+                                                  int k0, int k1) {
+  float zx = 0.f, zy = 0.f, zz = 0.f;
+#pragma unroll 8
+  for (int k = k0; k < k1; ++k) {
+    float m = M[k * BANK + lane];
+    float4 rk = rs[k];
+    zx += m * rk.x;
+    zy += m * rk.y;
+    zz += m * rk.z;
+  }
+  return make_float3(zx, zy, zz);
+}
 
 // Off-diagonal row sum plus the diagonal term, every column in shared memory.
 __device__ __forceinline__ float3 dsm_row(const int2* e, int rw, const float4* pl, float d,
@@ -1328,7 +1363,7 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     if (tc)
       stage_bank_frag(lv, bank, slot, lane);
     else
-      stage_bank(lv, 0, bank, slot, lane);
+      stage_bank_full(lv, bank, slot, lane);
   };
   // Store this CTA's N partial sums (s.tot after a block sum) into slots
   // slot0.. of every CTA's s.part row q.
@@ -1401,6 +1436,8 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
       s.hcm[tid] = a.cmap[hcol];
     }
   }
+  const int npush = a.push_off[q + 1] - a.push_off[q];
+  for (int i = tid; i < npush; i += T) s.push[i] = a.push[a.push_off[q] + i];
   auto gather_halo = [&](const float4* ex) {
     if (hcol >= 0) s.pl[T + tid] = ldcg4(ex + hcol);
     __syncthreads();
@@ -1480,7 +1517,7 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
       // reads between the SpMV and the next p update.
       s.pl[tid] = make_float4(r.x, r.y, r.z, 0.f);
       __syncwarp();
-      z0 = bank_apply_smem(s.Mf[warp], s.pl + warp * BANK, lane);
+      z0 = bank_apply_full(s.Mf[warp], s.pl + warp * BANK, lane, 0, BANK);
     }
     if (!own) z0 = make_float3(0.f, 0.f, 0.f);
     const double rz = own ? (double)r.x * z0.x + (double)r.y * z0.y + (double)r.z * z0.z : 0.0;
@@ -1492,10 +1529,15 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
         *dst = make_float4(sx, sy, sz, 0.f);
       }
     }
-    if (own) a.z0[v] = make_float4(z0.x, z0.y, z0.z, 0.f);
+    s.zown[tid] = make_float4(z0.x, z0.y, z0.z, 0.f);
     const double v2[2] = {rz, rr};
-    block_sum(v2, 2);
+    block_sum(v2, 2);  // its barriers also publish zown to the CTA
     push_partials(0, 2);
+    for (int i = tid; i < npush; i += T) {
+      const int e = s.push[i];
+      float4* dst = cl.map_shared_rank(&s.hzs[e >> 15], (e >> 10) & 31);
+      *dst = s.zown[e & 1023];
+    }
     tr.stamp(iter, 7);
   };
   // Phase A head: totals and every coarse level.
@@ -1504,21 +1546,16 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     rr = total(1);
     if (levels == 0) return;
     tr.stamp(iter, 9);
-    // Restriction chain (warp sums per connected component of a bank).
-    for (int l = 0; l + 1 < levels; ++l) {
+    // Restriction chain: one warp per node of the next level sums its
+    // members (at most 32, one per lane) with a warp sum.
+    for (int l = 1; l < levels; ++l) {
       const MasLevelDev& lv = a.coarse[l];
-      for (int g = warp; g < lv.nbank; g += W) {
-        const bool valid = g * BANK + lane < lv.nnode;
-        float4 qv = s.rc[(cbo[l] + g) * BANK + lane];
-        float3 rl = valid ? make_float3(qv.x, qv.y, qv.z) : make_float3(0.f, 0.f, 0.f);
-        const int ncc = lv.ncco[g], base = lv.cco_base[g];
-        const int mine = lv.slot_cco[(size_t)g * BANK + lane];
-        for (int c = 0; c < ncc; ++c) {
-          float qx = warp_sum(mine == c ? rl.x : 0.f);
-          float qy = warp_sum(mine == c ? rl.y : 0.f);
-          float qz = warp_sum(mine == c ? rl.z : 0.f);
-          if (lane == 0) s.rc[cbo[l + 1] * BANK + base + c] = make_float4(qx, qy, qz, 0.f);
-        }
+      for (int nd = warp; nd < lv.nnode; nd += W) {
+        const int m0 = lv.member_off[nd], cnt = lv.member_off[nd + 1] - m0;
+        float4 qv = lane < cnt ? s.rc[cbo[l - 1] * BANK + lv.member[m0 + lane]]
+                               : make_float4(0.f, 0.f, 0.f, 0.f);
+        float qx = warp_sum(qv.x), qy = warp_sum(qv.y), qz = warp_sum(qv.z);
+        if (lane == 0) s.rc[cbo[l] * BANK + nd] = make_float4(qx, qy, qz, 0.f);
       }
       __syncthreads();
     }
@@ -1552,18 +1589,8 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
       } else {
         if (gok) {
           const int cols = BANK / split, k0 = part * cols;
-          const float* sm = s.Mc[g];
-          const float4* rs = s.rc + g * BANK;
-          float zx = 0.f, zy = 0.f, zz = 0.f;
-#pragma unroll 8
-          for (int kk = k0; kk < k0 + cols; ++kk) {
-            float m = sm[upper_index(BANK, lane, kk)];
-            float4 rk = rs[kk];
-            zx += m * rk.x;
-            zy += m * rk.y;
-            zz += m * rk.z;
-          }
-          s.zs[warp][lane] = make_float4(zx, zy, zz, 0.f);
+          float3 zp = bank_apply_full(s.Mc[g], s.rc + g * BANK, lane, k0, k0 + cols);
+          s.zs[warp][lane] = make_float4(zp.x, zp.y, zp.z, 0.f);
         }
         __syncthreads();
         if (gok && part == 0) {
@@ -1593,7 +1620,7 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
   __syncthreads();  // every warp has read pl in the residual rows
   mas_fine();
   cl.sync();
-  if (hcol >= 0) hz = ldcg4(a.z0 + hcol);
+  if (hcol >= 0) hz = s.hzs[tid];
   double rz, rr;
   totals(rz, rr);
   iter = 0;
@@ -1652,7 +1679,7 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     }
     cl.sync();
     tr.stamp(iter, 8);
-    if (hcol >= 0) hz = ldcg4(a.z0 + hcol);
+    if (hcol >= 0) hz = s.hzs[tid];
     const double rz_old = rz;
     totals(rz, rr);
     tr.stamp(iter, 13);

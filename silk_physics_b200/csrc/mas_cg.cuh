@@ -27,6 +27,10 @@ struct MasLevelDev {
   float4* rin = nullptr;            // coarse: input per node (restriction)
   float4* zout = nullptr;           // coarse: output per node
   float4* rout = nullptr;           // restriction to the next coarse space
+  // Coarse levels above the first: the nodes of the level below that sum
+  // into each node (CSR over this level's nodes, members in slot order).
+  const int* member_off = nullptr;
+  const int* member = nullptr;
 };
 
 struct GalerkinDev {
@@ -96,6 +100,10 @@ struct CgArgs {
   // banks per CTA (8 or 16; 0 = not this form).  It uses the rb_ptr / rb_w /
   // rent / halo_off / halo_col layout built for blocks of dsm_f fine banks.
   int dsm_f = 0;
+  // Its pushes of fine-level z to the halos of other CTAs: per CTA (CSR)
+  // entries own slot | consumer CTA << 10 | consumer halo index << 15.
+  const int* push_off = nullptr;
+  const int* push = nullptr;
   // Optional phase trace of block 0 (null = off): [0] globaltimer and [1]
   // clock64 at entry, [2] and [3] at exit, [4] traced iterations, [5] kernel
   // form (0 streaming, 1 resident), then for each of the first kCgTraceIters
@@ -140,6 +148,8 @@ void launch_cg_resident(const CgArgs& a, int grid, cudaStream_t st);
 // for nbank0 fine banks if they form one launchable cluster (at most 16
 // CTAs), else 0.
 constexpr int kDsmCoarseBankLimit = 16;  // banks of all coarse levels together
+// Pushes of fine-level z per CTA of the cluster form: at most 2 per thread.
+constexpr int kDsmPushPerThread = 2;
 int cg_dsm_ctas(int nbank0, int f);
 void launch_cg_dsm(const CgArgs& a, int nctas, cudaStream_t st);
 

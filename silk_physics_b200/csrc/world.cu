@@ -573,7 +573,30 @@ void World::build_resident_layout(Cloth& c) {
       if (n == 0) continue;
       BlockLayout L = block_layout(S, f, BANK * f);
       if (!L.halo_full) continue;
+      // Pushes of fine-level z: each halo vertex of CTA k is stored by its
+      // owner into slot i of k's halo (entry: own slot | k << 10 | i << 15).
+      std::vector<std::vector<int>> pushes(n);
+      for (int k = 0; k < n; ++k)
+        for (int i = L.halo_off[k]; i < L.halo_off[k + 1]; ++i) {
+          const int col = L.halo_col[i];
+          int b = (int)(std::upper_bound(S.part_offsets.begin(), S.part_offsets.end(), col) -
+                        S.part_offsets.begin()) - 1;
+          const int owner = b / f;
+          const int slot = (b - owner * f) * BANK + (col - S.part_offsets[b]);
+          pushes[owner].push_back(slot | (k << 10) | ((i - L.halo_off[k]) << 15));
+        }
+      bool fits = true;
+      std::vector<int> poff(1, 0), plist;
+      for (auto& v : pushes) {
+        if ((int)v.size() > kDsmPushPerThread * BANK * f) fits = false;
+        plist.insert(plist.end(), v.begin(), v.end());
+        poff.push_back((int)plist.size());
+      }
+      if (!fits) continue;
+      if (plist.empty()) plist.push_back(0);
       upload(L);
+      d.dsm_push_off.upload(poff, st);
+      d.dsm_push.upload(plist, st);
       d.dsm_ctas = n;
       d.dsm_f = f;
       return;
@@ -669,6 +692,27 @@ void World::build_cloth_device(Cloth& c) {
     int nnode = S.galerkin[l - 1].n;
     int nnext = l < S.levels ? S.galerkin[l].n : 0;
     upload_level(S.coarse[l - 1], d.coarse[l - 1], nnode, nnext);
+    if (l >= 2) {
+      // Members of each node of this level: the slots of the level below
+      // whose connected component it is, in slot order.
+      const MasLevelPlan& below = S.coarse[l - 2];
+      std::vector<std::vector<int>> mem(nnode);
+      for (int g = 0; g < below.nbank; ++g)
+        for (int j = 0; j < BANK; ++j) {
+          const int c = below.slot_cco[(size_t)g * BANK + j];
+          if (c < 0) continue;
+          const int node = below.bank_cco_base[g] + c;
+          if (node >= 0 && node < nnode) mem[node].push_back(g * BANK + j);
+        }
+      std::vector<int> off(1, 0), list;
+      for (auto& m : mem) {
+        list.insert(list.end(), m.begin(), m.end());
+        off.push_back((int)list.size());
+      }
+      if (list.empty()) list.push_back(0);
+      d.coarse[l - 1].member_off.upload(off, st);
+      d.coarse[l - 1].member.upload(list, st);
+    }
   }
   d.gal.clear();
   d.gal.resize(S.levels);
@@ -740,6 +784,8 @@ void World::build_cloth_device(Cloth& c) {
     m.rin = rin;
     m.zout = L.zout.p;
     m.rout = L.rout.p;
+    m.member_off = L.member_off.p;
+    m.member = L.member.p;
     return m;
   };
   a.fine = lv_dev(S.fine, d.fine, nv, nullptr);
@@ -751,6 +797,8 @@ void World::build_cloth_device(Cloth& c) {
   }
   if (d.dsm_ctas > 0) {
     a.dsm_f = d.dsm_f;
+    a.push_off = d.dsm_push_off.p;
+    a.push = d.dsm_push.p;
     a.rb_ptr = d.rb_ptr.p;
     a.rb_w = d.rb_w.p;
     a.rent = d.rent.p;

@@ -83,6 +83,7 @@ struct ClothDev {
     DevBuf<float> M;
     DevBuf<__nv_bfloat16> Mb;
     DevBuf<float4> zout, rout;
+    DevBuf<int> member_off, member;  // levels above the first: nodes summed into each node
   };
   Level fine;
   std::vector<Level> coarse;
@@ -106,6 +107,7 @@ struct ClothDev {
   int res_grid = 0;           // cg_resident_grid(res_blocks)
   int dsm_ctas = 0;           // cluster form with redundant coarse levels: CTAs (0 = not used)
   int dsm_f = 0;              // its fine banks per CTA
+  DevBuf<int> dsm_push_off, dsm_push;  // its pushes of fine-level z to other CTAs' halos
   CgArgs cg;
   int cg_grid = 1;
   double bytes_per_iter_fp32 = 0.0;  // algorithmic DRAM bytes per CG iteration
