@@ -1290,6 +1290,12 @@ struct DsmShared {
   float4 zown[32 * W];                    // fine-level z of the own slots
   float4 hzs[32 * W];                     // fine-level z of the halo (pushed by the owners)
   int push[kDsmPushPerThread * 32 * W];   // this CTA's pushes (own slot, CTA, halo index)
+  // Coarse-level bookkeeping staged once per solve: per coarse bank its real
+  // slots; per node of a level above the first, first member | member count
+  // << 16 (members: rc indices of the level below).
+  int gval[kDsmCoarseBanks];
+  int mnode[kDsmCoarseBanks * BANK];
+  int mem[kDsmCoarseBanks * BANK];
 };
 
 __device__ __forceinline__ void stage_bank_full(const MasLevelDev& lv, int bank, float* slot,
@@ -1354,11 +1360,9 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
 #pragma unroll
   for (int l = 0; l < MAX_COARSE; ++l) cbo[l + 1] = cbo[l] + (l < levels ? a.coarse[l].nbank : 0);
   const int ncb = cbo[levels];
-  auto level_of = [&](int g) {
-    int l = 0;
-    while (l + 1 < levels && g >= cbo[l + 1]) ++l;
-    return l;
-  };
+  int cnode[MAX_COARSE];  // real nodes per coarse level
+#pragma unroll
+  for (int l = 0; l < MAX_COARSE; ++l) cnode[l] = l < levels ? a.coarse[l].nnode : 0;
   auto stage = [&](const MasLevelDev& lv, int bank, float* slot) {
     if (tc)
       stage_bank_frag(lv, bank, slot, lane);
@@ -1373,10 +1377,10 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
       for (int k = 0; k < N; ++k) dst[k] = s.tot[k];
     }
   };
+  // Sum of one partial slot over the CTAs: a warp sum in a fixed lane order,
+  // the same in every warp of every CTA.
   auto total = [&](int slot) {
-    double t = 0.0;
-    for (int j = 0; j < nctas; ++j) t += s.part[j][slot];
-    return t;
+    return warp_sum_d(lane < nctas ? s.part[lane][slot] : 0.0);
   };
   // Block sum of N doubles per thread into s.tot (fixed order).
   auto block_sum = [&](const double* v, int N) {
@@ -1403,9 +1407,26 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     rw = a.rb_w[fb];
     stage(a.fine, fb, s.Mf[warp]);
   }
-  for (int g = warp; g < ncb; g += W) {
-    const int l = level_of(g);
-    stage(a.coarse[l], g - cbo[l], s.Mc[g]);
+#pragma unroll
+  for (int l = 0; l < MAX_COARSE; ++l) {
+    if (l >= levels) break;
+    for (int g = cbo[l] + warp; g < cbo[l + 1]; g += W) {
+      stage(a.coarse[l], g - cbo[l], s.Mc[g]);
+      if (lane == 0) s.gval[g] = min(max(cnode[l] - (g - cbo[l]) * BANK, 0), BANK);
+    }
+    if (l >= 1) {
+      // Members of level l's nodes, after those of the levels below.
+      int base = 0;
+#pragma unroll
+      for (int k = 1; k < MAX_COARSE; ++k)
+        if (k < l) base += a.coarse[k].member_off[cnode[k]];
+      const MasLevelDev& lv = a.coarse[l];
+      for (int nd = tid; nd < cnode[l]; nd += T) {
+        const int m0 = lv.member_off[nd], m1 = lv.member_off[nd + 1];
+        s.mnode[cbo[l] * BANK + nd] = (base + m0) | ((m1 - m0) << 16);
+        for (int m = m0; m < m1; ++m) s.mem[base + m] = cbo[l - 1] * BANK + lv.member[m];
+      }
+    }
   }
   for (int i = tid; i < kDsmCoarseBanks * BANK; i += T) {
     s.rc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1548,12 +1569,13 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     tr.stamp(iter, 9);
     // Restriction chain: one warp per node of the next level sums its
     // members (at most 32, one per lane) with a warp sum.
-    for (int l = 1; l < levels; ++l) {
-      const MasLevelDev& lv = a.coarse[l];
-      for (int nd = warp; nd < lv.nnode; nd += W) {
-        const int m0 = lv.member_off[nd], cnt = lv.member_off[nd + 1] - m0;
-        float4 qv = lane < cnt ? s.rc[cbo[l - 1] * BANK + lv.member[m0 + lane]]
-                               : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int l = 1; l < MAX_COARSE; ++l) {
+      if (l >= levels) break;
+      for (int nd = warp; nd < cnode[l]; nd += W) {
+        const int e = s.mnode[cbo[l] * BANK + nd];
+        const int m0 = e & 0xffff, cnt = e >> 16;
+        float4 qv = lane < cnt ? s.rc[s.mem[m0 + lane]] : make_float4(0.f, 0.f, 0.f, 0.f);
         float qx = warp_sum(qv.x), qy = warp_sum(qv.y), qz = warp_sum(qv.z);
         if (lane == 0) s.rc[cbo[l] * BANK + nd] = make_float4(qx, qy, qz, 0.f);
       }
@@ -1569,13 +1591,7 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     for (int g0 = 0; g0 < ncb; g0 += per_round) {
       const int g = g0 + warp / split, part = warp - (warp / split) * split;
       const bool gok = g < ncb;
-      int l = 0, gl = 0;
-      bool gvalid = false;
-      if (gok) {
-        l = level_of(g);
-        gl = g - cbo[l];
-        gvalid = gl * BANK + lane < a.coarse[l].nnode;
-      }
+      const bool gvalid = gok && lane < s.gval[g];
       const int slot = g * BANK + lane;
       if (tc) {
         if (gok) {
