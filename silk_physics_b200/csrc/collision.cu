@@ -370,14 +370,27 @@ __device__ __forceinline__ float dot3(float3 a, float3 b) {
 // stick test compares squared lengths and the slide scales by
 // 1 - radius * rsqrt(|u_t|^2): one reciprocal square root instead of a square
 // root and a division.
+// The arithmetic uses fused multiply-adds (explicitly: this file is built
+// without contraction for the CCD), as does the rest of the contact
+// Gauss-Seidel (gs_accum, gs_move).
 __device__ __forceinline__ float3 coulomb_project(float3 us, float3 n, float mu) {
-  float un = dot3(us, n);
+  const float un = fmaf(us.z, n.z, fmaf(us.y, n.y, us.x * n.x));
   if (un >= 0.0f) return us;
-  float3 ut = sub3(us, sc3(un, n));
-  float ut2 = dot3(ut, ut);
-  float radius = -mu * un;
+  const float3 ut = make_float3(fmaf(-un, n.x, us.x), fmaf(-un, n.y, us.y), fmaf(-un, n.z, us.z));
+  const float ut2 = fmaf(ut.z, ut.z, fmaf(ut.y, ut.y, ut.x * ut.x));
+  const float radius = -mu * un;
   return ut2 <= radius * radius ? make_float3(0.f, 0.f, 0.f)
-                                : sc3(1.0f - radius * rsqrtf(ut2), ut);
+                                : sc3(fmaf(-radius, rsqrtf(ut2), 1.0f), ut);
+}
+
+// Contact Gauss-Seidel updates shared by its three forms (identical bits):
+// u += c x (relative position of a contact) and x += g d (a vertex moved by
+// its share g of a correction d).
+__device__ __forceinline__ float3 gs_accum(float3 u, float c, float4 x) {
+  return make_float3(fmaf(c, x.x, u.x), fmaf(c, x.y, u.y), fmaf(c, x.z, u.z));
+}
+__device__ __forceinline__ float4 gs_move(float4 x, float g, float3 d) {
+  return make_float4(fmaf(g, d.x, x.x), fmaf(g, d.y, x.y), fmaf(g, d.z, x.z), 0.f);
 }
 __device__ __forceinline__ float3 axpby3(float a, float3 x, float b, float3 y) {
   return make_float3(a * x.x + b * y.x, a * x.y + b * y.y, a * x.z + b * y.z);
@@ -1109,7 +1122,7 @@ __global__ void contact_gs_kernel(const ContactDev* contacts, const int* groups,
         if (k.gamma[s] == 0.0f) continue;
         float4 x = p[k.v[s]];
         float g = k.gamma[s];
-        p[k.v[s]] = make_float4(x.x + g * r.x, x.y + g * r.y, x.z + g * r.z, 0.f);
+        p[k.v[s]] = gs_move(x, g, make_float3(r.x, r.y, r.z));
       }
     }
     if (!bar.sync()) return;
@@ -1124,7 +1137,7 @@ __global__ void contact_gs_kernel(const ContactDev* contacts, const int* groups,
         for (int s = 0; s < 4; ++s)
           if (k.v[s] >= 0) {
             float4 x = p[k.v[s]];
-            u = add3(u, sc3(k.coef[s], make_float3(x.x, x.y, x.z)));
+            u = gs_accum(u, k.coef[s], x);
           }
         float4 o = corr[ci];
         float3 old = make_float3(o.x, o.y, o.z);
@@ -1137,7 +1150,7 @@ __global__ void contact_gs_kernel(const ContactDev* contacts, const int* groups,
           if (k.gamma[s] == 0.0f) continue;
           float4 x = p[k.v[s]];
           float g = k.gamma[s];
-          p[k.v[s]] = make_float4(x.x + g * du.x, x.y + g * du.y, x.z + g * du.z, 0.f);
+          p[k.v[s]] = gs_move(x, g, make_float3(du.x, du.y, du.z));
         }
       }
       if (!bar.sync()) return;
@@ -1230,7 +1243,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
         if (k.gamma[s] == 0.0f) continue;
         float4 x = sp[k.slot[s]];
         float g = k.gamma[s];
-        sp[k.slot[s]] = make_float4(x.x + g * r.x, x.y + g * r.y, x.z + g * r.z, 0.f);
+        sp[k.slot[s]] = gs_move(x, g, make_float3(r.x, r.y, r.z));
       }
     }
     __syncthreads();
@@ -1261,7 +1274,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
       for (int s = 0; s < 4; ++s)
         if (kc.slot[s] >= 0) {
           float4 x = sp[kc.slot[s]];
-          u = add3(u, sc3(kc.coef[s], make_float3(x.x, x.y, x.z)));
+          u = gs_accum(u, kc.coef[s], x);
         }
       float3 old = make_float3(o.x, o.y, o.z);
       float3 us = sub3(u, old);
@@ -1274,7 +1287,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
         if (kc.gamma[s] == 0.0f) continue;
         float4 x = sp[kc.slot[s]];
         float g = kc.gamma[s];
-        sp[kc.slot[s]] = make_float4(x.x + g * du.x, x.y + g * du.y, x.z + g * du.z, 0.f);
+        sp[kc.slot[s]] = gs_move(x, g, make_float3(du.x, du.y, du.z));
       }
     }
     __syncthreads();
@@ -1340,7 +1353,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
         if (k.gamma[s] == 0.0f) continue;
         float4 x = sp[k.slot[s]];
         float g = k.gamma[s];
-        sp[k.slot[s]] = make_float4(x.x + g * r.x, x.y + g * r.y, x.z + g * r.z, 0.f);
+        sp[k.slot[s]] = gs_move(x, g, make_float3(r.x, r.y, r.z));
       }
     }
     __syncthreads();
@@ -1382,7 +1395,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
       for (int s = 0; s < 4; ++s)
         if (kc.slot[s] >= 0) {
           xs[s] = sp[kc.slot[s]];
-          u = add3(u, sc3(kc.coef[s], make_float3(xs[s].x, xs[s].y, xs[s].z)));
+          u = gs_accum(u, kc.coef[s], xs[s]);
         }
       float3 old = make_float3(o.x, o.y, o.z);
       float3 us = sub3(u, old);
@@ -1395,7 +1408,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
         if (kc.gamma[s] == 0.0f) continue;
         float4 x = distinct ? xs[s] : sp[kc.slot[s]];
         float g = kc.gamma[s];
-        sp[kc.slot[s]] = make_float4(x.x + g * du.x, x.y + g * du.y, x.z + g * du.z, 0.f);
+        sp[kc.slot[s]] = gs_move(x, g, make_float3(du.x, du.y, du.z));
       }
     }
     __syncthreads();
