@@ -49,7 +49,7 @@ METRIC = "steps/s (6.4K-vertex sheet on sphere, active contact)"
 C3_WORKLOAD = "c3_sheet316_on_icosphere_r0.6_first_contact"
 STATE = ROOT / "oracle" / "reference_state_c2_step27.npz"
 MODEL = ROOT / "silk_physics_b200" / "models" / "warm_start.npy"
-TRAFFIC = ROOT / "profiles" / "cg_resident_c2_contact.json"
+TRAFFIC = ROOT / "profiles" / "cg_cluster_c2_contact.json"
 SCENES = ROOT / "tests" / "golden" / "reference_scenes.npz"
 C3_START_STEPS = 8  # free-fall steps before the drape's first contact step
 
@@ -203,7 +203,7 @@ def peaks() -> dict:
 
 def traffic_per_launch():
     """DRAM bytes per CG launch of a contact-regime solve, from the committed
-    ncu summary (profiles/cg_resident_c2_contact.json), or None."""
+    ncu summary (profiles/cg_cluster_c2_contact.json), or None."""
     if not TRAFFIC.exists():
         return None
     d = json.loads(TRAFFIC.read_text())
@@ -391,7 +391,7 @@ def run_ours(args) -> None:
     w.profile(reset=True)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
-    launches = admm = cg = solves = contacts = 0
+    launches = admm = cg = solves = contacts = cluster_solves = 0
     per_step_admm = []
     if world_size > 1:
         torch.distributed.barrier()
@@ -410,6 +410,7 @@ def run_ours(args) -> None:
             per_step_admm.append(st.admm_iterations)
             cg += st.cg_iterations
             solves += st.cg_solves
+            cluster_solves += st.cg_cluster_solves
             contacts = st.contacts
         torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in ev]
@@ -457,7 +458,9 @@ def run_ours(args) -> None:
     bytes_per_launch = prof["cg_algorithmic_bytes"] / max(prof["cg_launches"], 1)
     achieved = bytes_per_launch / (cg_launch_ms / 1e3) / 1e9 if cg_launch_ms > 0 else 0.0
     tr = traffic_per_launch()
-    roofline = {"bound": "hbm", "kernel": "cg_resident_cluster_kernel (persistent MAS-PCG)",
+    kernel = ("cg_dsm_cluster_kernel (persistent MAS-PCG, cluster form)"
+              if cluster_solves == solves else "cg_resident / cg_kernel (persistent MAS-PCG)")
+    roofline = {"bound": "hbm", "kernel": kernel,
                 "achieved": round(achieved, 2), "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved / pk["hbm_gbs"], 5), "peak_source": pk["source"],
                 "traffic": tr["bytes"] if tr else None,

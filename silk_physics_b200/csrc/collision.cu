@@ -1134,11 +1134,11 @@ __global__ void contact_gs_kernel(const ContactDev* contacts, const int* groups,
         int ci = groups[q];
         const ContactDev& k = contacts[ci];
         float3 u = k.affine;
-        for (int s = 0; s < 4; ++s)
-          if (k.v[s] >= 0) {
-            float4 x = p[k.v[s]];
-            u = gs_accum(u, k.coef[s], x);
-          }
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          const float4 x = k.v[s] >= 0 ? p[k.v[s]] : make_float4(0.f, 0.f, 0.f, 0.f);
+          u = gs_accum(u, k.coef[s], x);
+        }
         float4 o = corr[ci];
         float3 old = make_float3(o.x, o.y, o.z);
         float3 us = sub3(u, old);
@@ -1271,11 +1271,11 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
     if (ph + 1 < phases) fetch((ph + 1) % ncolors, qn, k, on);
     if (cur >= 0) {
       float3 u = kc.affine;
-      for (int s = 0; s < 4; ++s)
-        if (kc.slot[s] >= 0) {
-          float4 x = sp[kc.slot[s]];
-          u = gs_accum(u, kc.coef[s], x);
-        }
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const float4 x = kc.slot[s] >= 0 ? sp[kc.slot[s]] : make_float4(0.f, 0.f, 0.f, 0.f);
+        u = gs_accum(u, kc.coef[s], x);
+      }
       float3 old = make_float3(o.x, o.y, o.z);
       float3 us = sub3(u, old);
       float3 unew = coulomb_project(us, kc.normal, kc.friction);
@@ -1322,7 +1322,9 @@ __host__ __device__ inline GsPipeLayout gs_pipe_layout(int nslots, int total, in
                                                        int threads) {
   GsPipeLayout L;
   L.sp = 0;
-  L.sc = align16(L.sp + (size_t)nslots * sizeof(float4));
+  // Two extra position slots: nslots reads as zero (kinematic vertices),
+  // nslots + 1 takes the stores of zero-share vertices.
+  L.sc = align16(L.sp + (size_t)(nslots + 2) * sizeof(float4));
   L.go = align16(L.sc + (size_t)total * sizeof(float4));
   L.stage = align16(L.go + (size_t)(ncolors + 1) * sizeof(int));
   L.bytes = L.stage + (size_t)kGsStages * threads * sizeof(GsContact);
@@ -1340,6 +1342,8 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
   GsContact* stage = reinterpret_cast<GsContact*>(gs_raw + L.stage);
   const int t = threadIdx.x, nt = blockDim.x;
   for (int i = t; i < nslots; i += nt) sp[i] = p[vlist[i]];
+  if (t < 2) sp[nslots + t] = make_float4(0.f, 0.f, 0.f, 0.f);
+  const int zslot = nslots, tslot = nslots + 1;
   for (int q = t; q < total; q += nt) sc[q] = corr[cc[q].ci & 0x7fffffff];
   for (int c = t; c <= ncolors; c += nt) sgo[c] = group_off[c];
   __syncthreads();
@@ -1390,13 +1394,14 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
     if (active) {
       const GsContact kc = stage[(size_t)(ph & (kGsStages - 1)) * nt + t];
       const float4 o = sc[cur];
+      // All four positions read at once, without branches (a kinematic
+      // vertex reads the zero slot: u gains c * 0).
       float3 u = kc.affine;
       float4 xs[4];
-      for (int s = 0; s < 4; ++s)
-        if (kc.slot[s] >= 0) {
-          xs[s] = sp[kc.slot[s]];
-          u = gs_accum(u, kc.coef[s], xs[s]);
-        }
+#pragma unroll
+      for (int s = 0; s < 4; ++s) xs[s] = sp[kc.slot[s] >= 0 ? kc.slot[s] : zslot];
+#pragma unroll
+      for (int s = 0; s < 4; ++s) u = gs_accum(u, kc.coef[s], xs[s]);
       float3 old = make_float3(o.x, o.y, o.z);
       float3 us = sub3(u, old);
       float3 unew = coulomb_project(us, kc.normal, kc.friction);
@@ -1404,11 +1409,12 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
       float3 nc = add3(old, du);
       sc[cur] = make_float4(nc.x, nc.y, nc.z, 0.f);
       const bool distinct = kc.ci < 0;
+      // Zero-share vertices (kinematic, pinned) store into the scratch slot.
+#pragma unroll
       for (int s = 0; s < 4; ++s) {
-        if (kc.gamma[s] == 0.0f) continue;
-        float4 x = distinct ? xs[s] : sp[kc.slot[s]];
-        float g = kc.gamma[s];
-        sp[kc.slot[s]] = gs_move(x, g, make_float3(du.x, du.y, du.z));
+        const int sl = kc.gamma[s] != 0.0f && kc.slot[s] >= 0 ? kc.slot[s] : tslot;
+        const float4 x = distinct ? xs[s] : sp[sl];
+        sp[sl] = gs_move(x, kc.gamma[s], du);
       }
     }
     __syncthreads();
