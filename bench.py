@@ -355,9 +355,13 @@ def reference_scenes(N, steps_cloth_ball: int):
             path = H.write_scene(Path(tmp) / name, name, text, meshes)
             g = json.loads(text)["global"]
             _, wall = H.run(path, steps=steps, bench=True, log=None)
-            n = len(wall)
-            out[name] = {"steps": n, "dt": g["dt"], "value": round(n / (sum(wall) / 1e3), 3),
-                         "unit": "steps/s", "ms_per_step": round(sum(wall) / n, 2),
+            # The first step of a fresh world also builds its solver layout
+            # (partition, assembly, MAS plans); the rate is over the others.
+            n = len(wall) - 1
+            rest = sum(wall[1:])
+            out[name] = {"steps_timed": n, "dt": g["dt"], "value": round(n / (rest / 1e3), 3),
+                         "unit": "steps/s", "ms_per_step": round(rest / n, 2),
+                         "first_step_ms_with_setup": round(wall[0], 1),
                          "max_inner_iteration": g["max_inner_iteration"],
                          "cg_tolerance": "adaptive (reference default)"}
     out["note"] = ("README.md:7 of the reference: 'maintain 40 FPS' on a 6K cloth mesh with "
