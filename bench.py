@@ -297,6 +297,8 @@ def replay_variant(N, torch, stream, flush, V, F, SV, SF, x0, v0, cg_rel_tol, bf
             "cg_kernel_ms_per_step": round(prof["cg_time_ms"] / reps, 2),
             "contact_gs_ms_per_step": round(prof["contact_gs_ms"] / reps, 2),
             "ccd_host_ms_per_step": round(prof["ccd_host_ms"] / reps, 2),
+            "ccd_refit_host_ms_per_step": round(prof["ccd_refit_host_ms"] / reps, 2),
+            "ccd_candidates_host_ms_per_step": round(prof["ccd_candidates_host_ms"] / reps, 2),
             "contacts": s.contacts, "replays_identical": len(keys) == 1,
             "learned_starts_taken": s.learned_starts,
             "extrapolated_starts_taken": s.extrapolated_starts}

@@ -141,7 +141,8 @@ typedef struct {
   double dcd_host_ms;        /* host wall time of DCD + contact rebuild */
   double step_host_ms;       /* host wall time of solver_step */
   double contact_gs_ms;      /* events: contact Gauss-Seidel (part of admm_other_ms) */
-  double reserved[2];
+  double ccd_refit_host_ms;  /* part of ccd_host_ms: collider refit and tree builds */
+  double ccd_candidates_host_ms; /* part of ccd_host_ms: broadphase candidate gathering */
 } silk_profile;
 
 /* Statistics of the last solver_step. */

@@ -26,6 +26,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -2162,7 +2163,11 @@ float CollisionSystem::min_toi(float ts, float max_time, float ms, int* nq, int*
   *nq = 0;
   *nh = 0;
   if (max_time == 0.0f) return 0.0f;
+  const auto t_gather = std::chrono::steady_clock::now();
   int n = gather_candidates(I, st);
+  last_gather_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_gather)
+          .count();
   *nq = n;
   if (n == 0) return max_time;
   // Scene-wide magnitude for the numerical filter (find_collision.cu:157-172).

@@ -42,6 +42,7 @@ class CollisionSystem {
   int color_count() const;
   const int* active_dof_device() const;
   int last_candidates() const;
+  double last_gather_ms = 0.0;  // host wall time of the last candidate gathering
 
   // Inspection.
   int debug_candidates(int* out, int64_t cap);

@@ -1399,8 +1399,10 @@ silk_status World::solver_step() {
         NvtxRange ccd_range("refit + CCD");
         auto t0 = clk::now();
         coll_->refit(x.p, outer.p);
+        prof.ccd_refit_host_ms += ms_since(t0);
         int nq = 0, nh = 0;
         toi = coll_->min_toi(1.0f - remaining, remaining, ms, &nq, &nh);
+        prof.ccd_candidates_host_ms += coll_->last_gather_ms;
         stats.ccd_queries += nq;
         stats.ccd_hits += nh;
         prof.ccd_host_ms += ms_since(t0);

@@ -88,7 +88,7 @@ class _ProfileC(C.Structure):
                 ("admm_other_ms", C.c_double), ("admm_host_ms", C.c_double),
                 ("ccd_host_ms", C.c_double), ("dcd_host_ms", C.c_double),
                 ("step_host_ms", C.c_double), ("contact_gs_ms", C.c_double),
-                ("reserved", C.c_double * 2)]
+                ("ccd_refit_host_ms", C.c_double), ("ccd_candidates_host_ms", C.c_double)]
 
 
 class _StepStatsC(C.Structure):
@@ -438,7 +438,7 @@ class World:
     def profile(self, reset: bool = False) -> dict:
         p = _ProfileC()
         lib.silk_get_profile(self._w, C.byref(p), int(reset))
-        return {n: getattr(p, n) for n, _ in _ProfileC._fields_ if n != "reserved"}
+        return {n: getattr(p, n) for n, _ in _ProfileC._fields_}
 
     def set_cloth_state(self, handle: int, position, velocity=None) -> Result:
         """Restart a cloth from stored positions (and velocities; None = at
