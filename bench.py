@@ -299,6 +299,10 @@ def replay_variant(N, torch, stream, flush, V, F, SV, SF, x0, v0, cg_rel_tol, bf
             "ccd_host_ms_per_step": round(prof["ccd_host_ms"] / reps, 2),
             "ccd_refit_host_ms_per_step": round(prof["ccd_refit_host_ms"] / reps, 2),
             "ccd_candidates_host_ms_per_step": round(prof["ccd_candidates_host_ms"] / reps, 2),
+            "ccd_first_pass_ms_per_step": round(prof["ccd_first_pass_ms"] / reps, 2),
+            "ccd_second_pass_ms_per_step": round(prof["ccd_second_pass_ms"] / reps, 2),
+            "ccd_second_pass_queries_per_step": round(prof["ccd_second_pass_queries"] / reps, 1),
+            "ccd_calls_per_step": round(prof["ccd_calls"] / reps, 1),
             "contacts": s.contacts, "replays_identical": len(keys) == 1,
             "learned_starts_taken": s.learned_starts,
             "extrapolated_starts_taken": s.extrapolated_starts}

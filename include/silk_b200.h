@@ -127,7 +127,9 @@ typedef struct {
 } silk_solver_options;
 
 /* CUDA-event timing of the persistent CG kernel over the steps since the
- * last reset (silk_solver_options.profile = 1).  algorithmic_bytes counts
+ * last reset (silk_solver_options.profile = 1); the struct grew by the four
+ * narrowphase fields at its end, so callers compiled against a shorter
+ * silk_profile must be rebuilt.  algorithmic_bytes counts
  * compulsory DRAM traffic per CG iteration: matrix entries, MAS bank
  * inverses and each vector read or written once. */
 typedef struct {
@@ -143,6 +145,10 @@ typedef struct {
   double contact_gs_ms;      /* events: contact Gauss-Seidel (part of admm_other_ms) */
   double ccd_refit_host_ms;  /* part of ccd_host_ms: collider refit and tree builds */
   double ccd_candidates_host_ms; /* part of ccd_host_ms: broadphase candidate gathering */
+  double ccd_first_pass_ms;  /* events: narrowphase first pass (per-thread storage) */
+  double ccd_second_pass_ms; /* events: narrowphase second pass (searches that outgrew it) */
+  double ccd_second_pass_queries; /* queries that ran the second pass */
+  double ccd_calls;          /* narrowphase calls (one per outer iteration) */
 } silk_profile;
 
 /* Statistics of the last solver_step. */

@@ -1514,6 +1514,14 @@ struct CollisionImpl {
   DevBuf<int> ccd_overflow;
   DevBuf<IBox> ccd_spill;
   // Contacts.
+  cudaEvent_t ccd_ev[4] = {nullptr, nullptr, nullptr, nullptr};  // narrowphase pass timing
+  CollisionImpl() = default;
+  CollisionImpl(const CollisionImpl&) = delete;
+  CollisionImpl& operator=(const CollisionImpl&) = delete;
+  ~CollisionImpl() {
+    for (cudaEvent_t e : ccd_ev)
+      if (e) cudaEventDestroy(e);
+  }
   std::set<Key> keys;
   std::vector<Key> key_list;
   std::vector<uint64_t> prio_host;
@@ -2199,14 +2207,21 @@ float CollisionSystem::min_toi(float ts, float max_time, float ms, int* nq, int*
     return n;
   }();
   auto grid_for = [&](int m) { return std::max(1, std::min(div_up(m, kCollThreads), 8 * sms)); };
+  if (!I.ccd_ev[0]) {
+    for (auto& e : I.ccd_ev) CUDA_CHECK(cudaEventCreate(&e));
+  }
   CcdSpill first{nullptr, 0, nullptr, I.ccd_overflow.p, I.ccd_counts.p + 2};
+  CUDA_CHECK(cudaEventRecord(I.ccd_ev[0], st));
   ccd_kernel<<<grid_for(n), kCollThreads, 0, st>>>(
       I.table_d.p, I.cand.p, n, ts, max_time, ms, vf, ee, local_tol, I.min_bits.p,
       I.ccd_counts.p, first, I.ccd_counts.p + 3, prune ? 1 : 0);
   SILK_LAUNCHED();
+  CUDA_CHECK(cudaEventRecord(I.ccd_ev[1], st));
   int counts[3];
   CUDA_CHECK(cudaMemcpyAsync(counts, I.ccd_counts.p, sizeof(counts), cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaStreamSynchronize(st));
+  last_second_pass_queries = counts[2];
+  CUDA_CHECK(cudaEventRecord(I.ccd_ev[2], st));
   // Second pass for the searches that outgrew the per-thread array.
   const int cap = kCcdMaxIter + 2;
   int chunk_id = 0;
@@ -2221,10 +2236,18 @@ float CollisionSystem::min_toi(float ts, float max_time, float ms, int* nq, int*
         I.ccd_counts.p, second, next, prune ? 1 : 0);
     SILK_LAUNCHED();
   }
+  CUDA_CHECK(cudaEventRecord(I.ccd_ev[3], st));
   unsigned bits = 0;
   CUDA_CHECK(cudaMemcpyAsync(&bits, I.min_bits.p, 4, cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaMemcpyAsync(counts, I.ccd_counts.p, sizeof(counts), cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaStreamSynchronize(st));
+  {
+    float a = 0.f, b = 0.f;
+    CUDA_CHECK(cudaEventElapsedTime(&a, I.ccd_ev[0], I.ccd_ev[1]));
+    CUDA_CHECK(cudaEventElapsedTime(&b, I.ccd_ev[2], I.ccd_ev[3]));
+    last_first_pass_ms = a;
+    last_second_pass_ms = b;
+  }
   if (counts[1] > 0) throw CudaError("CCD search storage overflow");
   *nh = counts[0];
   float local;

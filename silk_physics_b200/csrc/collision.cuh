@@ -43,6 +43,10 @@ class CollisionSystem {
   const int* active_dof_device() const;
   int last_candidates() const;
   double last_gather_ms = 0.0;  // host wall time of the last candidate gathering
+  // Narrowphase of the last min_toi (CUDA events): first and second pass,
+  // queries that ran the second pass.
+  double last_first_pass_ms = 0.0, last_second_pass_ms = 0.0;
+  int last_second_pass_queries = 0;
 
   // Inspection.
   int debug_candidates(int* out, int64_t cap);

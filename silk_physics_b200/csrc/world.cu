@@ -1403,6 +1403,10 @@ silk_status World::solver_step() {
         int nq = 0, nh = 0;
         toi = coll_->min_toi(1.0f - remaining, remaining, ms, &nq, &nh);
         prof.ccd_candidates_host_ms += coll_->last_gather_ms;
+        prof.ccd_first_pass_ms += coll_->last_first_pass_ms;
+        prof.ccd_second_pass_ms += coll_->last_second_pass_ms;
+        prof.ccd_second_pass_queries += coll_->last_second_pass_queries;
+        prof.ccd_calls += 1;
         stats.ccd_queries += nq;
         stats.ccd_hits += nh;
         prof.ccd_host_ms += ms_since(t0);

@@ -88,7 +88,9 @@ class _ProfileC(C.Structure):
                 ("admm_other_ms", C.c_double), ("admm_host_ms", C.c_double),
                 ("ccd_host_ms", C.c_double), ("dcd_host_ms", C.c_double),
                 ("step_host_ms", C.c_double), ("contact_gs_ms", C.c_double),
-                ("ccd_refit_host_ms", C.c_double), ("ccd_candidates_host_ms", C.c_double)]
+                ("ccd_refit_host_ms", C.c_double), ("ccd_candidates_host_ms", C.c_double),
+                ("ccd_first_pass_ms", C.c_double), ("ccd_second_pass_ms", C.c_double),
+                ("ccd_second_pass_queries", C.c_double), ("ccd_calls", C.c_double)]
 
 
 class _StepStatsC(C.Structure):
