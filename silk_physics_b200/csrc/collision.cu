@@ -47,7 +47,6 @@ constexpr int kCcdMaxIter = 4096;      // main_loop.cuh:24
 constexpr float kCcdTolerance = 1e-6f; // main_loop.cuh:23
 constexpr int kGsSweeps = 10;          // contact_constraints.cuh:89
 constexpr int kCcdStack = 96;
-constexpr int kCcdSpillChunk = 512;  // overflowed queries per second pass
 
 // std::min / std::max semantics.
 __device__ __forceinline__ float smin(float a, float b) { return (b < a) ? b : a; }
@@ -675,11 +674,70 @@ __device__ float clamp_div(float a, float b, float mx) {
 // queries that outgrow it are re-run with a global-memory array of
 // max_iter + 2 entries, the most a search can hold (each evaluation pops one
 // box and pushes at most two, and pushes stop after max_iter evaluations).
+// Pending boxes of a search, in the reference's processing order: smallest
+// t.lower first and, for equal t.lower, the most recently pushed (its
+// std::map of per-t.lower stacks, interval_root_finder.cpp:430-500).  Two
+// stores of that one total order: a sorted array (top = next; an insertion
+// shifts the boxes with smaller t.lower, cheap while the search is shallow)
+// and a binary heap keyed on (t.lower ascending, push sequence descending),
+// O(log n) per operation for deep searches.
 struct DfsStack {
   IBox local[kCcdStack];
   IBox* e;
+  int* q = nullptr;  // heap: push sequence of each box
   int cap;
   int n;
+  bool heap = false;
+  int seq = 0;
+  __device__ __forceinline__ bool before(const IBox& a, int qa, const IBox& b, int qb) const {
+    return a.t0 < b.t0 || (a.t0 == b.t0 && qa > qb);
+  }
+  __device__ bool push(const IBox& b) {
+    if (n >= cap) return false;
+    if (heap) {
+      const int sq = seq++;
+      int i = n++;
+      while (i > 0) {
+        const int p = (i - 1) >> 1;
+        if (!before(b, sq, e[p], q[p])) break;
+        e[i] = e[p];
+        q[i] = q[p];
+        i = p;
+      }
+      e[i] = b;
+      q[i] = sq;
+      return true;
+    }
+    int pos = n;
+    while (pos > 0 && e[pos - 1].t0 < b.t0) --pos;
+    for (int k = n; k > pos; --k) e[k] = e[k - 1];
+    e[pos] = b;
+    ++n;
+    return true;
+  }
+  __device__ IBox pop() {
+    if (!heap) return e[--n];
+    const IBox top = e[0];
+    --n;
+    if (n > 0) {
+      const IBox last = e[n];
+      const int lq = q[n];
+      int i = 0;
+      for (;;) {
+        const int l = 2 * i + 1;
+        if (l >= n) break;
+        int c = l;
+        if (l + 1 < n && before(e[l + 1], q[l + 1], e[l], q[l])) c = l + 1;
+        if (!before(e[c], q[c], last, lq)) break;
+        e[i] = e[c];
+        q[i] = q[c];
+        i = c;
+      }
+      e[i] = last;
+      q[i] = lq;
+    }
+    return top;
+  }
 };
 
 // Returns 0 = no root, 1 = root, 2 = storage overflow, 3 = pruned.
@@ -717,22 +775,12 @@ __device__ int root_finder(bool vf, const float3* Pt, const float* tol,
   IBox cur{0.0f, max_time, 0.0f, 1.0f, 0.0f, 1.0f};
   bool has_cur = true;
   st.n = 0;
+  st.seq = 0;
   int iter = 0;
-  // Pending boxes are ordered so that the top is the next to process: the
-  // smallest t.lower first and, for equal t.lower, the most recently pushed
-  // (the std::map of per-t.lower stacks of the reference).
-  auto push = [&](const IBox& b) -> bool {
-    if (st.n >= st.cap) return false;
-    int pos = st.n;
-    while (pos > 0 && st.e[pos - 1].t0 < b.t0) --pos;
-    for (int k = st.n; k > pos; --k) st.e[k] = st.e[k - 1];
-    st.e[pos] = b;
-    ++st.n;
-    return true;
-  };
+  auto push = [&](const IBox& b) -> bool { return st.push(b); };
   float best = __int_as_float(0x7f800000);
   while (has_cur || st.n > 0) {
-    if (!has_cur) cur = st.e[--st.n];
+    if (!has_cur) cur = st.pop();
     has_cur = false;
     if (best_bits) {
       if ((iter & 15) == 0) best = __uint_as_float(*(volatile const unsigned*)best_bits);
@@ -888,10 +936,19 @@ struct CcdSpill {
   const int* list;    // second pass: query indices
   int* overflow;      // first pass: queries to re-run
   int* n_overflow;
+  int smem_heap = 0;  // second pass: one query per block, a heap of spill_cap
+                      // boxes in the block's shared memory (spill unused)
 };
 
+extern __shared__ __align__(16) unsigned char ccd_heap_smem[];
+
 __device__ __forceinline__ void bind_stack(DfsStack& st, const CcdSpill& sp, int i) {
-  if (sp.spill) {
+  if (sp.smem_heap) {
+    st.e = reinterpret_cast<IBox*>(ccd_heap_smem);
+    st.q = reinterpret_cast<int*>(ccd_heap_smem + (size_t)sp.spill_cap * sizeof(IBox));
+    st.cap = sp.spill_cap;
+    st.heap = true;
+  } else if (sp.spill) {
     st.e = sp.spill + (size_t)i * sp.spill_cap;
     st.cap = sp.spill_cap;
   } else {
@@ -962,11 +1019,30 @@ __global__ void __launch_bounds__(kCollThreads) ccd_kernel(
   }
 }
 
+// Second pass of the searches that outgrew the per-thread storage: one
+// query per block (block q takes list entry q), searched by thread 0 with
+// its pending boxes in a heap in the block's shared memory.
+__global__ void __launch_bounds__(32) ccd_heap_kernel(
+    const ObjDev* objs, const int4* cand, int n, float ts, float interval, float ms,
+    float3 vf_err, float3 ee_err, float local_tol, unsigned* min_bits, int* counts,
+    CcdSpill sp, int prune) {
+  if (threadIdx.x != 0 || (int)blockIdx.x >= n) return;
+  ccd_one(objs, cand, blockIdx.x, ts, interval, ms, vf_err, ee_err, local_tol, min_bits, counts,
+          sp, prune);
+}
+
+constexpr size_t kCcdHeapSmemMax = 200 * 1024;  // heap second pass: up to ~7,300 boxes
+
+size_t ccd_heap_smem_bytes(int cap) {
+  return (size_t)cap * (sizeof(IBox) + sizeof(int));
+}
+
 __global__ void ccd_batch_kernel(bool vf, const float* x, int n, float3 err,
                                  const float* ms, float tol, int max_iter,
                                  float max_time, int* hit, float* toi, float* tup,
                                  int* n_bad, CcdSpill sp) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int i = sp.smem_heap ? (threadIdx.x == 0 ? (int)blockIdx.x : n)
+                       : blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int q = sp.list ? sp.list[i] : i;
   float3 Pt[8];
@@ -1512,7 +1588,6 @@ struct CollisionImpl {
   DevBuf<unsigned> min_bits;
   DevBuf<int> ccd_counts;  // [hits, storage overflows, first-pass spills]
   DevBuf<int> ccd_overflow;
-  DevBuf<IBox> ccd_spill;
   // Contacts.
   cudaEvent_t ccd_ev[4] = {nullptr, nullptr, nullptr, nullptr};  // narrowphase pass timing
   CollisionImpl() = default;
@@ -2196,9 +2271,8 @@ float CollisionSystem::min_toi(float ts, float max_time, float ms, int* nq, int*
   float one = max_time / max_time;
   std::memcpy(&one_bits, &one, 4);
   CUDA_CHECK(cudaMemcpyAsync(I.min_bits.p, &one_bits, 4, cudaMemcpyHostToDevice, st));
-  // counts: [hits, storage overflows, first-pass spills, work counters...]
-  const int max_chunks = 64;
-  CUDA_CHECK(cudaMemsetAsync(I.ccd_counts.p, 0, (4 + max_chunks) * sizeof(int), st));
+  // counts: [hits, storage overflows, first-pass spills, work counter]
+  CUDA_CHECK(cudaMemsetAsync(I.ccd_counts.p, 0, 4 * sizeof(int), st));
   if ((int)I.ccd_overflow.n < n) I.ccd_overflow.alloc(n + n / 4);
   static const int sms = [] {
     int dev = 0, n = 0;
@@ -2222,18 +2296,21 @@ float CollisionSystem::min_toi(float ts, float max_time, float ms, int* nq, int*
   CUDA_CHECK(cudaStreamSynchronize(st));
   last_second_pass_queries = counts[2];
   CUDA_CHECK(cudaEventRecord(I.ccd_ev[2], st));
-  // Second pass for the searches that outgrew the per-thread array.
-  const int cap = kCcdMaxIter + 2;
-  int chunk_id = 0;
-  for (int start = 0; start < counts[2]; start += kCcdSpillChunk, ++chunk_id) {
-    int m = std::min(kCcdSpillChunk, counts[2] - start);
-    if (I.ccd_spill.n < (size_t)kCcdSpillChunk * cap) I.ccd_spill.alloc((size_t)kCcdSpillChunk * cap);
-    int* next = I.ccd_counts.p + 4 + (chunk_id % max_chunks);
-    if (chunk_id >= max_chunks) CUDA_CHECK(cudaMemsetAsync(next, 0, sizeof(int), st));
-    CcdSpill second{I.ccd_spill.p, cap, I.ccd_overflow.p + start, nullptr, nullptr};
-    ccd_kernel<<<grid_for(m), kCollThreads, 0, st>>>(
-        I.table_d.p, I.cand.p, m, ts, max_time, ms, vf, ee, local_tol, I.min_bits.p,
-        I.ccd_counts.p, second, next, prune ? 1 : 0);
+  // Second pass for the searches that outgrew the per-thread array: one
+  // query per block, its pending boxes in a heap in shared memory.
+  if (counts[2] > 0) {
+    const int cap = kCcdMaxIter + 2;
+    const size_t smem = ccd_heap_smem_bytes(cap);
+    static const bool attr = [smem] {
+      CUDA_CHECK(cudaFuncSetAttribute(ccd_heap_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      return true;
+    }();
+    (void)attr;
+    CcdSpill second{nullptr, cap, I.ccd_overflow.p, nullptr, nullptr, 1};
+    ccd_heap_kernel<<<counts[2], 32, smem, st>>>(I.table_d.p, I.cand.p, counts[2], ts, max_time,
+                                                 ms, vf, ee, local_tol, I.min_bits.p,
+                                                 I.ccd_counts.p, second, prune ? 1 : 0);
     SILK_LAUNCHED();
   }
   CUDA_CHECK(cudaEventRecord(I.ccd_ev[3], st));
@@ -2352,16 +2429,34 @@ void ccd_batch_host(bool vf, const float* x, int64_t n, const float* err3,
     // Second pass with max_iter + 2 pending boxes per search (unbounded
     // searches, max_iter <= 0, get 65536).
     int cap = max_iter > 0 ? max_iter + 2 : 65536;
-    int chunk = std::max(1, std::min(h[0], (int)((256ll << 20) / ((long long)cap * sizeof(IBox)))));
-    DevBuf<IBox> spill;
-    spill.alloc((size_t)chunk * cap);
-    for (int start = 0; start < h[0]; start += chunk) {
-      int m = std::min(chunk, h[0] - start);
-      CcdSpill second{spill.p, cap, over.p + start, nullptr, nullptr};
-      ccd_batch_kernel<<<div_up(m, kCollThreads), kCollThreads>>>(
-          vf, xd.p, m, e3, msd.p, tol, max_iter, max_time, hitd.p, toid.p, tupd.p,
-          counts.p + 1, second);
+    const size_t heap_smem = ccd_heap_smem_bytes(cap);
+    if (heap_smem <= kCcdHeapSmemMax) {
+      // One query per block, its pending boxes in a heap in shared memory.
+      static const bool attr = [] {
+        CUDA_CHECK(cudaFuncSetAttribute(ccd_batch_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kCcdHeapSmemMax));
+        return true;
+      }();
+      (void)attr;
+      CcdSpill second{nullptr, cap, over.p, nullptr, nullptr, 1};
+      ccd_batch_kernel<<<h[0], 32, heap_smem>>>(vf, xd.p, h[0], e3, msd.p, tol, max_iter,
+                                                max_time, hitd.p, toid.p, tupd.p, counts.p + 1,
+                                                second);
       SILK_LAUNCHED();
+    } else {
+      int chunk =
+          std::max(1, std::min(h[0], (int)((256ll << 20) / ((long long)cap * sizeof(IBox)))));
+      DevBuf<IBox> spill;
+      spill.alloc((size_t)chunk * cap);
+      for (int start = 0; start < h[0]; start += chunk) {
+        int m = std::min(chunk, h[0] - start);
+        CcdSpill second{spill.p, cap, over.p + start, nullptr, nullptr};
+        ccd_batch_kernel<<<div_up(m, kCollThreads), kCollThreads>>>(
+            vf, xd.p, m, e3, msd.p, tol, max_iter, max_time, hitd.p, toid.p, tupd.p,
+            counts.p + 1, second);
+        SILK_LAUNCHED();
+      }
     }
     CUDA_CHECK(cudaMemcpy(h, counts.p, sizeof(h), cudaMemcpyDeviceToHost));
     if (h[1] > 0) throw CudaError("CCD search storage overflow");
