@@ -92,8 +92,12 @@ typedef struct {
                                  CTAs of 8 or 16 fine banks, else the resident
                                  form where it fits, else streaming;
                                  2: resident where it fits, else streaming;
-                                 1: streaming always (applies when the solver
-                                 layout is built; changing it rebuilds it) */
+                                 1: streaming always;
+                                 3: as 0, the cluster form reading its matrix
+                                 rows from global memory in every SpMV instead
+                                 of holding them in tensor memory (applies
+                                 when the solver layout is built; changing it
+                                 rebuilds it) */
   int32_t learned_warm_start; /* 1: offer the loaded first-solve model's
                                  prediction as the start of each outer
                                  iteration's first CG solve and, when an

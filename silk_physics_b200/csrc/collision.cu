@@ -1373,22 +1373,55 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
   for (int i = t; i < nslots; i += blockDim.x) p[vlist[i]] = sp[i];
 }
 
-// Pipelined single-block form: the contacts of the next kGsStages - 1 colour
-// phases stream into shared memory with cp.async while the current phase is
-// processed, and the corrections and colour offsets stay in shared memory for
-// the whole call, so a phase never waits on a global load.  Same per-contact
-// operations as contact_gs_kernel.
+// Pipelined single-block form: the contact records of the next kGsStages - 1
+// colour phases arrive in shared memory by bulk copies (one per colour: its
+// records are contiguous in colour order) while the current phase is
+// processed, each completing on its stage's mbarrier; the corrections and
+// colour offsets stay in shared memory for the whole call, so a phase never
+// waits on a global load.  Same per-contact operations as contact_gs_kernel.
 constexpr int kGsStages = 4;  // a power of two (stage = phase & (kGsStages - 1))
 static_assert((kGsStages & (kGsStages - 1)) == 0, "power of two");
+static_assert(sizeof(GsContact) % 16 == 0, "bulk copies move whole 16-byte units");
+constexpr int kGsWaitSpins = 1 << 20;  // mbarrier polls before a phase gives up
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
-  unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gmem_src));
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for phase `parity` of an mbarrier: false if it did not complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  for (int spin = 0; spin < kGsWaitSpins; ++spin)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// Bulk copy global -> this CTA's shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes,
+                                              uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+      ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
 }
 
 struct GsPipeLayout {
@@ -1410,8 +1443,10 @@ __host__ __device__ inline GsPipeLayout gs_pipe_layout(int nslots, int total, in
 
 __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
     const GsContact* __restrict__ cc, const int* __restrict__ group_off, int ncolors, int total,
-    float4* __restrict__ corr, const int* __restrict__ vlist, int nslots, float4* __restrict__ p) {
+    float4* __restrict__ corr, const int* __restrict__ vlist, int nslots, float4* __restrict__ p,
+    int* __restrict__ fail) {
   extern __shared__ __align__(16) unsigned char gs_raw[];
+  __shared__ __align__(8) uint64_t bars[kGsStages];
   const GsPipeLayout L = gs_pipe_layout(nslots, total, ncolors, blockDim.x);
   float4* sp = reinterpret_cast<float4*>(gs_raw + L.sp);
   float4* sc = reinterpret_cast<float4*>(gs_raw + L.sc);
@@ -1440,19 +1475,29 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
     __syncthreads();
   }
   const int phases = kGsSweeps * ncolors;
-  // Stage ph % kGsStages of this thread receives the contact of phase ph
-  // (colour col_of_ph, tracked incrementally: no division per phase).
+  // The copies are issued by the block's last thread: its warp holds no
+  // contact in most colours, so the issue stays off the contacts' path.
+  const int producer = nt - 1;
+  if (t == producer) {
+    for (int s = 0; s < kGsStages; ++s) mbar_init(&bars[s], 1);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  }
+  __syncthreads();
+  // Copy the records of phase ph's colour into stage ph % kGsStages.  A
+  // thread reads its record of phase ph at the end of phase ph - 1, so the
+  // stage written at phase ph (for phase ph + kGsStages - 1) was last read in
+  // phase ph - 2, before a block barrier.
   auto issue = [&](int ph, int col) {
-    if (ph < phases) {
-      int q = sgo[col] + t;
-      if (q < sgo[col + 1]) {
-        const char* src = reinterpret_cast<const char*>(cc + q);
-        char* dst = reinterpret_cast<char*>(stage + (size_t)(ph & (kGsStages - 1)) * nt + t);
-#pragma unroll
-        for (int b = 0; b < (int)sizeof(GsContact); b += 16) cp_async16(dst + b, src + b);
-      }
+    if (t != producer || ph >= phases) return;
+    uint64_t* bar = &bars[ph & (kGsStages - 1)];
+    const unsigned bytes = (unsigned)((sgo[col + 1] - sgo[col]) * (int)sizeof(GsContact));
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    if (bytes) {
+      mbar_arrive_expect(bar, bytes);
+      bulk_copy_g2s(stage + (size_t)(ph & (kGsStages - 1)) * nt, cc + sgo[col], bytes, bar);
+    } else {
+      mbar_arrive(bar);
     }
-    cp_async_commit();
   };
   int col_issue = 0;
 #pragma unroll
@@ -1460,17 +1505,37 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
     issue(s, col_issue);
     col_issue = col_issue + 1 == ncolors ? 0 : col_issue + 1;
   }
+  // Registers carry the record and the correction of the phase about to run;
+  // they are loaded before the previous phase's barrier, so their latency
+  // overlaps the barrier.  A thread always takes the same contact of a
+  // colour, so the correction it loads was last written by itself (with one
+  // colour, in the phase just run, earlier in this thread's program order).
+  GsContact kn;
+  float4 on = make_float4(0.f, 0.f, 0.f, 0.f);
+  int qn = -1;
+  bool lost = false;  // a copy this thread waited for did not land in time
+  auto fetch = [&](int ph, int col) {
+    const bool landed = mbar_wait(&bars[ph & (kGsStages - 1)], (unsigned)(ph / kGsStages) & 1u);
+    qn = sgo[col] + t;
+    if (landed && qn < sgo[col + 1]) {
+      kn = stage[(size_t)(ph & (kGsStages - 1)) * nt + t];
+      on = sc[qn];
+    } else {
+      qn = -1;
+    }
+    lost = lost || !landed;
+  };
   int col = 0;
-  for (int ph = 0; ph < phases; ++ph) {
+  if (phases > 0) fetch(0, 0);
+  int ph = 0;
+  for (; ph < phases; ++ph) {
     issue(ph + kGsStages - 1, col_issue);
     col_issue = col_issue + 1 == ncolors ? 0 : col_issue + 1;
-    cp_async_wait<kGsStages - 1>();
-    const int cur = sgo[col] + t;
-    const bool active = cur < sgo[col + 1];
+    const int cur = qn;
+    const GsContact kc = kn;
+    const float4 o = on;
     col = col + 1 == ncolors ? 0 : col + 1;
-    if (active) {
-      const GsContact kc = stage[(size_t)(ph & (kGsStages - 1)) * nt + t];
-      const float4 o = sc[cur];
+    if (cur >= 0) {
       // All four positions read at once, without branches (a kinematic
       // vertex reads the zero slot: u gains c * 0).
       float3 u = kc.affine;
@@ -1494,9 +1559,22 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
         sp[sl] = gs_move(x, kc.gamma[s], du);
       }
     }
-    __syncthreads();
+    if (ph + 1 < phases) fetch(ph + 1, col);
+    // The block barrier that orders the colours also agrees on a lost copy,
+    // so every thread leaves the loop at the same phase.
+    if (__syncthreads_or(lost)) break;
   }
-  cp_async_wait<0>();
+  if (ph < phases) {
+    // A copy did not land in time: wait (bounded) for the copies still in
+    // flight, report the failure (the step then returns
+    // IterativeSolveFail) and leave the positions untouched.
+    if (t == producer) {
+      for (int q = ph; q < ph + kGsStages && q < phases; ++q)
+        mbar_wait(&bars[q & (kGsStages - 1)], (unsigned)(q / kGsStages) & 1u);
+      if (fail) atomicOr(fail, kFailContactWait);
+    }
+    return;
+  }
   for (int q = t; q < total; q += nt) corr[cc[q].ci & 0x7fffffff] = sc[q];
   for (int i = t; i < nslots; i += nt) p[vlist[i]] = sp[i];
 }
@@ -2207,7 +2285,7 @@ void CollisionSystem::contact_solve() {
       (void)pattr;
       contact_gs_pipe_kernel<<<1, threads, L.bytes, st>>>(
           I.gs_cc.p, I.group_off.p, I.n_colors, I.n_contacts, I.corr.p, I.gs_vlist.p,
-          I.gs_nslots, w_.contact_p.p);
+          I.gs_nslots, w_.contact_p.p, w_.cg_fail.p);
       SILK_LAUNCHED();
       return;
     }

@@ -1296,6 +1296,7 @@ struct DsmShared {
   int gval[kDsmCoarseBanks];
   int mnode[kDsmCoarseBanks * BANK];
   int mem[kDsmCoarseBanks * BANK];
+  unsigned tmem_base;  // tensor-memory address of the CTA's row store
 };
 
 __device__ __forceinline__ void stage_bank_full(const MasLevelDev& lv, int bank, float* slot,
@@ -1332,9 +1333,80 @@ __device__ __forceinline__ float3 dsm_row(const int2* e, int rw, const float4* p
     int2 q = e[j * BANK];
     float val = __int_as_float(q.y);
     float4 pj = pl[-1 - q.x];
-    yx += val * pj.x;
-    yy += val * pj.y;
-    yz += val * pj.z;
+    yx = fmaf(val, pj.x, yx);
+    yy = fmaf(val, pj.y, yy);
+    yz = fmaf(val, pj.z, yz);
+  }
+  return make_float3(yx, yy, yz);
+}
+
+// Tensor memory (sm_100a) as a per-CTA store for the SpMV rows.  A warp
+// reaches the 32 lanes 32 (w % 4) .. 32 (w % 4) + 31 of it; lane = row
+// (bank slot), two 32-bit columns per row entry (column index, value).
+// Every tcgen05 instruction here is warp-collective and runs in warp-uniform
+// control flow.
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void tmem_alloc(unsigned* dst, unsigned ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+               ::"r"(smem_addr(dst)), "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+}
+// Store 16 columns of this thread's lane, then wait for the warp's stores.
+__device__ __forceinline__ void tmem_st16_wait(unsigned taddr, const unsigned (&v)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16};\n"
+      "tcgen05.wait::st.sync.aligned;\n"
+      ::"r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]),
+      "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]),
+      "r"(v[13]), "r"(v[14]), "r"(v[15])
+      : "memory");
+}
+// Load 16 columns of this thread's lane; the wait is in the same statement,
+// so no use of the outputs can be scheduled before it.
+__device__ __forceinline__ void tmem_ld16_wait(unsigned taddr, unsigned (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];\n"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+        "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr)
+      : "memory");
+}
+
+// dsm_row with the row entries read from tensor memory, eight per load (the
+// entries of dsm_row in the same order, so the same sums).
+__device__ __forceinline__ float3 dsm_row_tmem(unsigned taddr, int rw, const float4* pl, float d,
+                                               float3 pv) {
+  float yx = d * pv.x, yy = d * pv.y, yz = d * pv.z;
+  for (int j0 = 0; j0 < rw; j0 += 8) {
+    unsigned e[16];
+    tmem_ld16_wait(taddr + 2 * j0, e);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (j0 + k < rw) {
+        const float val = __uint_as_float(e[2 * k + 1]);
+        const float4 pj = pl[-1 - (int)e[2 * k]];
+        yx = fmaf(val, pj.x, yx);
+        yy = fmaf(val, pj.y, yy);
+        yz = fmaf(val, pj.z, yz);
+      }
+    }
   }
   return make_float3(yx, yy, yz);
 }
@@ -1459,6 +1531,43 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
   }
   const int npush = a.push_off[q + 1] - a.push_off[q];
   for (int i = tid; i < npush; i += T) s.push[i] = a.push[a.push_off[q] + i];
+  // Row store in tensor memory: warp w keeps its bank's rows in lanes
+  // 32 (w % 4).. and columns 2 tm_rw (w / 4) .. 2 tm_rw (w / 4 + 1) - 1,
+  // entries past the bank's width padded with (own slot, 0) and never read.
+  const bool tm = a.tm_cols > 0 && (W / 4) * 2 * a.tm_rw <= a.tm_cols && rw <= a.tm_rw;
+  unsigned taddr = 0;
+  if (a.tm_cols > 0) {
+    if (warp == 0) tmem_alloc(&s.tmem_base, (unsigned)a.tm_cols);
+    tmem_fence_before();
+    __syncthreads();
+    tmem_fence_after();
+    taddr = s.tmem_base + ((unsigned)((warp & 3) * 32) << 16) + (unsigned)((warp >> 2) * 2 * a.tm_rw);
+    if (tm) {
+      for (int j0 = 0; j0 < rw; j0 += 8) {
+        unsigned e[16];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int2 qe = j0 + k < rw ? erow[(j0 + k) * BANK] : make_int2(-1 - tid, 0);
+          e[2 * k] = (unsigned)qe.x;
+          e[2 * k + 1] = (unsigned)qe.y;
+        }
+        tmem_st16_wait(taddr + 2 * j0, e);
+      }
+    }
+  }
+  auto row = [&](float3 pv) {
+    return tm ? dsm_row_tmem(taddr, rw, s.pl, d, pv) : dsm_row(erow, rw, s.pl, d, pv);
+  };
+  // Every warp's tensor-memory accesses are complete before warp 0 frees it.
+  auto tm_release = [&]() {
+    if (a.tm_cols <= 0) return;
+    tmem_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+      tmem_fence_after();
+      tmem_dealloc(s.tmem_base, (unsigned)a.tm_cols);
+    }
+  };
   auto gather_halo = [&](const float4* ex) {
     if (hcol >= 0) s.pl[T + tid] = ldcg4(ex + hcol);
     __syncthreads();
@@ -1486,7 +1595,7 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
   gather_halo(a.p);
   float3 r;
   {
-    float3 y = dsm_row(erow, rw, s.pl, d, x);
+    float3 y = row(x);
     r = own ? make_float3(b.x - y.x, b.y - y.y, b.z - y.z) : make_float3(0.f, 0.f, 0.f);
   }
   double rr_judge = -1.0;
@@ -1503,7 +1612,7 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     gather_halo(a.Ap);
     float3 ra;
     {
-      float3 y = dsm_row(erow, rw, s.pl, d, xa);
+      float3 y = row(xa);
       ra = own ? make_float3(b.x - y.x, b.y - y.y, b.z - y.z) : make_float3(0.f, 0.f, 0.f);
     }
     const double v3[3] = {(double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z,
@@ -1646,6 +1755,7 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
       a.result[1] = kCgInvalidInitialResidual;
       *a.result_rr = (float)rr;
     }
+    tm_release();
     return;  // every CTA takes the same decision; no store is in flight
   }
   const double rr0 = rr_judge >= 0.0 ? rr_judge : rr;
@@ -1673,7 +1783,7 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     __syncthreads();
     tr.stamp(iter, 1);
     {
-      Ap = dsm_row(erow, rw, s.pl, d, p);
+      Ap = row(p);
       if (!own) Ap = make_float3(0.f, 0.f, 0.f);
       tr.stamp(iter, 2);
       const double v1[1] = {own ? (double)p.x * Ap.x + (double)p.y * Ap.y + (double)p.z * Ap.z
@@ -1714,6 +1824,7 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     beta = fabs(rz_old) < 1e-20 ? 0.0 : rz / rz_old;
     if (stop) break;
   }
+  tm_release();
   if (own) a.x[v] = make_float4(x.x, x.y, x.z, 0.f);
   tr.finish(iter);
   if (q == 0 && tid == 0) {

@@ -12,6 +12,7 @@ namespace silkb {
 // convergence test and reported as IterativeSolveFail.
 constexpr int kFailBarrier = 1;   // a grid-barrier wait of a CG kernel gave up
 constexpr int kFailMasPivot = 2;  // a MAS bank had a zero or non-finite pivot
+constexpr int kFailContactWait = 4;  // a contact Gauss-Seidel copy did not land in time
 
 constexpr int kPacked = BANK * (BANK + 1) / 2;  // 528 packed upper entries
 
@@ -100,6 +101,11 @@ struct CgArgs {
   // banks per CTA (8 or 16; 0 = not this form).  It uses the rb_ptr / rb_w /
   // rent / halo_off / halo_col layout built for blocks of dsm_f fine banks.
   int dsm_f = 0;
+  // Its matrix rows in tensor memory: columns allocated per CTA (a power of
+  // two, 32..512; 0 = rows read from rent in global memory every SpMV) and
+  // row entries held per bank slot (a multiple of 8, at least every rb_w).
+  int tm_cols = 0;
+  int tm_rw = 0;
   // Its pushes of fine-level z to the halos of other CTAs: per CTA (CSR)
   // entries own slot | consumer CTA << 10 | consumer halo index << 15.
   const int* push_off = nullptr;

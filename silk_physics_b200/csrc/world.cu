@@ -537,7 +537,9 @@ BlockLayout block_layout(const ClothSetup& S, int bpb, int halo_cap) {
 //     to 16 or a cooperative grid);
 //  3. otherwise the streaming form.
 // Forms 1 and 2 need every fine bank to be one first-level coarse node.
-// solver option cg_form: 0 all forms, 2 forms 2 and 3, 1 form 3 only.
+// solver option cg_form: 0 all forms, 2 forms 2 and 3, 1 form 3 only; 3 as
+// 0 with form 1 reading its matrix rows from global memory in every SpMV
+// instead of holding them in tensor memory.
 void World::build_resident_layout(Cloth& c) {
   const ClothSetup& S = *c.setup;
   ClothDev& d = c.dev;
@@ -545,6 +547,8 @@ void World::build_resident_layout(Cloth& c) {
   d.res_grid = 0;
   d.dsm_ctas = 0;
   d.dsm_f = 0;
+  d.dsm_tm_cols = 0;
+  d.dsm_tm_rw = 0;
   const int nbank0 = S.fine.nbank;
   const int nblocks = div_up(nbank0, BANK);
   int upper = 0, all_coarse = 0;
@@ -567,7 +571,8 @@ void World::build_resident_layout(Cloth& c) {
     d.res_halo_full = L.halo_full;
     d.res_halo_col.upload(L.halo_col, st);
   };
-  if (opt.cg_form == 0 && S.levels > 0 && all_coarse <= kDsmCoarseBankLimit) {
+  if ((opt.cg_form == 0 || opt.cg_form == 3) && S.levels > 0 &&
+      all_coarse <= kDsmCoarseBankLimit) {
     for (int f : {8, 16}) {
       const int n = cg_dsm_ctas(nbank0, f);
       if (n == 0) continue;
@@ -599,6 +604,15 @@ void World::build_resident_layout(Cloth& c) {
       d.dsm_push.upload(plist, st);
       d.dsm_ctas = n;
       d.dsm_f = f;
+      // Rows in tensor memory: f / 4 warps share each 32-lane quarter, two
+      // columns per entry, the widest bank's entries rounded up to 8.
+      int wmax = 0;
+      for (int wd : L.width) wmax = std::max(wmax, wd);
+      const int rwpad = std::max(8, div_up(wmax, 8) * 8);
+      int cols = 32;
+      while (cols < (f / 4) * 2 * rwpad) cols *= 2;
+      d.dsm_tm_rw = rwpad;
+      d.dsm_tm_cols = opt.cg_form == 0 && cols <= 512 ? cols : 0;
       return;
     }
   }
@@ -799,6 +813,8 @@ void World::build_cloth_device(Cloth& c) {
     a.dsm_f = d.dsm_f;
     a.push_off = d.dsm_push_off.p;
     a.push = d.dsm_push.p;
+    a.tm_cols = d.dsm_tm_cols;
+    a.tm_rw = d.dsm_tm_rw;
     a.rb_ptr = d.rb_ptr.p;
     a.rb_w = d.rb_w.p;
     a.rent = d.rent.p;
@@ -1389,7 +1405,8 @@ silk_status World::solver_step() {
         CUDA_CHECK(cudaMemcpy(&f, cg_fail.p, sizeof(int), cudaMemcpyDeviceToHost));
         last_error = (f & kFailMasPivot) ? "MAS bank inverse failed: zero or non-finite pivot"
                      : (f & kFailBarrier) ? "CG barrier wait gave up"
-                                          : "solver diverged";
+                     : (f & kFailContactWait) ? "contact Gauss-Seidel copy wait gave up"
+                                              : "solver diverged";
         if (f) cg_fail.zero(st);
         return SILK_ERR_ITERATIVE_SOLVE_FAIL;
       }

@@ -163,7 +163,7 @@ class SolverOptions:
     cg_max_iter: int = 1000
     mas_bf16: bool = False
     profile: int = 0  # 1: CUDA-event kernel timing; 2: also the CG phase trace
-    cg_form: int = 0  # 0: cluster form, else resident, else streaming; 2: no cluster form; 1: streaming
+    cg_form: int = 0  # 0: cluster form, else resident, else streaming; 2: no cluster form; 1: streaming; 3: as 0, cluster rows from global memory
     learned_warm_start: bool = False  # offer the loaded model's first-solve start
     capture_samples: int = 0  # bit 1: first-solve samples, bit 2: iterate-model samples
     contact_gs_form: int = 0          # 0: single-block Gauss-Seidel where possible; 1: grid

@@ -203,6 +203,37 @@ def test_resident_and_streaming_forms_against_oracle(oracle, s):
     assert all(abs(a - b) <= 0.05 * b for a, b in zip(ic, is_))
 
 
+@pytest.mark.parametrize("s", [32, 80])
+@pytest.mark.parametrize("bf16", [False, True])
+def test_cluster_rows_tensor_memory_identical(s, bf16):
+    """The cluster form holds its SpMV rows in tensor memory (cg_form 0) or
+    reads them from global memory in every SpMV (cg_form 3): the same entries
+    in the same order, so bit-identical positions and iteration counts after
+    three steps (32: 5 CTAs of 8 fine banks, 80: 14 CTAs of 16)."""
+    out = []
+    for form in (0, 3):
+        V, F = S.grid_sheet(s, jitter=1e-4, seed=3)
+        w = N.World()
+        assert w.init()
+        assert w.set_global_config(N.GlobalConfig(max_inner_iteration=10))
+        assert w.set_solver_options(N.SolverOptions(fixed_linear_rel_tol=1e-5, cg_form=form,
+                                                    mas_bf16=bf16))
+        r, h = w.add_cloth(N.ClothConfig(), NO_COLLISION, V, F, S.top_corner_pins(s))
+        assert r
+        iters = []
+        for _ in range(3):
+            assert w.solver_step(), w
+            st = w.step_stats()
+            assert st.cg_cluster_solves == st.cg_solves > 0
+            iters.append(st.cg_iterations)
+        x = np.zeros(V.size, np.float32)
+        assert w.get_cloth_position(h, x)
+        out.append((iters, x))
+    print(f"s={s} bf16={bf16}: CG iterations {out[0][0]} (tensor memory) {out[1][0]} (global)")
+    assert out[0][0] == out[1][0]
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+
+
 @pytest.mark.parametrize("form", [0, 1])
 def test_admm_extrapolated_start_against_oracle(oracle, form):
     """CG solves started from 2 x_k - x_(k-1) of the ADMM iterates (blended
