@@ -524,6 +524,15 @@ def run_ours(args) -> None:
             "admm_host_wall": round(prof["admm_host_ms"] / args.steps, 2),
             "ccd_host_wall": round(prof["ccd_host_ms"] / args.steps, 2),
             "dcd_host_wall": round(prof["dcd_host_ms"] / args.steps, 2),
+            "dcd_parts_host_wall": {
+                k: round(prof[f"dcd_{k}_host_ms"] / args.steps, 2)
+                for k in ("refit", "candidates", "build", "coloring", "layout")},
+            "dcd_calls": round(prof["dcd_calls"] / args.steps, 1),
+            "ccd_parts": {
+                "refit_host_wall": round(prof["ccd_refit_host_ms"] / args.steps, 2),
+                "candidates_host_wall": round(prof["ccd_candidates_host_ms"] / args.steps, 2),
+                "first_pass_events": round(prof["ccd_first_pass_ms"] / args.steps, 2),
+                "second_pass_events": round(prof["ccd_second_pass_ms"] / args.steps, 2)},
             "step_host_wall": round(prof["step_host_ms"] / args.steps, 2)},
         "variants": variants,
         "reference_scenes": ref_scenes,

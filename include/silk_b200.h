@@ -93,11 +93,11 @@ typedef struct {
                                  form where it fits, else streaming;
                                  2: resident where it fits, else streaming;
                                  1: streaming always;
-                                 3: as 0, the cluster form reading its matrix
-                                 rows from global memory in every SpMV instead
-                                 of holding them in tensor memory (applies
-                                 when the solver layout is built; changing it
-                                 rebuilds it) */
+                                 3, 4: as 0 and 2, the cluster and resident
+                                 forms reading their matrix rows from global
+                                 memory in every SpMV instead of holding them
+                                 in tensor memory (applies when the solver
+                                 layout is built; changing it rebuilds it) */
   int32_t learned_warm_start; /* 1: offer the loaded first-solve model's
                                  prediction as the start of each outer
                                  iteration's first CG solve and, when an
@@ -132,8 +132,8 @@ typedef struct {
 
 /* CUDA-event timing of the persistent CG kernel over the steps since the
  * last reset (silk_solver_options.profile = 1); the struct grew by the four
- * narrowphase fields at its end, so callers compiled against a shorter
- * silk_profile must be rebuilt.  algorithmic_bytes counts
+ * narrowphase fields and the six DCD fields at its end, so callers compiled
+ * against a shorter silk_profile must be rebuilt.  algorithmic_bytes counts
  * compulsory DRAM traffic per CG iteration: matrix entries, MAS bank
  * inverses and each vector read or written once. */
 typedef struct {
@@ -153,6 +153,13 @@ typedef struct {
   double ccd_second_pass_ms; /* events: narrowphase second pass (searches that outgrew it) */
   double ccd_second_pass_queries; /* queries that ran the second pass */
   double ccd_calls;          /* narrowphase calls (one per outer iteration) */
+  double dcd_refit_host_ms;  /* part of dcd_host_ms: collider refit and tree builds */
+  double dcd_candidates_host_ms; /* part of dcd_host_ms: broadphase candidate gathering */
+  double dcd_build_host_ms;  /* part of dcd_host_ms: DCD kernel, dedup, contact records,
+                                vertex incidence */
+  double dcd_coloring_host_ms; /* part of dcd_host_ms: Jones-Plassmann colouring, groups */
+  double dcd_layout_host_ms; /* part of dcd_host_ms: Gauss-Seidel slots and records */
+  double dcd_calls;          /* DCD calls (step start and each rollback) */
 } silk_profile;
 
 /* Statistics of the last solver_step. */

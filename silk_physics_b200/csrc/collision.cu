@@ -2082,8 +2082,18 @@ void CollisionSystem::begin_step() {
 
 int CollisionSystem::append_active(float time, float dact) {
   CollisionImpl& I = *impl_;
+  using clk = std::chrono::steady_clock;
+  auto lap = [](clk::time_point& t) {
+    const clk::time_point now = clk::now();
+    const double ms = std::chrono::duration<double, std::milli>(now - t).count();
+    t = now;
+    return ms;
+  };
+  clk::time_point t_lap = clk::now();
+  last_dcd_gather_ms = last_dcd_build_ms = last_dcd_color_ms = last_dcd_layout_ms = 0.0;
   cudaStream_t st = w_.stream;
   int n = gather_candidates(I, st);
+  last_dcd_gather_ms = lap(t_lap);
   if (n == 0) return 0;
   if (I.cols_cap < n) {
     I.cols_cap = n + n / 4;
@@ -2179,6 +2189,7 @@ int CollisionSystem::append_active(float time, float dact) {
                                                            w_.contact_w_base.p,
                                                            w_.contact_w.p, I.active_dof.p);
   SILK_LAUNCHED();
+  last_dcd_build_ms = lap(t_lap);
   // Colouring by Jones-Plassmann rounds, kJpBatch rounds between host
   // checks: a round after the last contact is coloured changes nothing, so
   // the colours equal those of checking after every round.  The overflow
@@ -2221,6 +2232,7 @@ int CollisionSystem::append_active(float time, float dact) {
   I.groups.upload(grp, st);
   I.group_off.upload(goff, st);
   I.n_colors = nc;
+  last_dcd_color_ms = lap(t_lap);
   // Colour-ordered contacts on compact vertex slots for the single-block
   // Gauss-Seidel form.
   {
@@ -2254,6 +2266,7 @@ int CollisionSystem::append_active(float time, float dact) {
     I.gs_ready = true;
   }
   CUDA_CHECK(cudaStreamSynchronize(st));
+  last_dcd_layout_ms = lap(t_lap);
   return add;
 }
 

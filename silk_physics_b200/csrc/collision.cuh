@@ -47,6 +47,11 @@ class CollisionSystem {
   // queries that ran the second pass.
   double last_first_pass_ms = 0.0, last_second_pass_ms = 0.0;
   int last_second_pass_queries = 0;
+  // Host wall time of the parts of the last append_active: candidate
+  // gathering, contact build (DCD kernel, dedup, records, incidence),
+  // colouring and the Gauss-Seidel layout.
+  double last_dcd_gather_ms = 0.0, last_dcd_build_ms = 0.0, last_dcd_color_ms = 0.0,
+         last_dcd_layout_ms = 0.0;
 
   // Inspection.
   int debug_candidates(int* out, int64_t cap);

@@ -604,6 +604,7 @@ struct ResShared {
   float4 zs[kResWarps][BANK];             // BF16 apply: accumulator rows back to slots
   double red[kResWarps][3];
   double tot[3];
+  unsigned tmem_base;  // tensor-memory address of the block's row store
 };
 static_assert(offsetof(ResShared, M1) % 16 == 0 && offsetof(ResShared, Mc) % 16 == 0 &&
                   (kPacked * sizeof(float)) % 16 == 0,
@@ -727,6 +728,55 @@ __device__ double res_total(const double* partials, int slot, int nblocks, ResSh
 
 __device__ __forceinline__ float4 ldcg4(const float4* p) { return __ldcg(p); }
 
+// Tensor memory (sm_100a) as a per-CTA store for the SpMV rows.  A warp
+// reaches the 32 lanes 32 (w % 4) .. 32 (w % 4) + 31 of it; lane = row
+// (bank slot), two 32-bit columns per row entry (column index, value).
+// Every tcgen05 instruction here is warp-collective and runs in warp-uniform
+// control flow.
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void tmem_alloc(unsigned* dst, unsigned ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+               ::"r"(smem_addr(dst)), "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+}
+// Store 16 columns of this thread's lane, then wait for the warp's stores.
+__device__ __forceinline__ void tmem_st16_wait(unsigned taddr, const unsigned (&v)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16};\n"
+      "tcgen05.wait::st.sync.aligned;\n"
+      ::"r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]),
+      "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]),
+      "r"(v[13]), "r"(v[14]), "r"(v[15])
+      : "memory");
+}
+// Load 16 columns of this thread's lane; the wait is in the same statement,
+// so no use of the outputs can be scheduled before it.
+__device__ __forceinline__ void tmem_ld16_wait(unsigned taddr, unsigned (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];\n"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+        "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr)
+      : "memory");
+}
+
 // Off-diagonal row sum of this thread's vertex plus the diagonal term.
 __device__ __forceinline__ float3 res_row(const CgArgs& a, const ResShared& s,
                                           const float4* ex, int rptr, int rw,
@@ -738,9 +788,32 @@ __device__ __forceinline__ float3 res_row(const CgArgs& a, const ResShared& s,
     int2 q = e[j * BANK];
     float val = __int_as_float(q.y);
     float4 pj = q.x < 0 ? s.pl[-1 - q.x] : ldcg4(ex + q.x);
-    yx += val * pj.x;
-    yy += val * pj.y;
-    yz += val * pj.z;
+    yx = fmaf(val, pj.x, yx);
+    yy = fmaf(val, pj.y, yy);
+    yz = fmaf(val, pj.z, yz);
+  }
+  return make_float3(yx, yy, yz);
+}
+
+// res_row with the row entries read from tensor memory, eight per load (the
+// entries of res_row in the same order, so the same sums).
+__device__ __forceinline__ float3 res_row_tmem(const ResShared& s, const float4* ex,
+                                               unsigned taddr, int rw, float d, float3 pv) {
+  float yx = d * pv.x, yy = d * pv.y, yz = d * pv.z;
+  for (int j0 = 0; j0 < rw; j0 += 8) {
+    unsigned e[16];
+    tmem_ld16_wait(taddr + 2 * j0, e);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (j0 + k < rw) {
+        const int col = (int)e[2 * k];
+        const float val = __uint_as_float(e[2 * k + 1]);
+        const float4 pj = col < 0 ? s.pl[-1 - col] : ldcg4(ex + col);
+        yx = fmaf(val, pj.x, yx);
+        yy = fmaf(val, pj.y, yy);
+        yz = fmaf(val, pj.z, yz);
+      }
+    }
   }
   return make_float3(yx, yy, yz);
 }
@@ -756,7 +829,21 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
   CgTrace tr(a.trace, 1);
   int iter = -1;  // -1 while setting up (not traced)
   double* part = a.partials + 4 * k;
+  // Row store in tensor memory (allocated after the staging below): every
+  // warp's accesses complete before warp 0 frees it, on every way out.
+  unsigned taddr = 0;
+  bool tm = false;
+  auto tm_release = [&]() {
+    if (a.tm_cols <= 0) return;
+    tmem_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+      tmem_fence_after();
+      tmem_dealloc(s.tmem_base, (unsigned)a.tm_cols);
+    }
+  };
   auto fail = [&]() {
+    tm_release();
     if (tid == 0 && a.fail) atomicOr(a.fail, kFailBarrier);
   };
 
@@ -785,6 +872,31 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
   const bool own = lane < vsize;
   const int v = vbase + lane;
   if (has1 && warp == 0) stage(a.coarse[0], k, s.M1);
+  // Warp w keeps its bank's rows in lanes 32 (w % 4).. of the row store and
+  // columns 2 tm_rw (w / 4) .., entries past the bank's width padded with
+  // (own slot, 0) and never read.
+  if (a.tm_cols > 0) {
+    tm = (kResWarps / 4) * 2 * a.tm_rw <= a.tm_cols && rw <= a.tm_rw;
+    if (warp == 0) tmem_alloc(&s.tmem_base, (unsigned)a.tm_cols);
+    tmem_fence_before();
+    __syncthreads();
+    tmem_fence_after();
+    taddr = s.tmem_base + ((unsigned)((warp & 3) * 32) << 16) + (unsigned)((warp >> 2) * 2 * a.tm_rw);
+    if (tm) {
+      const int2* erow = a.rent + rptr + lane;
+      for (int j0 = 0; j0 < rw; j0 += 8) {
+        unsigned e[16];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int2 qe = j0 + q < rw ? erow[(j0 + q) * BANK] : make_int2(-1 - tid, 0);
+          e[2 * q] = (unsigned)qe.x;
+          e[2 * q + 1] = (unsigned)qe.y;
+        }
+        tmem_st16_wait(taddr + 2 * j0, e);
+      }
+    }
+  }
+
   // First-level restriction plan of this block's coarse bank (warp 0).
   int l1_ncco = 0, l1_base = 0, l1_mine = -1;
   if (has1 && warp == 0 && a.levels > 1) {
@@ -818,6 +930,9 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
       cm[3] = c.w;
     }
   }
+  auto row = [&](const float4* ex, float3 pv) {
+    return tm ? res_row_tmem(s, ex, taddr, rw, d, pv) : res_row(a, s, ex, rptr, rw, lane, d, pv);
+  };
   // Halo: thread i < nhalo gathers halo vertex i of the block into slot
   // kResThreads + i before each product (one round trip, all loads in flight).
   int hcol = -1;
@@ -842,7 +957,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
   gather_halo(a.p);
   float3 r;
   {
-    float3 y = res_row(a, s, a.p, rptr, rw, lane, d, x);
+    float3 y = row(a.p, x);
     r = own ? make_float3(b.x - y.x, b.y - y.y, b.z - y.z) : make_float3(0.f, 0.f, 0.f);
   }
   // Alternative start: residual of x_alt (published through the Ap buffer),
@@ -862,7 +977,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     gather_halo(a.Ap);
     float3 ra;
     {
-      float3 y = res_row(a, s, a.Ap, rptr, rw, lane, d, xa);
+      float3 y = row(a.Ap, xa);
       ra = own ? make_float3(b.x - y.x, b.y - y.y, b.z - y.z) : make_float3(0.f, 0.f, 0.f);
     }
     const double v3[3] = {(double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z,
@@ -1098,6 +1213,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
       a.result[1] = kCgInvalidInitialResidual;
       *a.result_rr = (float)rr;
     }
+    tm_release();
     return;
   }
   const double rr0 = rr_judge >= 0.0 ? rr_judge : rr;
@@ -1136,7 +1252,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     // B: Ap and p.Ap.
     {
       if (!halo_p) gather_halo(a.p);
-      Ap = res_row(a, s, a.p, rptr, rw, lane, d, p);
+      Ap = row(a.p, p);
       if (!own) Ap = make_float3(0.f, 0.f, 0.f);
       tr.stamp(iter, 2);
       const double v1[1] = {own ? (double)p.x * Ap.x + (double)p.y * Ap.y + (double)p.z * Ap.z
@@ -1178,6 +1294,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     beta = fabs(rz_old) < 1e-20 ? 0.0 : rz / rz_old;
     if (stop) break;
   }
+  tm_release();
   if (own) a.x[v] = make_float4(x.x, x.y, x.z, 0.f);
   tr.finish(iter);
   if (k == 0 && tid == 0) {
@@ -1338,55 +1455,6 @@ __device__ __forceinline__ float3 dsm_row(const int2* e, int rw, const float4* p
     yz = fmaf(val, pj.z, yz);
   }
   return make_float3(yx, yy, yz);
-}
-
-// Tensor memory (sm_100a) as a per-CTA store for the SpMV rows.  A warp
-// reaches the 32 lanes 32 (w % 4) .. 32 (w % 4) + 31 of it; lane = row
-// (bank slot), two 32-bit columns per row entry (column index, value).
-// Every tcgen05 instruction here is warp-collective and runs in warp-uniform
-// control flow.
-__device__ __forceinline__ unsigned smem_addr(const void* p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void tmem_alloc(unsigned* dst, unsigned ncols) {
-  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
-               ::"r"(smem_addr(dst)), "r"(ncols)
-               : "memory");
-  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
-}
-__device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols) {
-  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols)
-               : "memory");
-}
-__device__ __forceinline__ void tmem_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-}
-__device__ __forceinline__ void tmem_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-}
-// Store 16 columns of this thread's lane, then wait for the warp's stores.
-__device__ __forceinline__ void tmem_st16_wait(unsigned taddr, const unsigned (&v)[16]) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-      "%11, %12, %13, %14, %15, %16};\n"
-      "tcgen05.wait::st.sync.aligned;\n"
-      ::"r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]),
-      "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]),
-      "r"(v[13]), "r"(v[14]), "r"(v[15])
-      : "memory");
-}
-// Load 16 columns of this thread's lane; the wait is in the same statement,
-// so no use of the outputs can be scheduled before it.
-__device__ __forceinline__ void tmem_ld16_wait(unsigned taddr, unsigned (&v)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-      "%11, %12, %13, %14, %15}, [%16];\n"
-      "tcgen05.wait::ld.sync.aligned;\n"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-        "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(taddr)
-      : "memory");
 }
 
 // dsm_row with the row entries read from tensor memory, eight per load (the

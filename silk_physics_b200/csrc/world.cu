@@ -527,6 +527,21 @@ BlockLayout block_layout(const ClothSetup& S, int bpb, int halo_cap) {
   return L;
 }
 
+// Row store of the cluster and resident CG forms in tensor memory: the
+// bpb / 4 warps of a CTA that share a 32-lane quarter of it each hold their
+// bank's rows in 2 tm_rw columns (two per entry, the widest bank's entries
+// rounded up to 8); the allocation is the next power of two, at most the
+// 512 columns of an SM.  Off (cg_form 3 and 4): rows read from global memory.
+void set_row_store(ClothDev& d, const BlockLayout& L, int bpb, bool on) {
+  int wmax = 0;
+  for (int wd : L.width) wmax = std::max(wmax, wd);
+  const int rwpad = std::max(8, div_up(wmax, 8) * 8);
+  int cols = 32;
+  while (cols < (bpb / 4) * 2 * rwpad) cols *= 2;
+  d.tm_rw = rwpad;
+  d.tm_cols = on && cols <= 512 ? cols : 0;
+}
+
 }  // namespace
 
 // Launch form of the cloth's CG solve, chosen when its layout is built:
@@ -537,9 +552,9 @@ BlockLayout block_layout(const ClothSetup& S, int bpb, int halo_cap) {
 //     to 16 or a cooperative grid);
 //  3. otherwise the streaming form.
 // Forms 1 and 2 need every fine bank to be one first-level coarse node.
-// solver option cg_form: 0 all forms, 2 forms 2 and 3, 1 form 3 only; 3 as
-// 0 with form 1 reading its matrix rows from global memory in every SpMV
-// instead of holding them in tensor memory.
+// solver option cg_form: 0 all forms, 2 forms 2 and 3, 1 form 3 only; 3 and
+// 4 as 0 and 2 with forms 1 and 2 reading their matrix rows from global
+// memory in every SpMV instead of holding them in tensor memory.
 void World::build_resident_layout(Cloth& c) {
   const ClothSetup& S = *c.setup;
   ClothDev& d = c.dev;
@@ -547,8 +562,8 @@ void World::build_resident_layout(Cloth& c) {
   d.res_grid = 0;
   d.dsm_ctas = 0;
   d.dsm_f = 0;
-  d.dsm_tm_cols = 0;
-  d.dsm_tm_rw = 0;
+  d.tm_cols = 0;
+  d.tm_rw = 0;
   const int nbank0 = S.fine.nbank;
   const int nblocks = div_up(nbank0, BANK);
   int upper = 0, all_coarse = 0;
@@ -604,15 +619,7 @@ void World::build_resident_layout(Cloth& c) {
       d.dsm_push.upload(plist, st);
       d.dsm_ctas = n;
       d.dsm_f = f;
-      // Rows in tensor memory: f / 4 warps share each 32-lane quarter, two
-      // columns per entry, the widest bank's entries rounded up to 8.
-      int wmax = 0;
-      for (int wd : L.width) wmax = std::max(wmax, wd);
-      const int rwpad = std::max(8, div_up(wmax, 8) * 8);
-      int cols = 32;
-      while (cols < (f / 4) * 2 * rwpad) cols *= 2;
-      d.dsm_tm_rw = rwpad;
-      d.dsm_tm_cols = opt.cg_form == 0 && cols <= 512 ? cols : 0;
+      set_row_store(d, L, f, opt.cg_form == 0);
       return;
     }
   }
@@ -621,7 +628,9 @@ void World::build_resident_layout(Cloth& c) {
   if (grid == 0) return;
   const int halo_cap = opt.resident_halo_limit > 0 ? std::min(opt.resident_halo_limit, kResHalo)
                                                    : kResHalo;
-  upload(block_layout(S, BANK, halo_cap));
+  const BlockLayout L = block_layout(S, BANK, halo_cap);
+  upload(L);
+  set_row_store(d, L, BANK, opt.cg_form == 0 || opt.cg_form == 2);
   d.res_blocks = nblocks;
   d.res_grid = grid;
 }
@@ -813,8 +822,6 @@ void World::build_cloth_device(Cloth& c) {
     a.dsm_f = d.dsm_f;
     a.push_off = d.dsm_push_off.p;
     a.push = d.dsm_push.p;
-    a.tm_cols = d.dsm_tm_cols;
-    a.tm_rw = d.dsm_tm_rw;
     a.rb_ptr = d.rb_ptr.p;
     a.rb_w = d.rb_w.p;
     a.rent = d.rent.p;
@@ -822,6 +829,8 @@ void World::build_cloth_device(Cloth& c) {
     a.halo_col = d.res_halo_col.p;
     a.halo_full = 1;
   }
+  a.tm_cols = d.tm_cols;
+  a.tm_rw = d.tm_rw;
   if (d.res_grid != 0) {
     a.res_blocks = d.res_blocks;
     a.rb_ptr = d.rb_ptr.p;
@@ -1368,6 +1377,13 @@ silk_status World::solver_step() {
     CUDA_CHECK(cudaMemcpyAsync(outer_v.p, prev_v.p, nv * sizeof(float4), cudaMemcpyDeviceToDevice, st));
     bool collide = coll_ && coll_->has_colliders();
     float ms = 0.f, dact = 0.f;
+    auto add_dcd_profile = [&]() {
+      prof.dcd_candidates_host_ms += coll_->last_dcd_gather_ms;
+      prof.dcd_build_host_ms += coll_->last_dcd_build_ms;
+      prof.dcd_coloring_host_ms += coll_->last_dcd_color_ms;
+      prof.dcd_layout_host_ms += coll_->last_dcd_layout_ms;
+      prof.dcd_calls += 1;
+    };
     if (coll_) {
       coll_->refresh_obstacles();
       coll_->begin_step();
@@ -1379,7 +1395,9 @@ silk_status World::solver_step() {
       NvtxRange dcd_range("refit + DCD + contact rebuild");
       auto t0 = clk::now();
       coll_->refit(outer.p, outer.p);
+      prof.dcd_refit_host_ms += ms_since(t0);
       coll_->append_active(0.0f, dact);
+      add_dcd_profile();
       prof.dcd_host_ms += ms_since(t0);
     }
     float remaining = 1.0f;
@@ -1441,7 +1459,9 @@ silk_status World::solver_step() {
       NvtxRange dcd_range("refit + DCD + contact rebuild");
       auto t0 = clk::now();
       coll_->refit(outer.p, outer.p);
+      prof.dcd_refit_host_ms += ms_since(t0);
       coll_->append_active(1.0f - remaining, dact);
+      add_dcd_profile();
       prof.dcd_host_ms += ms_since(t0);
     }
     // Final velocity from the whole accepted displacement (main_loop.cu:248).

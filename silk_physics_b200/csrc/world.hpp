@@ -107,7 +107,7 @@ struct ClothDev {
   int res_grid = 0;           // cg_resident_grid(res_blocks)
   int dsm_ctas = 0;           // cluster form with redundant coarse levels: CTAs (0 = not used)
   int dsm_f = 0;              // its fine banks per CTA
-  int dsm_tm_cols = 0, dsm_tm_rw = 0;  // its rows in tensor memory (CgArgs::tm_cols / tm_rw)
+  int tm_cols = 0, tm_rw = 0;  // cluster / resident rows in tensor memory (CgArgs::tm_cols / tm_rw)
   DevBuf<int> dsm_push_off, dsm_push;  // its pushes of fine-level z to other CTAs' halos
   CgArgs cg;
   int cg_grid = 1;

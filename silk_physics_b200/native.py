@@ -90,7 +90,10 @@ class _ProfileC(C.Structure):
                 ("step_host_ms", C.c_double), ("contact_gs_ms", C.c_double),
                 ("ccd_refit_host_ms", C.c_double), ("ccd_candidates_host_ms", C.c_double),
                 ("ccd_first_pass_ms", C.c_double), ("ccd_second_pass_ms", C.c_double),
-                ("ccd_second_pass_queries", C.c_double), ("ccd_calls", C.c_double)]
+                ("ccd_second_pass_queries", C.c_double), ("ccd_calls", C.c_double),
+                ("dcd_refit_host_ms", C.c_double), ("dcd_candidates_host_ms", C.c_double),
+                ("dcd_build_host_ms", C.c_double), ("dcd_coloring_host_ms", C.c_double),
+                ("dcd_layout_host_ms", C.c_double), ("dcd_calls", C.c_double)]
 
 
 class _StepStatsC(C.Structure):
@@ -163,7 +166,7 @@ class SolverOptions:
     cg_max_iter: int = 1000
     mas_bf16: bool = False
     profile: int = 0  # 1: CUDA-event kernel timing; 2: also the CG phase trace
-    cg_form: int = 0  # 0: cluster form, else resident, else streaming; 2: no cluster form; 1: streaming; 3: as 0, cluster rows from global memory
+    cg_form: int = 0  # 0: cluster form, else resident, else streaming; 2: no cluster form; 1: streaming; 3/4: as 0/2 with the rows in global memory
     learned_warm_start: bool = False  # offer the loaded model's first-solve start
     capture_samples: int = 0  # bit 1: first-solve samples, bit 2: iterate-model samples
     contact_gs_form: int = 0          # 0: single-block Gauss-Seidel where possible; 1: grid

@@ -203,15 +203,22 @@ def test_resident_and_streaming_forms_against_oracle(oracle, s):
     assert all(abs(a - b) <= 0.05 * b for a, b in zip(ic, is_))
 
 
-@pytest.mark.parametrize("s", [32, 80])
+# (cg_form with rows in tensor memory, the same with rows in global memory,
+# sheet side): the cluster form on 5 CTAs of 8 fine banks and on 14 of 16;
+# the resident form as a 2- and a 7-block cluster and a 17-block cooperative
+# grid.
+ROW_STORE_CASES = [(0, 3, 32), (0, 3, 80), (2, 4, 32), (2, 4, 80), (2, 4, 128)]
+
+
+@pytest.mark.parametrize("form_tm,form_global,s", ROW_STORE_CASES)
 @pytest.mark.parametrize("bf16", [False, True])
-def test_cluster_rows_tensor_memory_identical(s, bf16):
-    """The cluster form holds its SpMV rows in tensor memory (cg_form 0) or
-    reads them from global memory in every SpMV (cg_form 3): the same entries
-    in the same order, so bit-identical positions and iteration counts after
-    three steps (32: 5 CTAs of 8 fine banks, 80: 14 CTAs of 16)."""
+def test_cg_rows_tensor_memory_identical(form_tm, form_global, s, bf16):
+    """The cluster and resident CG forms hold their SpMV rows in tensor
+    memory (cg_form 0 and 2) or read them from global memory in every SpMV
+    (cg_form 3 and 4): the same entries in the same order, so bit-identical
+    positions and iteration counts after three steps."""
     out = []
-    for form in (0, 3):
+    for form in (form_tm, form_global):
         V, F = S.grid_sheet(s, jitter=1e-4, seed=3)
         w = N.World()
         assert w.init()
@@ -224,12 +231,16 @@ def test_cluster_rows_tensor_memory_identical(s, bf16):
         for _ in range(3):
             assert w.solver_step(), w
             st = w.step_stats()
-            assert st.cg_cluster_solves == st.cg_solves > 0
+            if form_tm == 0:
+                assert st.cg_cluster_solves == st.cg_solves > 0
+            else:
+                assert st.cg_resident_solves == st.cg_solves > 0 and st.cg_cluster_solves == 0
             iters.append(st.cg_iterations)
         x = np.zeros(V.size, np.float32)
         assert w.get_cloth_position(h, x)
         out.append((iters, x))
-    print(f"s={s} bf16={bf16}: CG iterations {out[0][0]} (tensor memory) {out[1][0]} (global)")
+    print(f"forms {form_tm}/{form_global} s={s} bf16={bf16}: CG iterations {out[0][0]} "
+          f"(tensor memory) {out[1][0]} (global)")
     assert out[0][0] == out[1][0]
     np.testing.assert_array_equal(out[0][1], out[1][1])
 
