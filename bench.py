@@ -375,6 +375,60 @@ def reference_scenes(N, steps_cloth_ball: int):
     return out
 
 
+def config1(N, torch, stream, cg_rel_tol, steps, cpu_budget_s):
+    """Config 1 as stated: the 32x32 sheet (two top corners pinned, default
+    cloth and collision settings, self-collision on, no obstacle), 10 ADMM
+    iterations per step, `steps` steps on the GPU timed with CUDA events
+    (the first, which builds the solver layout, untimed), and the CPU
+    restatement on all host cores for as many of the same steps as fit
+    cpu_budget_s (None: skipped)."""
+    from silk_physics_b200 import scenes as S
+
+    V, F = S.grid_sheet(32, jitter=0.0, seed=7)
+    P = S.top_corner_pins(32)
+    w = N.World()
+    assert w.init()
+    w.set_stream(stream.cuda_stream)
+    assert w.set_global_config(N.GlobalConfig(max_inner_iteration=10, admm_abs_tol=0.0,
+                                              admm_rel_tol=0.0))
+    assert w.set_solver_options(N.SolverOptions(fixed_linear_rel_tol=cg_rel_tol))
+    r, h = w.add_cloth(N.ClothConfig(), N.CollisionConfig(), V, F, P)
+    assert r, r.to_string()
+    perm, offs = w.cloth_partition(h, len(V))
+    assert w.solver_step()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    contacts = 0
+    with torch.cuda.stream(stream):
+        a.record(stream)
+        for _ in range(steps - 1):
+            assert w.solver_step()
+            contacts = max(contacts, w.step_stats().contacts)
+        b.record(stream)
+    b.synchronize()
+    ms = a.elapsed_time(b) / (steps - 1)
+    out = {"workload": "c1_sheet32_pinned_selfcollision", "vertices": int(len(V)),
+           "steps_timed": steps - 1, "value": round(1e3 / ms, 2), "unit": "steps/s",
+           "ms_per_step": round(ms, 3), "admm_iterations_per_step": 10,
+           "max_contacts": contacts, "cg_rel_tol": cg_rel_tol}
+    if cpu_budget_s is not None:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import pyoracle
+
+        ow = pyoracle.OracleWorld(config=dict(max_inner_iteration=10, admm_abs_tol=0.0,
+                                              admm_rel_tol=0.0, fixed_linear_rel_tol=cg_rel_tol))
+        ow.add_cloth(V, F, P, perm, offs)
+        t0 = time.perf_counter()
+        n = 0
+        while n < steps and (n == 0 or time.perf_counter() - t0 < cpu_budget_s):
+            assert ow.step() == 0
+            n += 1
+        sec = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(n / sec, 4), "unit": "steps/s",
+                               "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": f"the first {n} of the same steps ({sec:.1f} s wall)"}
+    return out
+
+
 def run_ours(args) -> None:
     import torch
 
@@ -454,10 +508,12 @@ def run_ours(args) -> None:
     e2e_val = weak_value(1, world_size, args.steps, max_over_ranks(sum(e2e_ms), "cuda"))
 
     # Single-GPU diagnostics: not repeated on every replica.
-    variants, ref_scenes = {}, None
+    variants, ref_scenes, c1 = {}, None, None
     if args.variants and world_size == 1:
         variants = variants_ab(N, torch, stream, flush, args)
         ref_scenes = reference_scenes(N, args.scene_steps)
+        c1 = config1(N, torch, stream, args.cg_rel_tol, 100,
+                     None if args.no_cpu_baseline else args.cpu_budget)
 
     if rank != 0:
         if world_size > 1:
@@ -536,6 +592,7 @@ def run_ours(args) -> None:
             "step_host_wall": round(prof["step_host_ms"] / args.steps, 2)},
         "variants": variants,
         "reference_scenes": ref_scenes,
+        "config1": c1,
     }
     print(json.dumps(line), flush=True)
     if world_size > 1:

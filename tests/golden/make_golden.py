@@ -3,8 +3,11 @@ restatement of the reference algorithm in oracle/), on seeded inputs:
 
 * c1_sheet32.npz: the 32x32 sheet with its two top corners pinned, 10 ADMM
   iterations per step, CG relative tolerance 1e-6 (the C1 parity setting),
-  with the MAS partition (host setup, no GPU), and the FP64 and FP32 oracle
-  positions after steps 1, 5 and 10;
+  collision off, with the MAS partition (host setup, no GPU), and the FP64
+  and FP32 oracle positions after steps 1, 5 and 10;
+* c1_sheet32_selfcol.npz: the same with the default collision settings
+  (collision and self-collision on, as config 1 states), plus the oracle's
+  contact counts after those steps;
 * ccd_queries.npz: 256 vertex-face and 256 edge-edge Tight-Inclusion CCD
   queries (seeded motions, min separations 0 / 1e-4 / 1e-3) with the
   oracle's hit flags and time-of-impact intervals.
@@ -31,18 +34,24 @@ C1_CONFIG = dict(max_inner_iteration=10, admm_abs_tol=0.0, admm_rel_tol=0.0,
 CCD_ERR = {True: 4.053116e-06, False: 3.814698e-06}
 
 
-def c1_sheet():
+# (is_collision_on, is_self_collision_on, group, restitution, friction)
+C1_COLLISION = {False: (0, 0, 0, 0.3, 0.3), True: (1, 1, 0, 0.3, 0.3)}
+
+
+def c1_sheet(self_collision=False):
     V, F = S.grid_sheet(32, jitter=0.0, seed=7)
     P = S.top_corner_pins(32)
     perm, offs = N.partition_mesh(V, F)
     out = {"verts": V, "faces": F, "pins": P, "perm": perm, "part_offsets": offs}
     for name, fp64 in (("o64", True), ("o32", False)):
         ow = pyoracle.OracleWorld(fp64=fp64, config=C1_CONFIG)
-        h = ow.add_cloth(V, F, P, perm, offs, collision=(0, 0, 0, 0.3, 0.3))
+        h = ow.add_cloth(V, F, P, perm, offs, collision=C1_COLLISION[self_collision])
         for k in range(1, max(C1_STEPS) + 1):
             assert ow.step() == 0
             if k in C1_STEPS:
                 out[f"{name}_step{k}"] = ow.position(h)
+                if self_collision:
+                    out[f"{name}_contacts{k}"] = np.int32(ow.stats()["contacts"])
     return out
 
 
@@ -72,6 +81,7 @@ def ccd_queries(vf, n=256):
 def main():
     pyoracle.build()
     np.savez_compressed(HERE / "c1_sheet32.npz", **c1_sheet())
+    np.savez_compressed(HERE / "c1_sheet32_selfcol.npz", **c1_sheet(self_collision=True))
     out = {}
     for vf, tag in ((True, "vf"), (False, "ee")):
         x, ms, hit, toi, tup = ccd_queries(vf)

@@ -87,6 +87,43 @@ def test_gpu_c1_matches_golden():
 
 
 @pytest.mark.gpu
+def test_gpu_c1_self_collision_matches_golden():
+    """Config 1 as stated (collision and self-collision on): the same bounds
+    against the oracle run with self-collision, and the same contact counts
+    (none in the first ten steps: the pinned sheet swings without touching
+    itself, so broadphase and CCD run and find nothing)."""
+    g = _load("c1_sheet32_selfcol.npz")
+    V, F, P = g["verts"], g["faces"], g["pins"]
+    w = N.World()
+    assert w.init()
+    c = G.C1_CONFIG
+    assert w.set_global_config(N.GlobalConfig(max_inner_iteration=c["max_inner_iteration"],
+                                              admm_abs_tol=c["admm_abs_tol"],
+                                              admm_rel_tol=c["admm_rel_tol"]))
+    assert w.set_solver_options(N.SolverOptions(fixed_linear_rel_tol=c["fixed_linear_rel_tol"]))
+    r, h = w.add_cloth(N.ClothConfig(), N.CollisionConfig(), V, F, P)
+    assert r, r.to_string()
+    x = np.zeros(V.size, np.float32)
+    for k in range(1, max(G.C1_STEPS) + 1):
+        assert w.solver_step()
+        if k not in G.C1_STEPS:
+            continue
+        assert w.step_stats().contacts == int(g[f"o32_contacts{k}"])
+        assert w.get_cloth_position(h, x)
+        xg = x.reshape(-1, 3).astype(np.float64)
+        x32, x64 = g[f"o32_step{k}"], g[f"o64_step{k}"]
+        e32 = np.abs(xg - x32).max()
+        eg64 = np.abs(xg - x64).max()
+        e3264 = np.abs(x32 - x64).max()
+        print(f"step {k}: |gpu-o32| {e32:.2e} |gpu-o64| {eg64:.2e} |o32-o64| {e3264:.2e}")
+        if k == 1:
+            assert e32 < 1e-4
+        if k == 10:
+            assert e32 < 2e-3
+        assert eg64 <= max(3.0 * e3264, 2e-5)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("vf", [True, False])
 def test_gpu_ccd_matches_golden(vf):
     g = _load("ccd_queries.npz")
