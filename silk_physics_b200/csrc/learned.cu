@@ -1,9 +1,11 @@
-// Learned CG warm start: feature extraction, the MLP forward on the tensor
-// cores (mma.sync m16n8k16, BF16 operands, FP32 accumulation; the whole MLP
-// of 16 samples stays in one warp's registers, each layer's accumulators
-// becoming the next layer's A fragments), the backward pass (FP32, straight
-// through the BF16 rounding) with deterministic per-block gradient partials,
-// and the Adam update.  No counterpart in the reference.
+// Learned CG warm start: feature extraction, the inference forward on the
+// 5th-generation tensor cores (tcgen05.mma, accumulators in tensor memory),
+// the training forward on mma.sync m16n8k16 (BF16 operands, FP32
+// accumulation; the whole MLP of 16 samples stays in one warp's registers,
+// each layer's accumulators becoming the next layer's A fragments, the
+// pre-activations kept for the backward pass), the backward pass (FP32,
+// straight through the BF16 rounding) with deterministic per-block gradient
+// partials, and the Adam update.  No counterpart in the reference.
 #include <cuda_bf16.h>
 
 #include "learned.cuh"
@@ -174,27 +176,243 @@ __device__ void forward_tile(const SmemModel& s, const float* __restrict__ feat,
   }
 }
 
-__global__ void __launch_bounds__(kFwdThreads) mlp_forward_kernel(MlpDev m,
-                                                                  const float* __restrict__ feat,
-                                                                  int n, float* __restrict__ out) {
-  __shared__ SmemModel s;
-  load_model(m, s);
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const int warp = blockIdx.x * kFwdWarps + (threadIdx.x >> 5);
-  const int nwarps = gridDim.x * kFwdWarps;
-  for (int s0 = 16 * warp; s0 < n; s0 += 16 * nwarps) {
-    float o[4];
-    forward_tile(s, feat, nullptr, s0, n, nullptr, o);
-    if (t < 2) {
-      const int ra = s0 + g, rb = s0 + g + 8;
+// ---------------------------------------------------------------------------
+// Inference forward on the 5th-generation tensor cores: a CTA of 128 threads
+// carries tiles of 128 samples through the four layers as
+// tcgen05.mma.cta_group::1.kind::f16 products (M = 128, BF16 operands from
+// shared memory, FP32 accumulators in 64 tensor-memory columns), one thread
+// issuing each layer's K / 16 products and committing them to an mbarrier;
+// the four warps then read their 32 accumulator lanes (tcgen05.ld 32x32b),
+// add the bias, apply GELU and write the next layer's A operand as BF16.
+// Operands are K-major without swizzle: 8 x 8 BF16 core matrices of 128 B,
+// adjacent along K (leading byte offset 128) and K / 8 apart along M or N
+// (stride byte offset).  The same rounding points as forward_tile (BF16
+// layer inputs and weights, FP32 sums, bias added to the sum); the order of
+// the FP32 additions inside a product is the tensor core's.
+constexpr int kTcRows = 128;
+constexpr int kTcCols = 64;                 // tensor-memory columns (N <= 64)
+constexpr int kTcOutN = 16;                 // output layer padded to N = 16
+constexpr long long kTcWaitSpins = 1 << 20; // mbarrier polls before giving up
+
+struct TcSmem {
+  alignas(128) __nv_bfloat16 w1[kMlpH * kMlpK];      // B of layer 1: N 64, K 16
+  alignas(128) __nv_bfloat16 w2[kMlpH * kMlpH];      // N 64, K 64
+  alignas(128) __nv_bfloat16 w3[kMlpH * kMlpH];
+  alignas(128) __nv_bfloat16 w4[kTcOutN * kMlpH];    // N 16 (8..15 zero), K 64
+  alignas(128) __nv_bfloat16 a[kTcRows * kMlpH];     // A: M 128, K 16 or 64
+  float bias[3 * kMlpH + kMlpKOut];
+  float mean[kMlpK], inv_std[kMlpK];
+  alignas(8) uint64_t bar;
+  unsigned tmem;
+};
+
+// Element index of (row r, column k) in a K-major core-matrix layout of
+// width K.
+__device__ __forceinline__ int cm_index(int r, int k, int K) {
+  return (((r >> 3) * (K >> 3) + (k >> 3)) << 6) + ((r & 7) << 3) + (k & 7);
+}
+__device__ __forceinline__ unsigned su32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+// Shared-memory matrix descriptor (no swizzle, descriptor version 1).
+__device__ __forceinline__ uint64_t umma_desc(const void* p, unsigned lbo, unsigned sbo) {
+  return (uint64_t)((su32(p) & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// Instruction descriptor: F32 accumulator, BF16 A and B, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(m >> 4) << 24);
+}
+__device__ __forceinline__ void umma_bf16(unsigned d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                          unsigned accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   su32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool bar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(su32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, unsigned parity) {
+  for (long long i = 0; i < kTcWaitSpins; ++i)
+    if (bar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void proxy_fence() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// 16 accumulator columns of this thread's lane; the wait is in the same
+// statement, so no use of the outputs is scheduled before it.
+__device__ __forceinline__ void tc_ld16(unsigned taddr, float (&v)[16]) {
+  unsigned u[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];\n"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]),
+        "=r"(u[7]), "=r"(u[8]), "=r"(u[9]), "=r"(u[10]), "=r"(u[11]), "=r"(u[12]), "=r"(u[13]),
+        "=r"(u[14]), "=r"(u[15])
+      : "r"(taddr)
+      : "memory");
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        int col = 2 * t + q;
-        if (col >= kMlpOut) continue;
-        if (ra < n) out[(size_t)ra * kMlpOut + col] = o[q];
-        if (rb < n) out[(size_t)rb * kMlpOut + col] = o[2 + q];
+  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(u[j]);
+}
+
+__global__ void __launch_bounds__(kTcRows) mlp_forward_tc_kernel(MlpDev m,
+                                                                 const float* __restrict__ feat,
+                                                                 int n, float* __restrict__ out,
+                                                                 int* __restrict__ fail) {
+  extern __shared__ __align__(128) unsigned char tc_raw[];
+  TcSmem& s = *reinterpret_cast<TcSmem*>(tc_raw);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  // Weights as K-major B operands (B(n, k) = W[k][n]), biases, statistics.
+  const float* P = m.params;
+  for (int i = tid; i < kMlpH * kMlpK; i += kTcRows) {
+    const int nn = i / kMlpK, k = i % kMlpK;
+    s.w1[cm_index(nn, k, kMlpK)] = __float2bfloat16_rn(P[kOffW1 + k * kMlpH + nn]);
+  }
+  for (int i = tid; i < kMlpH * kMlpH; i += kTcRows) {
+    const int nn = i / kMlpH, k = i % kMlpH;
+    s.w2[cm_index(nn, k, kMlpH)] = __float2bfloat16_rn(P[kOffW2 + k * kMlpH + nn]);
+    s.w3[cm_index(nn, k, kMlpH)] = __float2bfloat16_rn(P[kOffW3 + k * kMlpH + nn]);
+  }
+  for (int i = tid; i < kTcOutN * kMlpH; i += kTcRows) {
+    const int nn = i / kMlpH, k = i % kMlpH;
+    s.w4[cm_index(nn, k, kMlpH)] =
+        __float2bfloat16_rn(nn < kMlpKOut ? P[kOffW4 + k * kMlpKOut + nn] : 0.0f);
+  }
+  for (int i = tid; i < kMlpH; i += kTcRows) {
+    s.bias[i] = P[kOffB1 + i];
+    s.bias[kMlpH + i] = P[kOffB2 + i];
+    s.bias[2 * kMlpH + i] = P[kOffB3 + i];
+  }
+  if (tid < kMlpKOut) s.bias[3 * kMlpH + tid] = P[kOffB4 + tid];
+  if (tid < kMlpK) {
+    s.mean[tid] = P[kOffMean + tid];
+    s.inv_std[tid] = 1.0f / P[kOffStd + tid];
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&s.bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     su32(&s.tmem)),
+                 "r"(kTcCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  proxy_fence();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const unsigned tmem = s.tmem;
+  const unsigned taddr = tmem + ((unsigned)(warp * 32) << 16);  // this warp's 32 lanes
+  unsigned phase = 0;
+  bool ok = true;
+  // One layer's products: D (128 x N) = A (128 x K) B^T, then wait for them.
+  auto layer_mma = [&](const __nv_bfloat16* w, int K, int N) {
+    if (tid == 0) {
+      tc_fence_after();
+      const unsigned sbo = (unsigned)(K / 8) * 128u;
+      for (int kc = 0; kc < K / 16; ++kc)
+        umma_bf16(tmem, umma_desc(s.a + kc * 128, 128u, sbo), umma_desc(w + kc * 128, 128u, sbo),
+                  umma_idesc(kTcRows, N), kc > 0 ? 1u : 0u);
+      umma_commit(&s.bar);
+    }
+    const bool done = bar_wait(&s.bar, phase);
+    phase ^= 1u;
+    tc_fence_after();
+    return __syncthreads_and(done) != 0;
+  };
+  const int ntiles = (n + kTcRows - 1) / kTcRows;
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const int r = tid, row = tile * kTcRows + r;
+    // Layer-1 input: normalised features in BF16 (rows past n are zero).
+    {
+      float x[kMlpK];
+#pragma unroll
+      for (int c = 0; c < kMlpK; ++c)
+        x[c] = row < n ? (feat[(size_t)row * kMlpK + c] - s.mean[c]) * s.inv_std[c] : 0.0f;
+#pragma unroll
+      for (int c0 = 0; c0 < kMlpK; c0 += 8) {
+        uint4 q;
+        q.x = pack_bf16(x[c0], x[c0 + 1]);
+        q.y = pack_bf16(x[c0 + 2], x[c0 + 3]);
+        q.z = pack_bf16(x[c0 + 4], x[c0 + 5]);
+        q.w = pack_bf16(x[c0 + 6], x[c0 + 7]);
+        *reinterpret_cast<uint4*>(s.a + cm_index(r, c0, kMlpK)) = q;
       }
     }
+    proxy_fence();
+    __syncthreads();
+    const __nv_bfloat16* ws[3] = {s.w1, s.w2, s.w3};
+    for (int l = 0; l < 3 && ok; ++l) {
+      ok = layer_mma(ws[l], l == 0 ? kMlpK : kMlpH, kMlpH);
+      if (!ok) break;
+      // Bias, GELU, BF16: the next layer's A (K = 64) from this thread's row.
+#pragma unroll
+      for (int c0 = 0; c0 < kMlpH; c0 += 16) {
+        float v[16];
+        tc_ld16(taddr + c0, v);
+        uint4 q[2];
+        uint32_t* qw = reinterpret_cast<uint32_t*>(q);
+#pragma unroll
+        for (int j = 0; j < 16; j += 2)
+          qw[j / 2] = pack_bf16(gelu(v[j] + s.bias[l * kMlpH + c0 + j]),
+                                gelu(v[j + 1] + s.bias[l * kMlpH + c0 + j + 1]));
+        *reinterpret_cast<uint4*>(s.a + cm_index(r, c0, kMlpH)) = q[0];
+        *reinterpret_cast<uint4*>(s.a + cm_index(r, c0 + 8, kMlpH)) = q[1];
+      }
+      tc_fence_before();
+      proxy_fence();
+      __syncthreads();
+    }
+    if (!ok) break;
+    ok = layer_mma(s.w4, kMlpH, kTcOutN);
+    if (!ok) break;
+    float v[16];
+    tc_ld16(taddr, v);
+    if (row < n)
+#pragma unroll
+      for (int c = 0; c < kMlpOut; ++c)
+        out[(size_t)row * kMlpOut + c] = v[c] + s.bias[3 * kMlpH + c];
+    tc_fence_before();
+    __syncthreads();  // every lane's accumulators read before the next tile's products
+  }
+  if (!ok) {
+    // A product did not complete in time: report it and wait (bounded) for
+    // the products still in flight before the tensor memory is freed.
+    if (tid == 0 && fail) atomicOr(fail, kFailMlpWait);
+    bar_wait(&s.bar, phase ^ 1u);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTcCols)
+                 : "memory");
   }
 }
 
@@ -576,7 +794,15 @@ void mlp_prepare(const float* params, uint32_t* frag, cudaStream_t st) {
 
 void mlp_forward(const MlpDev& m, const float* feat, int n, float* out, cudaStream_t st) {
   if (n <= 0) return;
-  mlp_forward_kernel<<<fwd_grid(n), kFwdThreads, 0, st>>>(m, feat, n, out);
+  static const int max_grid = [] {
+    int dev = 0, sms = 0;
+    CUDA_CHECK(cudaGetDevice(&dev));
+    CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return 4 * sms;  // 128 threads and ~29 KB of shared memory per CTA; 4 x 64 TMEM columns per SM
+  }();
+  const int tiles = (n + kTcRows - 1) / kTcRows;
+  mlp_forward_tc_kernel<<<tiles < max_grid ? tiles : max_grid, kTcRows, sizeof(TcSmem), st>>>(
+      m, feat, n, out, m.fail);
   SILK_LAUNCHED();
 }
 

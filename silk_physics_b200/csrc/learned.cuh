@@ -38,7 +38,12 @@ constexpr int kMlpFragWords = kMlpTiles * 32 * 2;  // uint32 words
 struct MlpDev {
   const float* params = nullptr;   // kMlpParams
   const uint32_t* frag = nullptr;  // kMlpFragWords
+  int* fail = nullptr;             // kFailMlpWait is set here when a tensor-core wait gives up
 };
+
+// Bit of the solver's failure word: a tensor-core product of the inference
+// forward did not complete within its bounded wait.
+constexpr int kFailMlpWait = 8;
 
 // Build the BF16 fragments of a parameter vector (device pointers).
 void mlp_prepare(const float* params, uint32_t* frag, cudaStream_t st);

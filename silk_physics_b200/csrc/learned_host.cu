@@ -53,9 +53,16 @@ void mlp_forward_host(const float* params, const float* feat, int64_t n, float* 
   MlpBuffers b;
   b.load(params, feat, nullptr, (int)n, st);
   b.out.alloc((size_t)kMlpOut * n);
-  mlp_prepare(b.params.p, b.frag.p, st);
-  mlp_forward(b.dev(), b.feat.p, (int)n, b.out.p, st);
+  DevBuf<int> fail;
+  fail.alloc(1);
+  fail.zero(st);
+  MlpDev m = b.dev();
+  m.fail = fail.p;
+  mlp_forward(m, b.feat.p, (int)n, b.out.p, st);
   CUDA_CHECK(cudaMemcpy(out, b.out.p, (size_t)kMlpOut * n * sizeof(float), cudaMemcpyDeviceToHost));
+  int f = 0;
+  CUDA_CHECK(cudaMemcpy(&f, fail.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (f) throw CudaError("tensor-core wait gave up");
 }
 
 void mlp_loss_grad_host(const float* params, const float* feat, const float* tgt, int64_t n,

@@ -1248,7 +1248,7 @@ bool World::admm_solve() {
       // x holds x_(it-1); slots (it-1) % 3 and (it-2) % 3 hold x_(it-2) and
       // x_(it-3) from the previous iterations.
       if (it >= 3) {
-        MlpDev m{iter_model ? mlp2_params.p : nullptr, mlp2_frag.p};
+        MlpDev m{iter_model ? mlp2_params.p : nullptr, mlp2_frag.p, cg_fail.p};
         iterate_predict(m, nv_total, x.p, iter_ring[(it - 1) % 3]->p, iter_ring[(it - 2) % 3]->p,
                         pin_flag.p, ring_off.p, ring.p, iter_sigma.p, iter_feat.p, iter_out.p,
                         iter_pred.p, st);
@@ -1413,7 +1413,7 @@ silk_status World::solver_step() {
         warm_features(nv, outer.p, hist1.p, hist2.p, ypred.p, pin_flag.p, ring_off.p, ring.p,
                       1.0f / sigma, warm_feat.p, st);
         if (has_model && opt.learned_warm_start) {
-          MlpDev m{mlp_params.p, mlp_frag.p};
+          MlpDev m{mlp_params.p, mlp_frag.p, cg_fail.p};
           warm_predict(m, nv, warm_feat.p, ypred.p, sigma, mlp_out.p, xpred.p, st);
         }
       }
@@ -1424,7 +1424,8 @@ silk_status World::solver_step() {
         last_error = (f & kFailMasPivot) ? "MAS bank inverse failed: zero or non-finite pivot"
                      : (f & kFailBarrier) ? "CG barrier wait gave up"
                      : (f & kFailContactWait) ? "contact Gauss-Seidel copy wait gave up"
-                                              : "solver diverged";
+                     : (f & kFailMlpWait) ? "learned warm start tensor-core wait gave up"
+                                          : "solver diverged";
         if (f) cg_fail.zero(st);
         return SILK_ERR_ITERATIVE_SOLVE_FAIL;
       }

@@ -167,13 +167,17 @@ def test_plain_and_learned_bf16_contact_sets_agree(scene_name):
     keys (same positions in); the contacts activated after each CCD rollback
     depend on where the rollback lands, which FP32 rounding moves: both forms
     stop the CG at the same relative residual but not at the same bits.  The
-    rounding baseline is the plain method run by another CG kernel form (the
-    streaming kernel: the same iteration with FP32 sums in another order).
-    Bound: the learned + BF16 form's key set overlaps the plain one's
-    (Jaccard index) no less than the baseline's does, less 0.05; the
-    rollback counts differ by at most 2; positions within the contact
+    rounding baselines are the plain method run by another CG kernel form (the
+    streaming kernel: the same iteration with FP32 sums in another order) and
+    the BF16-MAS form alone (the same iteration with the inverses rounded to
+    BF16).  Bound: the learned + BF16 form's key set overlaps the plain one's
+    (Jaccard index) no less than the lower of the baselines does, less 0.05;
+    the rollback counts differ by at most 2; positions within the contact
     tolerance.  (On the first contact step of the 100K-vertex drape, over
-    twenty rollbacks, the baseline itself overlaps by well under 1.)"""
+    twenty rollbacks, the baselines themselves overlap by well under 1, and
+    any rounding-level change of the solve, such as the order of the FP32
+    additions inside a tensor-core product of the learned start, moves the
+    overlap by a few hundredths.)"""
     if scene_name == "c2":
         g = _fixture("c2_contact")
         scene = S.c2_scene()
@@ -183,7 +187,7 @@ def test_plain_and_learned_bf16_contact_sets_agree(scene_name):
         x0, v0 = S.free_fall_state(scene[0], 8)
     out = {}
     forms = (("plain", False, False, 0), ("plain_streaming", False, False, 1),
-             ("learned_bf16", True, True, 0))
+             ("bf16", True, False, 0), ("learned_bf16", True, True, 0))
     for form, bf16, learned, cg_form in forms:
         w, h = _world(scene, bf16=bf16, learned=learned)
         if cg_form:
@@ -201,12 +205,15 @@ def test_plain_and_learned_bf16_contact_sets_agree(scene_name):
 
     kp, xp, sp = out["plain"]
     ks, _, ss = out["plain_streaming"]
+    kb, _, sb = out["bf16"]
     kl, xl, sl = out["learned_bf16"]
-    j_base, j_learned = jaccard(kp, ks), jaccard(kp, kl)
-    print(f"{scene_name}: contacts {len(kp)} / {len(ks)} / {len(kl)} (plain / streaming / "
-          f"learned+BF16), Jaccard to plain: streaming {j_base:.4f}, learned+BF16 "
-          f"{j_learned:.4f}; outer {sp.outer_iterations} / {ss.outer_iterations} / "
-          f"{sl.outer_iterations}; |dx| = {np.abs(xp - xl).max():.2e}; learned starts "
+    j_stream, j_bf16, j_learned = jaccard(kp, ks), jaccard(kp, kb), jaccard(kp, kl)
+    j_base = min(j_stream, j_bf16)
+    print(f"{scene_name}: contacts {len(kp)} / {len(ks)} / {len(kb)} / {len(kl)} (plain / "
+          f"streaming / BF16 / learned+BF16), Jaccard to plain: streaming {j_stream:.4f}, "
+          f"BF16 {j_bf16:.4f}, learned+BF16 {j_learned:.4f}; outer {sp.outer_iterations} / "
+          f"{ss.outer_iterations} / {sb.outer_iterations} / {sl.outer_iterations}; "
+          f"|dx| = {np.abs(xp - xl).max():.2e}; learned starts "
           f"{sl.learned_starts} first / {sl.learned_iterate_starts} iterate")
     assert len(kp) > 0
     assert j_learned >= j_base - 0.05

@@ -83,6 +83,27 @@ def test_forward_matches_oracle():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 127, 129, 200_003])
+def test_forward_tiles_match_oracle(n):
+    """The inference forward (tcgen05.mma, 128-sample tiles, accumulators in
+    tensor memory; persistent CTAs take several tiles once n passes 4 tiles
+    per SM): every size against the oracle, and a sample's output does not
+    depend on the batch it is in (tiles are independent, so the first rows
+    of a larger batch are bit-identical to the same rows alone)."""
+    p, f, _ = _random_case(n, 5)
+    out = N.mlp_forward(p, f)
+    P = M.unpack(p)
+    ref, _ = M.forward(P, (f.astype(np.float64) - P["feat_mean"]) / P["feat_std"])
+    ref = ref[:, :3]
+    err = np.linalg.norm(out - ref) / np.linalg.norm(ref)
+    print(f"n={n}: relative error {err:.2e}, max abs {np.abs(out - ref).max():.2e}")
+    assert np.isfinite(out).all()
+    assert err < FWD_TOL
+    head = min(n, 100)
+    np.testing.assert_array_equal(N.mlp_forward(p, f[:head]), out[:head])
+
+
+@pytest.mark.gpu
 def test_loss_gradient_matches_oracle():
     p, f, t = _random_case(3000, 2)
     loss, grad = N.mlp_loss_grad(p, f, t)
