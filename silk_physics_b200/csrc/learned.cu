@@ -1,9 +1,7 @@
-// Learned CG warm start: feature extraction, the inference forward on the
-// 5th-generation tensor cores (tcgen05.mma, accumulators in tensor memory),
-// the training forward on mma.sync m16n8k16 (BF16 operands, FP32
-// accumulation; the whole MLP of 16 samples stays in one warp's registers,
-// each layer's accumulators becoming the next layer's A fragments, the
-// pre-activations kept for the backward pass), the backward pass (FP32,
+// Learned CG warm start: feature extraction, the forward on the
+// 5th-generation tensor cores (tcgen05.mma, BF16 operands in shared memory,
+// FP32 accumulators in tensor memory; for training it also keeps the
+// pre-activations and the output gradient), the backward pass (FP32,
 // straight through the BF16 rounding) with deterministic per-block gradient
 // partials, and the Adam update.  No counterpart in the reference.
 #include <cuda_bf16.h>
@@ -14,8 +12,6 @@ namespace silkb {
 
 namespace {
 
-constexpr int kFwdWarps = 4;
-constexpr int kFwdThreads = 32 * kFwdWarps;
 constexpr int kBwdThreads = 256;
 constexpr int kBwdTile = 32;  // samples per backward tile
 constexpr int kBwdBlocks = 296;
@@ -35,174 +31,45 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
          ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(hi)) << 16);
 }
 
-__device__ __forceinline__ void mma(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
-                                    uint32_t a3, uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, "
-      "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
-// Layer table: weight offset, K, N, first fragment tile.
-struct LayerDesc {
-  int w, k, n, tile;
-};
-__host__ __device__ constexpr LayerDesc layer(int l) {
-  return l == 0   ? LayerDesc{kOffW1, kMlpK, kMlpH, 0}
-         : l == 1 ? LayerDesc{kOffW2, kMlpH, kMlpH, kTilesL1}
-         : l == 2 ? LayerDesc{kOffW3, kMlpH, kMlpH, kTilesL1 + kTilesL2}
-                  : LayerDesc{kOffW4, kMlpH, kMlpKOut, kTilesL1 + kTilesL2 + kTilesL3};
-}
-
-// B fragment of tile (kt, nt) for lane (g, t): W[16kt + 2t (+1)][8nt + g] and
-// W[16kt + 2t + 8 (+9)][8nt + g], packed BF16 pairs.
-__global__ void mlp_prepare_kernel(const float* __restrict__ p, uint32_t* __restrict__ frag) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= kMlpTiles * 32) return;
-  int tile = i / 32, lane = i % 32;
-  int l = 0;
-  while (l < 3 && tile >= layer(l + 1).tile) ++l;
-  LayerDesc d = layer(l);
-  int local = tile - d.tile;
-  int ntiles_n = d.n / 8;
-  int kt = local / ntiles_n, nt = local % ntiles_n;
-  int g = lane >> 2, t = lane & 3;
-  const float* W = p + d.w;
-  int col = 8 * nt + g;
-  int r0 = 16 * kt + 2 * t;
-  frag[2 * i] = pack_bf16(W[r0 * d.n + col], W[(r0 + 1) * d.n + col]);
-  frag[2 * i + 1] = pack_bf16(W[(r0 + 8) * d.n + col], W[(r0 + 9) * d.n + col]);
-}
-
-struct SmemModel {
-  uint2 frag[kMlpTiles * 32];
-  float bias[3 * kMlpH + kMlpKOut];
-  float mean[kMlpK], inv_std[kMlpK], out_scale[kMlpKOut];
-};
-
-__device__ void load_model(const MlpDev& m, SmemModel& s) {
-  const uint2* src = reinterpret_cast<const uint2*>(m.frag);
-  for (int i = threadIdx.x; i < kMlpTiles * 32; i += blockDim.x) s.frag[i] = src[i];
-  for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
-    s.bias[i] = m.params[kOffB1 + i];
-    s.bias[kMlpH + i] = m.params[kOffB2 + i];
-    s.bias[2 * kMlpH + i] = m.params[kOffB3 + i];
-  }
-  for (int i = threadIdx.x; i < kMlpKOut; i += blockDim.x) {
-    s.bias[3 * kMlpH + i] = m.params[kOffB4 + i];
-    s.out_scale[i] = m.params[kOffOutScale + i];
-  }
-  for (int i = threadIdx.x; i < kMlpK; i += blockDim.x) {
-    s.mean[i] = m.params[kOffMean + i];
-    s.inv_std[i] = 1.0f / m.params[kOffStd + i];
-  }
-  __syncthreads();
-}
-
-// Forward of 16 samples (rows) by one warp.  Row g and g + 8 of the tile are
-// samples s0 + g and s0 + g + 8 (rows >= n are zero input).  Returns the output
-// accumulators c (rows g, g+8; columns 2t, 2t+1).  With z != null the hidden
-// pre-activations are stored (z[l][row][64], stride n).
-__device__ void forward_tile(const SmemModel& s, const float* __restrict__ feat,
-                             const int* __restrict__ index, int s0, int n, float* z,
-                             float (&out)[4]) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const int ra = s0 + g, rb = s0 + g + 8;
-  const int ia = ra < n ? (index ? index[ra] : ra) : -1;
-  const int ib = rb < n ? (index ? index[rb] : rb) : -1;
-  auto xn = [&](int src, int c) -> float {
-    if (src < 0) return 0.0f;
-    return (feat[(size_t)src * kMlpK + c] - s.mean[c]) * s.inv_std[c];
-  };
-  // Layer-1 A fragment (K = 16).
-  uint32_t a[4][4];
-  a[0][0] = pack_bf16(xn(ia, 2 * t), xn(ia, 2 * t + 1));
-  a[0][1] = pack_bf16(xn(ib, 2 * t), xn(ib, 2 * t + 1));
-  a[0][2] = pack_bf16(xn(ia, 2 * t + 8), xn(ia, 2 * t + 9));
-  a[0][3] = pack_bf16(xn(ib, 2 * t + 8), xn(ib, 2 * t + 9));
-  int kts = 1;
-  float c[8][4];
-#pragma unroll
-  for (int l = 0; l < 3; ++l) {
-    const LayerDesc d = layer(l);
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      float b0 = s.bias[l * kMlpH + 8 * nt + 2 * t], b1 = s.bias[l * kMlpH + 8 * nt + 2 * t + 1];
-      c[nt][0] = b0;
-      c[nt][1] = b1;
-      c[nt][2] = b0;
-      c[nt][3] = b1;
-    }
-#pragma unroll
-    for (int kt = 0; kt < 4; ++kt) {
-      if (kt >= kts) break;
-#pragma unroll
-      for (int nt = 0; nt < 8; ++nt) {
-        uint2 b = s.frag[(d.tile + kt * 8 + nt) * 32 + lane];
-        mma(c[nt], a[kt][0], a[kt][1], a[kt][2], a[kt][3], b.x, b.y);
-      }
-    }
-    if (z) {
-      float* zl = z + (size_t)l * n * kMlpH;
-#pragma unroll
-      for (int nt = 0; nt < 8; ++nt) {
-        int col = 8 * nt + 2 * t;
-        if (ra < n) *reinterpret_cast<float2*>(zl + (size_t)ra * kMlpH + col) = make_float2(c[nt][0], c[nt][1]);
-        if (rb < n) *reinterpret_cast<float2*>(zl + (size_t)rb * kMlpH + col) = make_float2(c[nt][2], c[nt][3]);
-      }
-    }
-    // GELU; the accumulators of output tiles 2kt and 2kt+1 are the A
-    // fragment of the next layer's k-tile kt.
-#pragma unroll
-    for (int kt = 0; kt < 4; ++kt) {
-      a[kt][0] = pack_bf16(gelu(c[2 * kt][0]), gelu(c[2 * kt][1]));
-      a[kt][1] = pack_bf16(gelu(c[2 * kt][2]), gelu(c[2 * kt][3]));
-      a[kt][2] = pack_bf16(gelu(c[2 * kt + 1][0]), gelu(c[2 * kt + 1][1]));
-      a[kt][3] = pack_bf16(gelu(c[2 * kt + 1][2]), gelu(c[2 * kt + 1][3]));
-    }
-    kts = 4;
-  }
-  const LayerDesc d = layer(3);
-  float b0 = s.bias[3 * kMlpH + 2 * t], b1 = s.bias[3 * kMlpH + 2 * t + 1];
-  out[0] = b0;
-  out[1] = b1;
-  out[2] = b0;
-  out[3] = b1;
-#pragma unroll
-  for (int kt = 0; kt < 4; ++kt) {
-    uint2 b = s.frag[(d.tile + kt) * 32 + lane];
-    mma(out, a[kt][0], a[kt][1], a[kt][2], a[kt][3], b.x, b.y);
-  }
-}
-
 // ---------------------------------------------------------------------------
-// Inference forward on the 5th-generation tensor cores: a CTA of 128 threads
-// carries tiles of 128 samples through the four layers as
+// Forward on the 5th-generation tensor cores: a CTA of 256 threads carries
+// tiles of 128 samples through the four layers as
 // tcgen05.mma.cta_group::1.kind::f16 products (M = 128, BF16 operands from
 // shared memory, FP32 accumulators in 64 tensor-memory columns), one thread
 // issuing each layer's K / 16 products and committing them to an mbarrier;
-// the four warps then read their 32 accumulator lanes (tcgen05.ld 32x32b),
-// add the bias, apply GELU and write the next layer's A operand as BF16.
+// warps w and w + 4 then read the 32 accumulator lanes of quarter w % 4
+// (tcgen05.ld 32x32b), each half of the columns, add the bias, apply GELU and
+// write the next layer's A operand as BF16.
 // Operands are K-major without swizzle: 8 x 8 BF16 core matrices of 128 B,
 // adjacent along K (leading byte offset 128) and K / 8 apart along M or N
-// (stride byte offset).  The same rounding points as forward_tile (BF16
-// layer inputs and weights, FP32 sums, bias added to the sum); the order of
-// the FP32 additions inside a product is the tensor core's.
+// (stride byte offset).  The rounding points of the model (BF16
+// layer inputs and weights, FP32 sums, bias added to the sum, as the CPU
+// oracle's forward); the order of the FP32 additions inside a product is the
+// tensor core's.
 constexpr int kTcRows = 128;
+constexpr int kTcThreads = 256;             // two warps per 32-lane quarter of the accumulators
 constexpr int kTcCols = 64;                 // tensor-memory columns (N <= 64)
 constexpr int kTcOutN = 16;                 // output layer padded to N = 16
 constexpr long long kTcWaitSpins = 1 << 20; // mbarrier polls before giving up
 
+// The B operands of the four layers, in the order and layout they take in
+// shared memory (the weight image, prepared once per parameter vector).
+struct TcWeights {
+  __nv_bfloat16 w1[kMlpH * kMlpK];      // B of layer 1: N 64, K 16
+  __nv_bfloat16 w2[kMlpH * kMlpH];      // N 64, K 64
+  __nv_bfloat16 w3[kMlpH * kMlpH];
+  __nv_bfloat16 w4[kTcOutN * kMlpH];    // N 16 (8..15 zero), K 64
+};
+static_assert(sizeof(TcWeights) % 128 == 0 && sizeof(TcWeights) == 2 * kMlpWeightImage,
+              "one bulk copy of 16-byte units");
+
 struct TcSmem {
-  alignas(128) __nv_bfloat16 w1[kMlpH * kMlpK];      // B of layer 1: N 64, K 16
-  alignas(128) __nv_bfloat16 w2[kMlpH * kMlpH];      // N 64, K 64
-  alignas(128) __nv_bfloat16 w3[kMlpH * kMlpH];
-  alignas(128) __nv_bfloat16 w4[kTcOutN * kMlpH];    // N 16 (8..15 zero), K 64
+  alignas(128) TcWeights w;
   alignas(128) __nv_bfloat16 a[kTcRows * kMlpH];     // A: M 128, K 16 or 64
   float bias[3 * kMlpH + kMlpKOut];
   float mean[kMlpK], inv_std[kMlpK];
-  alignas(8) uint64_t bar;
+  alignas(8) uint64_t bar;   // the layers' products
+  alignas(8) uint64_t wbar;  // the weight image's bulk copy
   unsigned tmem;
 };
 
@@ -278,30 +145,57 @@ __device__ __forceinline__ void tc_ld16(unsigned taddr, float (&v)[16]) {
   for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(u[j]);
 }
 
-__global__ void __launch_bounds__(kTcRows) mlp_forward_tc_kernel(MlpDev m,
-                                                                 const float* __restrict__ feat,
-                                                                 int n, float* __restrict__ out,
-                                                                 int* __restrict__ fail) {
+// kTrain: rows index[r] (or r) of feat / t_hat, the hidden pre-activations
+// stored (z[l][r][64], stride n), the output gradient d4 = 2 (o - t) / (3n)
+// (n x 8, columns >= 3 zero) and a per-block loss partial instead of out.
+// Weight image: B(n, k) = W[k][n] of each layer in BF16, K-major core
+// matrices (the output layer's columns 8..15 zero).
+__global__ void mlp_image_kernel(const float* __restrict__ P, TcWeights* __restrict__ img) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < kMlpH * kMlpK) {
+    const int nn = i / kMlpK, k = i % kMlpK;
+    img->w1[cm_index(nn, k, kMlpK)] = __float2bfloat16_rn(P[kOffW1 + k * kMlpH + nn]);
+  }
+  if (i < kMlpH * kMlpH) {
+    const int nn = i / kMlpH, k = i % kMlpH;
+    img->w2[cm_index(nn, k, kMlpH)] = __float2bfloat16_rn(P[kOffW2 + k * kMlpH + nn]);
+    img->w3[cm_index(nn, k, kMlpH)] = __float2bfloat16_rn(P[kOffW3 + k * kMlpH + nn]);
+  }
+  if (i < kTcOutN * kMlpH) {
+    const int nn = i / kMlpH, k = i % kMlpH;
+    img->w4[cm_index(nn, k, kMlpH)] =
+        __float2bfloat16_rn(nn < kMlpKOut ? P[kOffW4 + k * kMlpKOut + nn] : 0.0f);
+  }
+}
+
+// kTrain: rows index[r] (or r) of feat / t_hat, the hidden pre-activations
+// stored (z[l][r][64], stride n), the output gradient d4 = 2 (o - t) / (3n)
+// (n x 8, columns >= 3 zero) and a per-block loss partial instead of out.
+template <bool kTrain>
+__global__ void __launch_bounds__(kTcThreads) mlp_forward_tc_kernel(
+    MlpDev m, const float* __restrict__ feat, int n, float* __restrict__ out,
+    int* __restrict__ fail, const float* __restrict__ t_hat, const int* __restrict__ index,
+    float* __restrict__ z, float* __restrict__ d4, double* __restrict__ loss_part) {
   extern __shared__ __align__(128) unsigned char tc_raw[];
   TcSmem& s = *reinterpret_cast<TcSmem*>(tc_raw);
   const int tid = threadIdx.x, warp = tid >> 5;
-  // Weights as K-major B operands (B(n, k) = W[k][n]), biases, statistics.
+  const int quarter = warp & 3, half = warp >> 2;  // accumulator lanes and column half
+  // The weight image arrives by one bulk copy; biases and statistics by
+  // plain loads meanwhile.
   const float* P = m.params;
-  for (int i = tid; i < kMlpH * kMlpK; i += kTcRows) {
-    const int nn = i / kMlpK, k = i % kMlpK;
-    s.w1[cm_index(nn, k, kMlpK)] = __float2bfloat16_rn(P[kOffW1 + k * kMlpH + nn]);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&s.bar)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&s.wbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(&s.wbar)),
+                 "r"((unsigned)sizeof(TcWeights))
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(su32(&s.w)), "l"(m.image), "r"((unsigned)sizeof(TcWeights)), "r"(su32(&s.wbar))
+        : "memory");
   }
-  for (int i = tid; i < kMlpH * kMlpH; i += kTcRows) {
-    const int nn = i / kMlpH, k = i % kMlpH;
-    s.w2[cm_index(nn, k, kMlpH)] = __float2bfloat16_rn(P[kOffW2 + k * kMlpH + nn]);
-    s.w3[cm_index(nn, k, kMlpH)] = __float2bfloat16_rn(P[kOffW3 + k * kMlpH + nn]);
-  }
-  for (int i = tid; i < kTcOutN * kMlpH; i += kTcRows) {
-    const int nn = i / kMlpH, k = i % kMlpH;
-    s.w4[cm_index(nn, k, kMlpH)] =
-        __float2bfloat16_rn(nn < kMlpKOut ? P[kOffW4 + k * kMlpKOut + nn] : 0.0f);
-  }
-  for (int i = tid; i < kMlpH; i += kTcRows) {
+  for (int i = tid; i < kMlpH; i += kTcThreads) {
     s.bias[i] = P[kOffB1 + i];
     s.bias[kMlpH + i] = P[kOffB2 + i];
     s.bias[2 * kMlpH + i] = P[kOffB3 + i];
@@ -310,10 +204,6 @@ __global__ void __launch_bounds__(kTcRows) mlp_forward_tc_kernel(MlpDev m,
   if (tid < kMlpK) {
     s.mean[tid] = P[kOffMean + tid];
     s.inv_std[tid] = 1.0f / P[kOffStd + tid];
-  }
-  if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&s.bar)) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -326,10 +216,10 @@ __global__ void __launch_bounds__(kTcRows) mlp_forward_tc_kernel(MlpDev m,
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
+  bool ok = __syncthreads_and(bar_wait(&s.wbar, 0u)) != 0;
   const unsigned tmem = s.tmem;
-  const unsigned taddr = tmem + ((unsigned)(warp * 32) << 16);  // this warp's 32 lanes
-  unsigned phase = 0;
-  bool ok = true;
+  const unsigned taddr = tmem + ((unsigned)(quarter * 32) << 16);  // this warp's 32 lanes
+  unsigned phase = 0, commits = 0;
   // One layer's products: D (128 x N) = A (128 x K) B^T, then wait for them.
   auto layer_mma = [&](const __nv_bfloat16* w, int K, int N) {
     if (tid == 0) {
@@ -340,47 +230,57 @@ __global__ void __launch_bounds__(kTcRows) mlp_forward_tc_kernel(MlpDev m,
                   umma_idesc(kTcRows, N), kc > 0 ? 1u : 0u);
       umma_commit(&s.bar);
     }
+    ++commits;
     const bool done = bar_wait(&s.bar, phase);
     phase ^= 1u;
     tc_fence_after();
     return __syncthreads_and(done) != 0;
   };
   const int ntiles = (n + kTcRows - 1) / kTcRows;
+  const float scale = 2.0f / (3.0f * (float)n);
+  double loss = 0.0;
   for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const int r = tid, row = tile * kTcRows + r;
-    // Layer-1 input: normalised features in BF16 (rows past n are zero).
+    const int r = quarter * 32 + (tid & 31), row = tile * kTcRows + r;
+    const int src = row < n ? (kTrain && index ? index[row] : row) : -1;
+    // Layer-1 input: normalised features in BF16 (rows past n are zero), this
+    // thread's half of its row's 16.
     {
-      float x[kMlpK];
+      const int c0 = 8 * half;
+      float x[8];
 #pragma unroll
-      for (int c = 0; c < kMlpK; ++c)
-        x[c] = row < n ? (feat[(size_t)row * kMlpK + c] - s.mean[c]) * s.inv_std[c] : 0.0f;
-#pragma unroll
-      for (int c0 = 0; c0 < kMlpK; c0 += 8) {
-        uint4 q;
-        q.x = pack_bf16(x[c0], x[c0 + 1]);
-        q.y = pack_bf16(x[c0 + 2], x[c0 + 3]);
-        q.z = pack_bf16(x[c0 + 4], x[c0 + 5]);
-        q.w = pack_bf16(x[c0 + 6], x[c0 + 7]);
-        *reinterpret_cast<uint4*>(s.a + cm_index(r, c0, kMlpK)) = q;
-      }
+      for (int c = 0; c < 8; ++c)
+        x[c] = src >= 0 ? (feat[(size_t)src * kMlpK + c0 + c] - s.mean[c0 + c]) * s.inv_std[c0 + c]
+                        : 0.0f;
+      uint4 q;
+      q.x = pack_bf16(x[0], x[1]);
+      q.y = pack_bf16(x[2], x[3]);
+      q.z = pack_bf16(x[4], x[5]);
+      q.w = pack_bf16(x[6], x[7]);
+      *reinterpret_cast<uint4*>(s.a + cm_index(r, c0, kMlpK)) = q;
     }
     proxy_fence();
     __syncthreads();
-    const __nv_bfloat16* ws[3] = {s.w1, s.w2, s.w3};
+    const __nv_bfloat16* ws[3] = {s.w.w1, s.w.w2, s.w.w3};
     for (int l = 0; l < 3 && ok; ++l) {
       ok = layer_mma(ws[l], l == 0 ? kMlpK : kMlpH, kMlpH);
       if (!ok) break;
       // Bias, GELU, BF16: the next layer's A (K = 64) from this thread's row.
 #pragma unroll
-      for (int c0 = 0; c0 < kMlpH; c0 += 16) {
+      for (int cc = 0; cc < kMlpH / 2; cc += 16) {
+        const int c0 = (kMlpH / 2) * half + cc;
         float v[16];
         tc_ld16(taddr + c0, v);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] += s.bias[l * kMlpH + c0 + j];
+        if (kTrain && row < n) {
+          float4* zr = reinterpret_cast<float4*>(z + (size_t)l * n * kMlpH + (size_t)row * kMlpH + c0);
+#pragma unroll
+          for (int j = 0; j < 16; j += 4) zr[j / 4] = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+        }
         uint4 q[2];
         uint32_t* qw = reinterpret_cast<uint32_t*>(q);
 #pragma unroll
-        for (int j = 0; j < 16; j += 2)
-          qw[j / 2] = pack_bf16(gelu(v[j] + s.bias[l * kMlpH + c0 + j]),
-                                gelu(v[j + 1] + s.bias[l * kMlpH + c0 + j + 1]));
+        for (int j = 0; j < 16; j += 2) qw[j / 2] = pack_bf16(gelu(v[j]), gelu(v[j + 1]));
         *reinterpret_cast<uint4*>(s.a + cm_index(r, c0, kMlpH)) = q[0];
         *reinterpret_cast<uint4*>(s.a + cm_index(r, c0 + 8, kMlpH)) = q[1];
       }
@@ -389,22 +289,50 @@ __global__ void __launch_bounds__(kTcRows) mlp_forward_tc_kernel(MlpDev m,
       __syncthreads();
     }
     if (!ok) break;
-    ok = layer_mma(s.w4, kMlpH, kTcOutN);
+    ok = layer_mma(s.w.w4, kMlpH, kTcOutN);
     if (!ok) break;
     float v[16];
-    tc_ld16(taddr, v);
-    if (row < n)
+    if (half == 0) tc_ld16(taddr, v);  // warp-uniform: warps 0-3 hold the 16 output columns
+    if (half == 0 && row < n) {
+      if constexpr (kTrain) {
 #pragma unroll
-      for (int c = 0; c < kMlpOut; ++c)
-        out[(size_t)row * kMlpOut + c] = v[c] + s.bias[3 * kMlpH + c];
+        for (int c = 0; c < kMlpKOut; ++c) {
+          float dv = 0.0f;
+          if (c < kMlpOut) {
+            const float e = (v[c] + s.bias[3 * kMlpH + c]) - t_hat[(size_t)src * 4 + c];
+            loss += (double)e * e;
+            dv = scale * e;
+          }
+          d4[(size_t)row * kMlpKOut + c] = dv;
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < kMlpOut; ++c)
+          out[(size_t)row * kMlpOut + c] = v[c] + s.bias[3 * kMlpH + c];
+      }
+    }
     tc_fence_before();
     __syncthreads();  // every lane's accumulators read before the next tile's products
   }
+  if constexpr (kTrain) {
+    // Loss partial of this block, in a fixed order (warp sums, then warps).
+    __shared__ double red[kTcThreads / 32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, off);
+    if ((tid & 31) == 0) red[warp] = loss;
+    __syncthreads();
+    if (tid == 0) {
+      double a = 0.0;
+      for (int w = 0; w < kTcThreads / 32; ++w) a += red[w];
+      loss_part[blockIdx.x] = a;
+    }
+  }
   if (!ok) {
-    // A product did not complete in time: report it and wait (bounded) for
-    // the products still in flight before the tensor memory is freed.
+    // A copy or product did not complete in time: report it and wait
+    // (bounded) for what is still in flight before the tensor memory is freed.
     if (tid == 0 && fail) atomicOr(fail, kFailMlpWait);
-    bar_wait(&s.bar, phase ^ 1u);
+    bar_wait(&s.wbar, 0u);
+    if (commits > 0u) bar_wait(&s.bar, phase ^ 1u);  // the last commit's phase
   }
   tc_fence_before();
   __syncthreads();
@@ -413,53 +341,6 @@ __global__ void __launch_bounds__(kTcRows) mlp_forward_tc_kernel(MlpDev m,
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(kTcCols)
                  : "memory");
-  }
-}
-
-// Training forward: pre-activations, the output gradient d4 = 2 (o - t) / (3n)
-// (n x 8, columns >= 3 zero) and per-block loss partials.
-__global__ void __launch_bounds__(kFwdThreads) mlp_train_forward_kernel(
-    MlpDev m, const float* __restrict__ feat, const float* __restrict__ t_hat,
-    const int* __restrict__ index, int n, float* __restrict__ z, float* __restrict__ d4,
-    double* __restrict__ loss_part) {
-  __shared__ SmemModel s;
-  __shared__ double red[kFwdWarps];
-  load_model(m, s);
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const int warp = blockIdx.x * kFwdWarps + (threadIdx.x >> 5);
-  const int nwarps = gridDim.x * kFwdWarps;
-  const float scale = 2.0f / (3.0f * (float)n);
-  double loss = 0.0;
-  for (int s0 = 16 * warp; s0 < n; s0 += 16 * nwarps) {
-    float o[4];
-    forward_tile(s, feat, index, s0, n, z, o);
-    const int rows[2] = {s0 + g, s0 + g + 8};
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int r = rows[h];
-      if (r >= n) continue;
-      const int src = index ? index[r] : r;
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int col = 2 * t + q;
-        float dv = 0.0f;
-        if (col < kMlpOut) {
-          float e = o[2 * h + q] - t_hat[(size_t)src * 4 + col];
-          loss += (double)e * e;
-          dv = scale * e;
-        }
-        d4[(size_t)r * kMlpKOut + col] = dv;
-      }
-    }
-  }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, off);
-  if (lane == 0) red[threadIdx.x >> 5] = loss;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 0.0;
-    for (int w = 0; w < kFwdWarps; ++w) a += red[w];
-    loss_part[blockIdx.x] = a;
   }
 }
 
@@ -779,37 +660,41 @@ __global__ void iterate_sample_kernel(int m, int n, unsigned salt, const float* 
   }
 }
 
-int fwd_grid(int n) {
-  int tiles = (n + 15) / 16;
-  int blocks = (tiles + kFwdWarps - 1) / kFwdWarps;
-  return blocks < 1 ? 1 : (blocks > 1184 ? 1184 : blocks);
-}
 
 }  // namespace
 
-void mlp_prepare(const float* params, uint32_t* frag, cudaStream_t st) {
-  mlp_prepare_kernel<<<div_up(kMlpTiles * 32, 128), 128, 0, st>>>(params, frag);
+
+// Persistent grid of the tensor-core forward: one CTA per 128-sample tile, at
+// most 4 per SM (256 threads, ~37 KB of shared memory and 64 tensor-memory
+// columns each).
+int tc_grid(int n) {
+  static const int max_grid = [] {
+    int dev = 0, sms = 0;
+    CUDA_CHECK(cudaGetDevice(&dev));
+    CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return 4 * sms;
+  }();
+  const int tiles = (n + kTcRows - 1) / kTcRows;
+  return tiles < 1 ? 1 : (tiles < max_grid ? tiles : max_grid);
+}
+
+void mlp_image(const float* params, uint16_t* image, cudaStream_t st) {
+  mlp_image_kernel<<<div_up(kMlpH * kMlpH, 256), 256, 0, st>>>(
+      params, reinterpret_cast<TcWeights*>(image));
   SILK_LAUNCHED();
 }
 
 void mlp_forward(const MlpDev& m, const float* feat, int n, float* out, cudaStream_t st) {
   if (n <= 0) return;
-  static const int max_grid = [] {
-    int dev = 0, sms = 0;
-    CUDA_CHECK(cudaGetDevice(&dev));
-    CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    return 4 * sms;  // 128 threads and ~29 KB of shared memory per CTA; 4 x 64 TMEM columns per SM
-  }();
-  const int tiles = (n + kTcRows - 1) / kTcRows;
-  mlp_forward_tc_kernel<<<tiles < max_grid ? tiles : max_grid, kTcRows, sizeof(TcSmem), st>>>(
-      m, feat, n, out, m.fail);
+  mlp_forward_tc_kernel<false><<<tc_grid(n), kTcThreads, sizeof(TcSmem), st>>>(
+      m, feat, n, out, m.fail, nullptr, nullptr, nullptr, nullptr, nullptr);
   SILK_LAUNCHED();
 }
 
 size_t mlp_work_floats(int n) {
   // z (3 x n x 64) + d4 (n x 8) + backward partials + loss partials (doubles).
   return (size_t)3 * n * kMlpH + (size_t)n * kMlpKOut +
-         (size_t)kBwdBlocks * kMlpTrainParams + 2 * (size_t)fwd_grid(n) + 4;
+         (size_t)kBwdBlocks * kMlpTrainParams + 2 * (size_t)tc_grid(n) + 4;
 }
 
 void mlp_loss_grad(const MlpDev& m, const float* feat, const float* t_hat, int n,
@@ -821,9 +706,9 @@ void mlp_loss_grad(const MlpDev& m, const float* feat, const float* t_hat, int n
   size_t off = (size_t)3 * n * kMlpH + (size_t)n * kMlpKOut + (size_t)kBwdBlocks * kMlpTrainParams;
   off = (off + 1) & ~(size_t)1;  // 8-byte alignment for the doubles
   double* loss_part = reinterpret_cast<double*>(work + off);
-  const int fg = fwd_grid(n);
-  mlp_train_forward_kernel<<<fg, kFwdThreads, 0, st>>>(m, feat, t_hat, index, n, z, d4,
-                                                      loss_part);
+  const int fg = tc_grid(n);
+  mlp_forward_tc_kernel<true><<<fg, kTcThreads, sizeof(TcSmem), st>>>(
+      m, feat, n, nullptr, m.fail, t_hat, index, z, d4, loss_part);
   SILK_LAUNCHED();
   static const bool attr = [] {
     CUDA_CHECK(cudaFuncSetAttribute(mlp_backward_kernel,

@@ -29,24 +29,24 @@ constexpr int kOffStd = kOffMean + kMlpK;       // feature std (16)
 constexpr int kOffOutScale = kOffStd + kMlpK;   // output scale (8)
 constexpr int kMlpParams = kOffOutScale + kMlpKOut;
 constexpr int kMlpTrainParams = kOffMean;       // learned part
-// B-operand fragment tiles of m16n8k16 per layer: (K / 16) x (N / 8).
-constexpr int kTilesL1 = 1 * 8, kTilesL2 = 4 * 8, kTilesL3 = 4 * 8, kTilesL4 = 4 * 1;
-constexpr int kMlpTiles = kTilesL1 + kTilesL2 + kTilesL3 + kTilesL4;
-constexpr int kMlpFragWords = kMlpTiles * 32 * 2;  // uint32 words
 
-// Device model: FP32 parameters and their BF16 B-operand fragments.
+// BF16 elements of the weight image (the four layers' B operands as the
+// forward holds them in shared memory: 64x16, 64x64, 64x64, 16x64).
+constexpr int kMlpWeightImage = kMlpH * kMlpK + 2 * kMlpH * kMlpH + 16 * kMlpH;
+
+// Device model: FP32 parameters and their BF16 weight image.
 struct MlpDev {
-  const float* params = nullptr;   // kMlpParams
-  const uint32_t* frag = nullptr;  // kMlpFragWords
-  int* fail = nullptr;             // kFailMlpWait is set here when a tensor-core wait gives up
+  const float* params = nullptr;    // kMlpParams
+  const uint16_t* image = nullptr;  // kMlpWeightImage BF16 (mlp_image of params)
+  int* fail = nullptr;              // kFailMlpWait is set here when a tensor-core wait gives up
 };
 
-// Bit of the solver's failure word: a tensor-core product of the inference
-// forward did not complete within its bounded wait.
-constexpr int kFailMlpWait = 8;
+// Build the weight image of a parameter vector (device pointers).
+void mlp_image(const float* params, uint16_t* image, cudaStream_t st);
 
-// Build the BF16 fragments of a parameter vector (device pointers).
-void mlp_prepare(const float* params, uint32_t* frag, cudaStream_t st);
+// Bit of the solver's failure word: a tensor-core product of the forward did
+// not complete within its bounded wait.
+constexpr int kFailMlpWait = 8;
 
 // Output o (n x 3, normalised units) of raw features (n x 16: displacement
 // features divided by the step scale, pin flag, zero padding).

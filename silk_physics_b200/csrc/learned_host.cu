@@ -25,12 +25,14 @@ __global__ void sample_index_kernel(int* idx, int batch, int n, unsigned long lo
 
 struct MlpBuffers {
   DevBuf<float> params, feat, tgt, out, grad, work, m, v;
-  DevBuf<uint32_t> frag;
+  DevBuf<uint16_t> image;
   DevBuf<double> loss;
-  DevBuf<int> idx;
+  DevBuf<int> idx, fail;
   void load(const float* p, const float* f, const float* t, int n, cudaStream_t st) {
     params.alloc(kMlpParams);
-    frag.alloc(kMlpFragWords);
+    image.alloc(kMlpWeightImage);
+    fail.alloc(1);
+    fail.zero(st);
     CUDA_CHECK(cudaMemcpyAsync(params.p, p, kMlpParams * sizeof(float), cudaMemcpyHostToDevice, st));
     if (f) {
       feat.alloc((size_t)kMlpK * n);
@@ -43,7 +45,14 @@ struct MlpBuffers {
                                  cudaMemcpyHostToDevice, st));
     }
   }
-  MlpDev dev() const { return MlpDev{params.p, frag.p}; }
+  MlpDev dev() const { return MlpDev{params.p, image.p, fail.p}; }
+  // A tensor-core wait of the forward gave up (after the work on `st`).
+  void check(cudaStream_t st) const {
+    int f = 0;
+    CUDA_CHECK(cudaMemcpyAsync(&f, fail.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_CHECK(cudaStreamSynchronize(st));
+    if (f) throw CudaError("tensor-core wait gave up");
+  }
 };
 
 }  // namespace
@@ -53,16 +62,10 @@ void mlp_forward_host(const float* params, const float* feat, int64_t n, float* 
   MlpBuffers b;
   b.load(params, feat, nullptr, (int)n, st);
   b.out.alloc((size_t)kMlpOut * n);
-  DevBuf<int> fail;
-  fail.alloc(1);
-  fail.zero(st);
-  MlpDev m = b.dev();
-  m.fail = fail.p;
-  mlp_forward(m, b.feat.p, (int)n, b.out.p, st);
+  mlp_image(b.params.p, b.image.p, st);
+  mlp_forward(b.dev(), b.feat.p, (int)n, b.out.p, st);
+  b.check(st);
   CUDA_CHECK(cudaMemcpy(out, b.out.p, (size_t)kMlpOut * n * sizeof(float), cudaMemcpyDeviceToHost));
-  int f = 0;
-  CUDA_CHECK(cudaMemcpy(&f, fail.p, sizeof(int), cudaMemcpyDeviceToHost));
-  if (f) throw CudaError("tensor-core wait gave up");
 }
 
 void mlp_loss_grad_host(const float* params, const float* feat, const float* tgt, int64_t n,
@@ -73,8 +76,9 @@ void mlp_loss_grad_host(const float* params, const float* feat, const float* tgt
   b.grad.alloc(kMlpParams);
   b.work.alloc(mlp_work_floats((int)n));
   b.loss.alloc(1);
-  mlp_prepare(b.params.p, b.frag.p, st);
+  mlp_image(b.params.p, b.image.p, st);
   mlp_loss_grad(b.dev(), b.feat.p, b.tgt.p, (int)n, nullptr, b.work.p, b.grad.p, b.loss.p, st);
+  b.check(st);
   CUDA_CHECK(cudaMemcpy(grad, b.grad.p, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost));
   CUDA_CHECK(cudaMemcpy(loss, b.loss.p, sizeof(double), cudaMemcpyDeviceToHost));
 }
@@ -99,11 +103,12 @@ void mlp_train_host(float* params, const float* feat, const float* tgt, int64_t 
       sample_index_kernel<<<div_up(nb, 256), 256, 0, st>>>(b.idx.p, nb, (int)n, seed, step);
       SILK_LAUNCHED();
     }
-    mlp_prepare(b.params.p, b.frag.p, st);
+    mlp_image(b.params.p, b.image.p, st);
     mlp_loss_grad(b.dev(), b.feat.p, b.tgt.p, nb, full ? nullptr : b.idx.p, b.work.p, b.grad.p,
                   b.loss.p + (step - 1), st);
     mlp_adam(b.params.p, b.grad.p, b.m.p, b.v.p, step, lr, st);
   }
+  b.check(st);
   CUDA_CHECK(cudaMemcpy(params, b.params.p, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost));
   if (loss_hist && steps > 0) {
     std::vector<double> h(steps);

@@ -1123,17 +1123,17 @@ silk_status World::set_warm_start_model(const float* params, int64_t n) {
     if (!std::isfinite(params[i])) return SILK_ERR_INVALID_CONFIG;
   ensure_stream();
   mlp_params.alloc(kMlpParams);
-  mlp_frag.alloc(kMlpFragWords);
+  mlp_image_buf.alloc(kMlpWeightImage);
   CUDA_CHECK(cudaMemcpyAsync(mlp_params.p, params, kMlpParams * sizeof(float),
                              cudaMemcpyHostToDevice, stream));
-  mlp_prepare(mlp_params.p, mlp_frag.p, stream);
+  mlp_image(mlp_params.p, mlp_image_buf.p, stream);
   has_iter_model = n == 2 * (int64_t)kMlpParams;
   if (has_iter_model) {
     mlp2_params.alloc(kMlpParams);
-    mlp2_frag.alloc(kMlpFragWords);
+    mlp2_image_buf.alloc(kMlpWeightImage);
     CUDA_CHECK(cudaMemcpyAsync(mlp2_params.p, params + kMlpParams, kMlpParams * sizeof(float),
                                cudaMemcpyHostToDevice, stream));
-    mlp_prepare(mlp2_params.p, mlp2_frag.p, stream);
+    mlp_image(mlp2_params.p, mlp2_image_buf.p, stream);
   }
   sync();
   has_model = true;
@@ -1248,7 +1248,7 @@ bool World::admm_solve() {
       // x holds x_(it-1); slots (it-1) % 3 and (it-2) % 3 hold x_(it-2) and
       // x_(it-3) from the previous iterations.
       if (it >= 3) {
-        MlpDev m{iter_model ? mlp2_params.p : nullptr, mlp2_frag.p, cg_fail.p};
+        MlpDev m{iter_model ? mlp2_params.p : nullptr, mlp2_image_buf.p, cg_fail.p};
         iterate_predict(m, nv_total, x.p, iter_ring[(it - 1) % 3]->p, iter_ring[(it - 2) % 3]->p,
                         pin_flag.p, ring_off.p, ring.p, iter_sigma.p, iter_feat.p, iter_out.p,
                         iter_pred.p, st);
@@ -1413,7 +1413,7 @@ silk_status World::solver_step() {
         warm_features(nv, outer.p, hist1.p, hist2.p, ypred.p, pin_flag.p, ring_off.p, ring.p,
                       1.0f / sigma, warm_feat.p, st);
         if (has_model && opt.learned_warm_start) {
-          MlpDev m{mlp_params.p, mlp_frag.p, cg_fail.p};
+          MlpDev m{mlp_params.p, mlp_image_buf.p, cg_fail.p};
           warm_predict(m, nv, warm_feat.p, ypred.p, sigma, mlp_out.p, xpred.p, st);
         }
       }

@@ -223,10 +223,10 @@ class World {
   DevBuf<int> vf_off, vf_list;
   DevBuf<double> face_partials, vertex_partials;
   DevBuf<AdmmControl> ctl;
-  DevBuf<int> cg_fail;  // set by a CG kernel whose barrier wait gave up
+  DevBuf<int> cg_fail;  // kFail* bits: a bounded device wait gave up, a bank pivot failed
   // Learned warm start: model, step history, features and training samples.
   DevBuf<float> mlp_params, mlp_out, warm_feat, warm_tgt;
-  DevBuf<uint32_t> mlp_frag;
+  DevBuf<uint16_t> mlp_image_buf, mlp2_image_buf;  // BF16 weight images of the two models
   DevBuf<float4> hist1, hist2, step_start, ypred, xpred;
   // ADMM-extrapolated CG start: the previous ADMM iterate and 2 x_k - x_(k-1).
   DevBuf<float4> admm_prev, admm_ext;
@@ -236,7 +236,6 @@ class World {
   // three: at iteration k, slot k % 3 receives x_(k-1) before the solve),
   // scale, features, prediction and the step's training samples.
   DevBuf<float> mlp2_params, iter_feat, iter_out, iter_sigma, iter_samp_feat, iter_samp_tgt;
-  DevBuf<uint32_t> mlp2_frag;
   DevBuf<float4> iter_hist0, iter_hist1, iter_hist2, iter_pred;
   DevBuf<int> iter_samp_n;
   bool has_iter_model = false;
