@@ -1402,7 +1402,6 @@ struct DsmShared {
   __nv_bfloat16 rb[W][8][BANK];           // BF16 apply: residual as B operand
   float4 zs[W][BANK];                     // BF16 apply / split bank rows
   double red[W][3];
-  double tot[3];
   double part[kDsmMaxCtas][kDsmPartSlots];  // partials of every CTA (pushed)
   float4 zown[32 * W];                    // fine-level z of the own slots
   float4 hzs[32 * W];                     // fine-level z of the halo (pushed by the owners)
@@ -1509,12 +1508,12 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     else
       stage_bank_full(lv, bank, slot, lane);
   };
-  // Store this CTA's N partial sums (s.tot after a block sum) into slots
-  // slot0.. of every CTA's s.part row q.
-  auto push_partials = [&](int slot0, int N) {
+  // Store this CTA's N block sums t[] into slots slot0.. of every CTA's
+  // s.part row q.
+  auto push_partials = [&](int slot0, const double* t, int N) {
     if (warp == 0 && lane < nctas) {
       double* dst = cl.map_shared_rank(&s.part[q][slot0], lane);
-      for (int k = 0; k < N; ++k) dst[k] = s.tot[k];
+      for (int k = 0; k < N; ++k) dst[k] = t[k];
     }
   };
   // Sum of one partial slot over the CTAs: a warp sum in a fixed lane order,
@@ -1522,19 +1521,18 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
   auto total = [&](int slot) {
     return warp_sum_d(lane < nctas ? s.part[lane][slot] : 0.0);
   };
-  // Block sum of N doubles per thread into s.tot (fixed order).
-  auto block_sum = [&](const double* v, int N) {
+  // Block sum of N doubles per thread into t[] of every thread: warp sums
+  // into s.red, one block barrier, then every warp sums the warps' values
+  // with the same butterfly (identical totals in all warps, in a fixed
+  // order).  The next write of s.red comes after a later block or cluster
+  // barrier.
+  auto block_sum = [&](const double* v, int N, double* t) {
     for (int k = 0; k < N; ++k) {
       double x = warp_sum_d(v[k]);
       if (lane == 0) s.red[warp][k] = x;
     }
     __syncthreads();
-    if (warp == 0)
-      for (int k = 0; k < N; ++k) {
-        double x = warp_sum_d(lane < W ? s.red[lane][k] : 0.0);
-        if (lane == 0) s.tot[k] = x;
-      }
-    __syncthreads();
+    for (int k = 0; k < N; ++k) t[k] = warp_sum_d(lane < W ? s.red[lane][k] : 0.0);
   };
 
   // ---- one-time staging ----------------------------------------------------
@@ -1686,8 +1684,9 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     const double v3[3] = {(double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z,
                           (double)r.x * ra.x + (double)r.y * ra.y + (double)r.z * ra.z,
                           (double)ra.x * ra.x + (double)ra.y * ra.y + (double)ra.z * ra.z};
-    block_sum(v3, 3);
-    push_partials(3, 3);
+    double t3[3];
+    block_sum(v3, 3, t3);
+    push_partials(3, t3, 3);
     cl.sync();
     const double rr_plain = total(3), r_pa = total(4), rr_alt = total(5);
     rr_judge = rr_plain;
@@ -1729,8 +1728,9 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     }
     s.zown[tid] = make_float4(z0.x, z0.y, z0.z, 0.f);
     const double v2[2] = {rz, rr};
-    block_sum(v2, 2);  // its barriers also publish zown to the CTA
-    push_partials(0, 2);
+    double t2[2];
+    block_sum(v2, 2, t2);  // its barrier also publishes zown to the CTA
+    push_partials(0, t2, 2);
     for (int i = tid; i < npush; i += T) {
       const int e = s.push[i];
       float4* dst = cl.map_shared_rank(&s.hzs[e >> 15], (e >> 10) & 31);
@@ -1800,13 +1800,16 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
           s.zc[slot] = make_float4(zq.x, zq.y, zq.z, 0.f);
           rzc += (double)rl.x * zq.x + (double)rl.y * zq.y + (double)rl.z * zq.z;
         }
-        __syncthreads();
+        // s.zs is reused by the next round; after the last one the block sum's
+        // barrier publishes s.zc.
+        if (g0 + per_round < ncb) __syncthreads();
       }
     }
     tr.stamp(iter, 11);
     const double v1[1] = {rzc};
-    block_sum(v1, 1);
-    rz += s.tot[0];
+    double t1[1];
+    block_sum(v1, 1, t1);
+    rz += t1[0];
     tr.stamp(iter, 12);
   };
 
@@ -1856,8 +1859,9 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
       tr.stamp(iter, 2);
       const double v1[1] = {own ? (double)p.x * Ap.x + (double)p.y * Ap.y + (double)p.z * Ap.z
                                 : 0.0};
-      block_sum(v1, 1);
-      push_partials(2, 1);
+      double t1[1];
+      block_sum(v1, 1, t1);
+      push_partials(2, t1, 1);
     }
     tr.stamp(iter, 3);
     cl.sync();
