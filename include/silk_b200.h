@@ -128,6 +128,11 @@ typedef struct {
                                  k - 1 of a cooperative-grid CG launch skip its
                                  barrier arrivals, so the other blocks' bounded
                                  waits run out; 0: off */
+  int32_t admm_check_interval; /* ADMM iterations enqueued between the host's
+                                 reads of the convergence state (the device
+                                 decides convergence; iterations enqueued after
+                                 it do nothing); 0: 4; 1: a read after every
+                                 iteration */
 } silk_solver_options;
 
 /* CUDA-event timing of the persistent CG kernel over the steps since the

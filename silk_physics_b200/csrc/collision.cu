@@ -1185,7 +1185,8 @@ __global__ void jp_round_kernel(const ContactDev* c, const unsigned long long* p
 
 __global__ void contact_gs_kernel(const ContactDev* contacts, const int* groups,
                                   const int* group_off, int ncolors, float4* corr,
-                                  float4* p, unsigned* barrier) {
+                                  float4* p, unsigned* barrier, const int* skip) {
+  if (skip && *skip) return;  // the ADMM solve already ended (every block alike)
   GridBarrier bar{barrier, barrier + 1, barrier + 2, gridDim.x};
   int stride = gridDim.x * blockDim.x;
   int tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1304,7 +1305,8 @@ __global__ void gs_gather_kernel(const ContactDev* __restrict__ c, const int* __
 __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
     const GsContact* __restrict__ cc, const int* __restrict__ group_off, int ncolors, int total,
     float4* __restrict__ corr, float4* __restrict__ ccorr, const int* __restrict__ vlist,
-    int nslots, float4* __restrict__ p) {
+    int nslots, float4* __restrict__ p, const int* __restrict__ skip) {
+  if (skip && *skip) return;  // the ADMM solve already ended
   extern __shared__ float4 sp[];
   const int t = threadIdx.x;
   for (int i = t; i < nslots; i += blockDim.x) sp[i] = p[vlist[i]];
@@ -1444,7 +1446,8 @@ __host__ __device__ inline GsPipeLayout gs_pipe_layout(int nslots, int total, in
 __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
     const GsContact* __restrict__ cc, const int* __restrict__ group_off, int ncolors, int total,
     float4* __restrict__ corr, const int* __restrict__ vlist, int nslots, float4* __restrict__ p,
-    int* __restrict__ fail) {
+    int* __restrict__ fail, const int* __restrict__ skip) {
+  if (skip && *skip) return;  // the ADMM solve already ended
   extern __shared__ __align__(16) unsigned char gs_raw[];
   __shared__ __align__(8) uint64_t bars[kGsStages];
   const GsPipeLayout L = gs_pipe_layout(nslots, total, ncolors, blockDim.x);
@@ -2270,7 +2273,7 @@ int CollisionSystem::append_active(float time, float dact) {
   return add;
 }
 
-void CollisionSystem::contact_solve() {
+void CollisionSystem::contact_solve_launch() {
   CollisionImpl& I = *impl_;
   if (I.n_contacts == 0) return;
   cudaStream_t st = w_.stream;
@@ -2298,13 +2301,13 @@ void CollisionSystem::contact_solve() {
       (void)pattr;
       contact_gs_pipe_kernel<<<1, threads, L.bytes, st>>>(
           I.gs_cc.p, I.group_off.p, I.n_colors, I.n_contacts, I.corr.p, I.gs_vlist.p,
-          I.gs_nslots, w_.contact_p.p, w_.cg_fail.p);
+          I.gs_nslots, w_.contact_p.p, w_.cg_fail.p, gs_skip_);
       SILK_LAUNCHED();
       return;
     }
     contact_gs_block_kernel<<<1, threads, smem, st>>>(
         I.gs_cc.p, I.group_off.p, I.n_colors, I.n_contacts, I.corr.p, I.gs_ccorr.p,
-        I.gs_vlist.p, I.gs_nslots, w_.contact_p.p);
+        I.gs_vlist.p, I.gs_nslots, w_.contact_p.p, gs_skip_);
     SILK_LAUNCHED();
     return;
   }
@@ -2324,7 +2327,8 @@ void CollisionSystem::contact_solve() {
   float4* corr = I.corr.p;
   float4* p = w_.contact_p.p;
   unsigned* bar = I.gs_barrier.p;
-  void* args[] = {&c, &g, &go, &nc, &corr, &p, &bar};
+  const int* skip = gs_skip_;
+  void* args[] = {&c, &g, &go, &nc, &corr, &p, &bar, &skip};
   CUDA_CHECK(cudaLaunchCooperativeKernel((const void*)contact_gs_kernel, dim3(grid), dim3(256),
                                          args, 0, st));
   SILK_LAUNCHED();

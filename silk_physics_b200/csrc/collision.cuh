@@ -36,8 +36,13 @@ class CollisionSystem {
   // n_hits then counts completed searches only).
   float min_toi(float time_start, float max_time, float min_separation,
                 int* n_queries, int* n_hits, bool prune = true);
-  // Contact projection of one ADMM iteration (after contact_init).
-  void contact_solve();
+  // Contact projection of one ADMM iteration (after contact_init); with
+  // skip set (AdmmControl::done of the running ADMM solve) the kernels return
+  // at entry once the solve has ended.
+  void contact_solve(const int* skip = nullptr) {
+    gs_skip_ = skip;
+    contact_solve_launch();
+  }
   int contact_count() const;
   int color_count() const;
   const int* active_dof_device() const;
@@ -60,6 +65,8 @@ class CollisionSystem {
   int debug_contacts(int* keys, int64_t cap);
 
  private:
+  void contact_solve_launch();
+  const int* gs_skip_ = nullptr;
   World& w_;
   std::unique_ptr<CollisionImpl> impl_;
 };

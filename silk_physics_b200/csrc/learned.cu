@@ -641,7 +641,9 @@ __global__ void iterate_sample_kernel(int m, int n, unsigned salt, const float* 
                                       const float4* __restrict__ x_old,
                                       const float* __restrict__ sigma,
                                       float* __restrict__ out_feat, float* __restrict__ out_tgt,
-                                      int* __restrict__ counter, int cap) {
+                                      int* __restrict__ counter, int cap,
+                                      const int* __restrict__ skip) {
+  if (skip && *skip) return;  // the ADMM solve already ended: no iterate to sample
   __shared__ int base;
   if (threadIdx.x == 0) base = atomicAdd(counter, m);
   __syncthreads();
@@ -774,10 +776,10 @@ void iterate_predict(const MlpDev& m, int n, const float4* x, const float4* h1, 
 
 void iterate_samples(int m, int n, unsigned salt, const float* feat, const float4* x_new,
                      const float4* x_old, const float* sigma, float* out_feat, float* out_tgt,
-                     int* counter, int cap, cudaStream_t st) {
+                     int* counter, int cap, const int* skip, cudaStream_t st) {
   if (n <= 0 || m <= 0) return;
   iterate_sample_kernel<<<1, 256, 0, st>>>(m, n, salt, feat, x_new, x_old, sigma, out_feat,
-                                           out_tgt, counter, cap);
+                                           out_tgt, counter, cap, skip);
   SILK_LAUNCHED();
 }
 

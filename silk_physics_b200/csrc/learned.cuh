@@ -86,7 +86,7 @@ void iterate_predict(const MlpDev& m, int n, const float4* x, const float4* h1, 
 // out_feat / out_tgt at the counter's position while below cap.
 void iterate_samples(int m, int n, unsigned salt, const float* feat, const float4* x_new,
                      const float4* x_old, const float* sigma, float* out_feat, float* out_tgt,
-                     int* counter, int cap, cudaStream_t st);
+                     int* counter, int cap, const int* skip, cudaStream_t st);
 constexpr int kIterSamplesPerSolve = 256;   // vertices recorded per ADMM iteration
 constexpr int kIterSampleCap = 1 << 19;     // samples per step
 

@@ -422,6 +422,7 @@ __device__ __forceinline__ void mark_fail(const CgArgs& a) {
 
 template <class Barrier>
 __device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm_all) {
+  if (a.skip && *a.skip) return;  // the ADMM solve already ended (every block alike)
   double* part = a.partials + 4 * blockIdx.x;
   CgTrace tr(a.trace, 0);
   // r = b - A x.
@@ -484,7 +485,8 @@ __device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm
   }
   const double rr0 = rr_judge >= 0.0 ? rr_judge : rr;
   const double abs2 = (double)a.abs_tol * a.abs_tol;
-  const double rel2 = (double)a.rel_tol * a.rel_tol;
+  const float rel_tol = a.rel_tol_dev ? *a.rel_tol_dev : a.rel_tol;
+  const double rel2 = (double)rel_tol * rel_tol;
   double beta = 0.0;
   int iter = 0;
   int status = kCgMaxIter;
@@ -820,6 +822,7 @@ __device__ __forceinline__ float3 res_row_tmem(const ResShared& s, const float4*
 
 template <class Barrier>
 __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
+  if (a.skip && *a.skip) return;  // the ADMM solve already ended (every block alike)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int k = blockIdx.x;
   const int nblocks = gridDim.x;
@@ -1218,7 +1221,8 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
   }
   const double rr0 = rr_judge >= 0.0 ? rr_judge : rr;
   const double abs2 = (double)a.abs_tol * a.abs_tol;
-  const double rel2 = (double)a.rel_tol * a.rel_tol;
+  const float rel_tol = a.rel_tol_dev ? *a.rel_tol_dev : a.rel_tol;
+  const double rel2 = (double)rel_tol * rel_tol;
   double beta = 0.0;
   int status = kCgMaxIter;
   while (true) {
@@ -1480,6 +1484,7 @@ __device__ __forceinline__ float3 dsm_row_tmem(unsigned taddr, int rw, const flo
 
 template <int F>
 __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
+  if (a.skip && *a.skip) return;  // the ADMM solve already ended (every CTA alike)
   constexpr int W = F, T = 32 * F;
   extern __shared__ __align__(16) unsigned char dsm_smem[];
   DsmShared<W>& s = *reinterpret_cast<DsmShared<W>*>(dsm_smem);
@@ -1831,7 +1836,8 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
   }
   const double rr0 = rr_judge >= 0.0 ? rr_judge : rr;
   const double abs2 = (double)a.abs_tol * a.abs_tol;
-  const double rel2 = (double)a.rel_tol * a.rel_tol;
+  const float rel_tol = a.rel_tol_dev ? *a.rel_tol_dev : a.rel_tol;
+  const double rel2 = (double)rel_tol * rel_tol;
   double beta = 0.0;
   int status = kCgMaxIter;
   while (true) {

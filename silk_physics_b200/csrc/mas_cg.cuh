@@ -95,6 +95,11 @@ struct CgArgs {
   const int* halo_col = nullptr;  // halo vertices (outside the block, read by its rows)
   int halo_full = 0;  // every off-block column of the resident rows is in its block's halo
   int* fail = nullptr;          // kFail* bits: a barrier wait gave up
+  // Device-decided ADMM iterations: the kernel returns at entry when *skip is
+  // set (the ADMM solve already ended) and takes its relative tolerance from
+  // *rel_tol_dev (the finalize kernel's next tolerance) when not null.
+  const int* skip = nullptr;
+  const float* rel_tol_dev = nullptr;
   long long barrier_spin_limit = 0;  // > 0: grid-barrier polls before giving up
   int withhold_block = -1;      // >= 0: that block skips its barrier arrivals (tests)
   // Cluster form with redundant coarse levels (cg_dsm_cluster_kernel): fine

@@ -128,6 +128,7 @@ __global__ void inertia_kernel(SolverView s) {
 // per-vertex dual scatter, which the vertex kernel gathers instead.
 __global__ void __launch_bounds__(THREADS) face_step_kernel(SolverView s,
                                                             double* partials) {
+  if (s.skip && *s.skip) return;  // the ADMM solve already ended
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[3] = {0.0, 0.0, 0.0};
   if (f < s.nf) {
@@ -178,6 +179,7 @@ __global__ void __launch_bounds__(THREADS) face_step_kernel(SolverView s,
 
 // initialize_aux (contact_constraints.cu:203-215): p <- x - eta / w.
 __global__ void contact_init_kernel(SolverView s) {
+  if (s.skip && *s.skip) return;  // the ADMM solve already ended
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.nv) return;
   float w = s.contact_w[i];
@@ -201,6 +203,7 @@ __global__ void contact_init_kernel(SolverView s) {
 // contact_constraints.cu:302-318).
 __global__ void __launch_bounds__(THREADS) vertex_step_kernel(SolverView s,
                                                               double* partials) {
+  if (s.skip && *s.skip) return;  // the ADMM solve already ended
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   if (i < s.nv) {
@@ -295,6 +298,7 @@ __global__ void __launch_bounds__(THREADS) vertex_step_kernel(SolverView s,
 }
 
 __global__ void admm_finalize_kernel(AdmmFinalizeArgs a) {
+  if (a.ctl->done) return;  // the ADMM solve already ended
   __shared__ double sh[kAdmmSlots][32];
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // warp k < 3 sums face slot k, warps 3.. sum vertex slots.
@@ -319,6 +323,7 @@ __global__ void admm_finalize_kernel(AdmmFinalizeArgs a) {
   if (sh[kNonFinite][0] > 0.0 || (a.cg_fail && *a.cg_fail)) {
     c->diverged = 1;
     c->converged = 0;
+    c->done = 1;
     return;
   }
   float pnorm = sqrtf((float)pn2);
@@ -337,6 +342,7 @@ __global__ void admm_finalize_kernel(AdmmFinalizeArgs a) {
   c->dual_norm = dnorm;
   c->converged = (pnorm <= peps && dnorm <= deps) ? 1 : 0;
   c->diverged = 0;
+  c->done = c->converged;
   float rel = fminf(fmaxf(a.init_lin_rel * ratio, a.lin_rel_min), a.lin_rel_max);
   c->next_rel_tol = a.fixed_rel > 0.0f ? a.fixed_rel : rel;
 }

@@ -41,6 +41,9 @@ struct SolverView {
   float* lhs = nullptr;
   float4* rhs = nullptr;
   float4* inertia = nullptr;  // -x_prev/dt^2 - v_prev/dt - a
+  // AdmmControl::done of the running ADMM solve: the per-iteration kernels
+  // (face step, contact init, vertex step) return at entry when it is set.
+  const int* skip = nullptr;
 };
 
 // ADMM reduction slots (double partial sums per block).
@@ -66,7 +69,10 @@ struct AdmmControl {
   float init_dual;
   float ratio;
   int iteration;
-  int pad[7];
+  // Set with converged or diverged: the iterations the host enqueued beyond
+  // this one find it at entry and do nothing.
+  int done;
+  int pad[6];
 };
 
 void launch_compute_inertia(const SolverView& s, cudaStream_t st);

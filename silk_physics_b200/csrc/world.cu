@@ -1063,8 +1063,11 @@ void World::cg_solve(Cloth& c, float rel_tol, bool first, cudaStream_t st) {
   a.withhold_block = opt.debug_withhold_block - 1;
   const bool dsm = c.dev.dsm_ctas > 0;
   const bool resident = !dsm && c.dev.res_grid != 0;
-  if (dsm || resident) stats.cg_resident_solves += 1;
-  if (dsm) stats.cg_cluster_solves += 1;
+  // Counted by admm_solve for the iterations that ran.
+  if (dsm || resident) solve_resident_ += 1;
+  if (dsm) solve_cluster_ += 1;
+  a.skip = cg_skip_;
+  a.rel_tol_dev = cg_skip_ ? &ctl.p->next_rel_tol : nullptr;
   auto launch = [&]() {
     if (dsm)
       launch_cg_dsm(a, c.dev.dsm_ctas, st);
@@ -1211,6 +1214,29 @@ bool World::admm_solve() {
   float rel = std::min(std::max(g.initial_linear_rel_tol, g.linear_solver_rel_tol_min),
                        g.linear_solver_rel_tol_max);
   if (opt.fixed_linear_rel_tol > 0) rel = opt.fixed_linear_rel_tol;
+  // Iterations are decided on the device: the finalize kernel sets
+  // AdmmControl::done when the solve converges or diverges, and every kernel
+  // of a later iteration returns at entry; the host enqueues
+  // admm_check_interval iterations between reads of the control block, so
+  // the GPU does not idle on a host round trip after every iteration.  The
+  // CG takes each solve's tolerance from the control block.
+  {
+    AdmmControl init{};
+    init.next_rel_tol = rel;
+    CUDA_CHECK(cudaMemcpyAsync(ctl.p, &init, sizeof(AdmmControl), cudaMemcpyHostToDevice, st));
+  }
+  const int check_every = opt.admm_check_interval > 0 ? opt.admm_check_interval : 4;
+  ctl_host_ = AdmmControl{};
+  const int* done = &ctl.p->done;
+  s.skip = done;
+  cg_skip_ = done;
+  struct SkipReset {
+    const int*& p;
+    ~SkipReset() { p = nullptr; }
+  } skip_reset{cg_skip_};
+  solve_resident_ = solve_cluster_ = 0;
+  const int prior_iterations = stats.admm_iterations;
+  int enqueued = 0;
   int fb = face_step_blocks(nf_total), vb = vertex_step_blocks(nv_total);
   AdmmFinalizeArgs fa;
   fa.face_partials = face_partials.p;
@@ -1305,9 +1331,9 @@ bool World::admm_solve() {
         samples_valid = true;
       }
       if (iter_capture && it >= 3)
-        iterate_samples(kIterSamplesPerSolve, nv_total, (unsigned)(it * 7919 + stats.admm_iterations),
+        iterate_samples(kIterSamplesPerSolve, nv_total, (unsigned)(it * 7919 + prior_iterations + it),
                         iter_feat.p, x.p, iter_ring[it % 3]->p, iter_sigma.p, iter_samp_feat.p,
-                        iter_samp_tgt.p, iter_samp_n.p, kIterSampleCap, st);
+                        iter_samp_tgt.p, iter_samp_n.p, kIterSampleCap, done, st);
     }
     std::pair<cudaEvent_t, cudaEvent_t>* oe = opt.profile ? next_event_pair(events_other, events_other_used) : nullptr;
     if (oe) CUDA_CHECK(cudaEventRecord(oe->first, st));
@@ -1317,22 +1343,30 @@ bool World::admm_solve() {
       std::pair<cudaEvent_t, cudaEvent_t>* ge =
           opt.profile ? next_event_pair(events_gs, events_gs_used) : nullptr;
       if (ge) CUDA_CHECK(cudaEventRecord(ge->first, st));
-      coll_->contact_solve();
+      coll_->contact_solve(done);
       if (ge) CUDA_CHECK(cudaEventRecord(ge->second, st));
     }
     launch_vertex_step(s, vertex_partials.p, vb, st);
     if (oe) CUDA_CHECK(cudaEventRecord(oe->second, st));
-    stats.admm_iterations += 1;
+    enqueued = it + 1;
     if (it == 0) continue;
     fa.iteration = it;
     launch_admm_finalize(fa, st);
-    AdmmControl h;
-    CUDA_CHECK(cudaMemcpyAsync(&h, ctl.p, sizeof(AdmmControl), cudaMemcpyDeviceToHost, st));
+    if (it % check_every != 0 && it + 1 < g.max_inner_iteration) continue;
+    CUDA_CHECK(cudaMemcpyAsync(&ctl_host_, ctl.p, sizeof(AdmmControl), cudaMemcpyDeviceToHost, st));
     sync();
-    if (h.diverged) return false;
-    if (h.converged) break;
-    rel = h.next_rel_tol;
+    if (ctl_host_.done) break;
   }
+  // Iterations that ran: 0 .. the last one finalized (the first has no
+  // finalize); each one from the second on ran one CG solve per cloth.
+  const int ran = enqueued <= 1 ? enqueued : ctl_host_.iteration + 1;
+  stats.admm_iterations += ran;
+  if (enqueued > 1) {
+    const int per_it_res = solve_resident_ / (enqueued - 1), per_it_cl = solve_cluster_ / (enqueued - 1);
+    stats.cg_resident_solves += per_it_res * (ran - 1);
+    stats.cg_cluster_solves += per_it_cl * (ran - 1);
+  }
+  if (ctl_host_.diverged) return false;
   launch_enforce(s, st);
   return true;
 }
@@ -1497,7 +1531,9 @@ silk_status World::solver_step() {
         CUDA_CHECK(cudaEventElapsedTime(&ms, events[e].first, events[e].second));
         prof.cg_time_ms += ms;
       }
-      prof.cg_launches += (int64_t)events_used;
+      // Solves that ran (launches of iterations enqueued after the ADMM
+      // solve ended return at entry; their events add a few us).
+      for (size_t k = 0; k < cloths.size(); ++k) prof.cg_launches += cgs[kCgStats * k + 1];
       for (size_t e = 0; e < events_gs_used; ++e) {
         float ms = 0.f;
         CUDA_CHECK(cudaEventElapsedTime(&ms, events_gs[e].first, events_gs[e].second));

@@ -223,6 +223,9 @@ class World {
   DevBuf<int> vf_off, vf_list;
   DevBuf<double> face_partials, vertex_partials;
   DevBuf<AdmmControl> ctl;
+  AdmmControl ctl_host_{};          // last control block read by admm_solve
+  const int* cg_skip_ = nullptr;    // AdmmControl::done while an ADMM solve is enqueued
+  int solve_resident_ = 0, solve_cluster_ = 0;  // CG launches of the solve, by form
   DevBuf<int> cg_fail;  // kFail* bits: a bounded device wait gave up, a bank pivot failed
   // Learned warm start: model, step history, features and training samples.
   DevBuf<float> mlp_params, mlp_out, warm_feat, warm_tgt;

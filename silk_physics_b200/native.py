@@ -79,7 +79,7 @@ class _SolverOptionsC(C.Structure):
                 ("learned_warm_start", C.c_int32), ("capture_samples", C.c_int32),
                 ("contact_gs_form", C.c_int32), ("admm_extrapolated_start", C.c_int32),
                 ("resident_halo_limit", C.c_int32), ("barrier_spin_limit", C.c_int32),
-                ("debug_withhold_block", C.c_int32)]
+                ("debug_withhold_block", C.c_int32), ("admm_check_interval", C.c_int32)]
 
 
 class _ProfileC(C.Structure):
@@ -174,6 +174,7 @@ class SolverOptions:
     resident_halo_limit: int = 0  # > 0: fewer halo slots per resident-CG block (0: 1024)
     barrier_spin_limit: int = 0  # > 0: polls before a CG grid-barrier wait gives up
     debug_withhold_block: int = 0  # k > 0: block k - 1 of a cooperative CG grid never arrives
+    admm_check_interval: int = 0  # ADMM iterations between host reads of the device's convergence state (0: 4)
 
     def to_c(self) -> _SolverOptionsC:
         o = _SolverOptionsC()
@@ -189,6 +190,7 @@ class SolverOptions:
         o.resident_halo_limit = int(self.resident_halo_limit)
         o.barrier_spin_limit = int(self.barrier_spin_limit)
         o.debug_withhold_block = int(self.debug_withhold_block)
+        o.admm_check_interval = int(self.admm_check_interval)
         return o
 
 

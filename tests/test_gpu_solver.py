@@ -1,4 +1,6 @@
 """GPU solver path against the oracle: ADMM + MAS-PCG + pins (no contacts)."""
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -243,6 +245,61 @@ def test_cg_rows_tensor_memory_identical(form_tm, form_global, s, bf16):
           f"(tensor memory) {out[1][0]} (global)")
     assert out[0][0] == out[1][0]
     np.testing.assert_array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("interval", [2, 4, 7])
+def test_device_decided_admm_iterations_identical(interval):
+    """The host reads the device's ADMM convergence state every
+    admm_check_interval iterations (1: after each, the reference's loop);
+    the iterations enqueued after convergence find AdmmControl::done set and
+    do nothing.  On the 80x80 contact scene from the stored state (three
+    steps: ADMM solves of tens to hundreds of iterations, CCD rollbacks,
+    contacts) and on config 1 (10 iterations, never converged): bit-identical
+    positions and the same ADMM / CG / contact counts."""
+    from silk_physics_b200 import scenes as SC
+    g = np.load(Path(__file__).resolve().parent / "golden" / "c2_contact.npz")
+    V, F, SV, SF = SC.c2_scene()
+
+    def run(iv, scene):
+        w = N.World()
+        assert w.init()
+        if scene == "c2":
+            assert w.set_global_config(N.GlobalConfig(acceleration_z=-9.81))
+            assert w.set_solver_options(N.SolverOptions(fixed_linear_rel_tol=1e-5,
+                                                        admm_check_interval=iv))
+            r, h = w.add_cloth(N.ClothConfig(), N.CollisionConfig(), V, F, [])
+            assert r
+            r, _ = w.add_obstacle(N.CollisionConfig(), SV, SF)
+            assert r
+            assert w.set_cloth_state(h, g["x0"], g["v0"])
+            n, steps = len(V), 3
+        else:
+            V1, F1 = S.grid_sheet(32, jitter=0.0, seed=7)
+            assert w.set_global_config(N.GlobalConfig(max_inner_iteration=10, admm_abs_tol=0.0,
+                                                      admm_rel_tol=0.0))
+            assert w.set_solver_options(N.SolverOptions(fixed_linear_rel_tol=1e-5,
+                                                        admm_check_interval=iv))
+            r, h = w.add_cloth(N.ClothConfig(), N.CollisionConfig(), V1, F1,
+                               S.top_corner_pins(32))
+            assert r
+            n, steps = len(V1), 4
+        counts = []
+        for _ in range(steps):
+            assert w.solver_step(), w
+            st = w.step_stats()
+            counts.append((st.admm_iterations, st.cg_iterations, st.cg_solves, st.contacts,
+                           st.outer_iterations, st.cg_resident_solves, st.cg_cluster_solves))
+        x = np.zeros(3 * n, np.float32)
+        assert w.get_cloth_position(h, x)
+        return counts, x
+
+    for scene in ("c2", "c1"):
+        c_ref, x_ref = run(1, scene)
+        c, x = run(interval, scene)
+        print(f"{scene} interval {interval}: (ADMM, CG, solves, contacts, outer, resident, cluster) "
+              f"{c} vs every iteration {c_ref}")
+        assert c == c_ref
+        np.testing.assert_array_equal(x, x_ref)
 
 
 @pytest.mark.parametrize("form", [0, 1])
