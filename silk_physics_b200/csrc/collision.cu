@@ -1148,11 +1148,14 @@ __global__ void activate_weights_kernel(const int* count, int nv, const float* b
 
 // One Jones-Plassmann round: a contact whose higher-priority neighbours are
 // all coloured takes the smallest colour none of them uses.
-__global__ void jp_round_kernel(const ContactDev* c, const unsigned long long* prio,
-                                int n, const int* off, const int* list, int* color,
-                                int* remaining, int* overflow) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || color[i] != 0) return;
+// One Jones-Plassmann step of contact i: 0 when a higher-priority neighbour
+// (sharing a movable vertex) is still uncoloured, else the smallest colour
+// none of them holds (1025 past 1,024 colours).  A neighbour coloured in the
+// same round may or may not be seen; either way contact i ends with the
+// smallest colour its higher-priority neighbours leave free, so the result
+// is the sequential greedy colouring in priority order.
+__device__ int jp_pick(const ContactDev* c, const unsigned long long* prio, int i,
+                       const int* off, const int* list, const int* color) {
   unsigned long long pi = prio[i];
   unsigned used[32];
   for (int k = 0; k < 32; ++k) used[k] = 0u;
@@ -1165,22 +1168,80 @@ __global__ void jp_round_kernel(const ContactDev* c, const unsigned long long* p
       unsigned long long pj = prio[j];
       bool higher = pj > pi || (pj == pi && j < i);
       if (!higher) continue;
-      int cj = ((volatile int*)color)[j];
-      if (cj == 0) {
-        atomicAdd(remaining, 1);
-        return;
-      }
+      int cj = ((const volatile int*)color)[j];
+      if (cj == 0) return 0;
       if (cj <= 1024) used[(cj - 1) >> 5] |= 1u << ((cj - 1) & 31);
     }
   }
   int col = 0;
   for (int k = 0; k < 32 && col == 0; ++k)
     if (used[k] != 0xffffffffu) col = 32 * k + __ffs(~used[k]);
-  if (col == 0) {
-    atomicAdd(overflow, 1);
-    col = 1025;
+  return col == 0 ? 1025 : col;
+}
+
+// Every round in one cooperative launch: one thread per contact (grid-
+// stride), the bounded grid barrier between rounds instead of launches and
+// host checks.  Round r counts its uncoloured contacts in rem[r % 3]; the
+// counter of round r + 1 is cleared during round r, after every block has
+// read it for round r - 2.  info: [0] highest colour, [1] contacts past
+// 1,024 colours, [3] set when a barrier wait gave up or the rounds ran out.
+constexpr int kJpMaxRounds = 4096;
+__global__ void jp_grid_kernel(const ContactDev* c, const unsigned long long* prio, int n,
+                               const int* off, const int* list, int* color, int* info, int* rem,
+                               unsigned* barrier, long long spin_limit) {
+  GridBarrier bar{barrier, barrier + 1, barrier + 2, gridDim.x};
+  if (spin_limit > 0) bar.limit = spin_limit;
+  const int stride = gridDim.x * blockDim.x;
+  for (int round = 0; round < kJpMaxRounds; ++round) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) rem[(round + 1) % 3] = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+      if (color[i] != 0) continue;
+      const int col = jp_pick(c, prio, i, off, list, color);
+      if (col == 0) {
+        atomicAdd(rem + round % 3, 1);
+        continue;
+      }
+      if (col > 1024) atomicAdd(info + 1, 1);
+      atomicMax(info, col);
+      color[i] = col;
+    }
+    if (!bar.sync()) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) info[3] = 1;  // a barrier wait gave up
+      return;
+    }
+    if (((volatile int*)rem)[round % 3] == 0) return;  // the same in every block
   }
-  color[i] = col;
+  if (blockIdx.x == 0 && threadIdx.x == 0) info[3] = 1;  // rounds exhausted
+}
+
+__global__ void iota_kernel(int n, int* v) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = i;
+}
+
+// Colour groups from the colours sorted ascending (stable, so contact index
+// order inside a colour): group_off[k] = first position of colour k + 1,
+// group_off[nc] = n; info[2] = the largest group.
+__global__ void group_offsets_kernel(const int* sorted, int n, int* info, int* group_off) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = info[0];
+  if (k > nc) return;
+  auto lower = [&](int key) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (sorted[mid] < key) lo = mid + 1;
+      else hi = mid;
+    }
+    return lo;
+  };
+  const int a = lower(k + 1);
+  group_off[k] = a;
+  if (k < nc) atomicMax(info + 2, lower(k + 2) - a);
+}
+
+__global__ void gs_nslots_kernel(const int* slot, const int* flag, int nv, int* info) {
+  info[4] = slot[nv - 1] + flag[nv - 1];
 }
 
 __global__ void contact_gs_kernel(const ContactDev* contacts, const int* groups,
@@ -1695,6 +1756,10 @@ struct CollisionImpl {
   bool gs_ready = false;
   DevBuf<int> active_dof;
   DevBuf<int> jp_flags;
+  // Colouring results read by the host once per contact build: highest
+  // colour, overflow, largest group, uncoloured left, Gauss-Seidel slots.
+  DevBuf<int> col_info, col_sorted, grp_in;
+  DevBuf<char> sort_temp;
   DevBuf<int> pick_d;  // DCD records picked as new contacts (grow-only)
   DevBuf<unsigned> gs_barrier;
   DevBuf<char> scan_temp;
@@ -1708,7 +1773,8 @@ CollisionSystem::CollisionSystem(World& w) : w_(w), impl_(new CollisionImpl) {
   impl_->counter.alloc(4);
   impl_->min_bits.alloc(1);
   impl_->ccd_counts.alloc(4 + 64);
-  impl_->jp_flags.alloc(2);
+  impl_->jp_flags.alloc(3);
+  impl_->col_info.alloc(5);
   impl_->gs_barrier.alloc(4);
   CUDA_CHECK(cudaMemset(impl_->gs_barrier.p, 0, 4 * sizeof(unsigned)));
 }
@@ -2193,48 +2259,57 @@ int CollisionSystem::append_active(float time, float dact) {
                                                            w_.contact_w.p, I.active_dof.p);
   SILK_LAUNCHED();
   last_dcd_build_ms = lap(t_lap);
-  // Colouring by Jones-Plassmann rounds, kJpBatch rounds between host
-  // checks: a round after the last contact is coloured changes nothing, so
-  // the colours equal those of checking after every round.  The overflow
-  // count accumulates over the rounds; the remaining count is per round.
-  constexpr int kJpBatch = 8;
+  // Colouring by Jones-Plassmann rounds, all in one cooperative launch (a
+  // round after the last contact is coloured changes nothing, so stopping
+  // at the first round that leaves none uncoloured gives the colours of the
+  // sequential greedy colouring in priority order).
   I.colors.alloc(total);
   I.colors.zero(st);
-  CUDA_CHECK(cudaMemsetAsync(I.jp_flags.p + 1, 0, sizeof(int), st));
-  for (int round = 0; round < 4096; round += kJpBatch) {
-    for (int b = 0; b < kJpBatch; ++b) {
-      CUDA_CHECK(cudaMemsetAsync(I.jp_flags.p, 0, sizeof(int), st));
-      jp_round_kernel<<<div_up(total, kCollThreads), kCollThreads, 0, st>>>(
-          I.contacts.p, I.prio.p, total, I.inc_off.p, I.inc_list.p, I.colors.p,
-          I.jp_flags.p, I.jp_flags.p + 1);
-      SILK_LAUNCHED();
-    }
-    int flags[2];
-    CUDA_CHECK(cudaMemcpyAsync(flags, I.jp_flags.p, sizeof(flags), cudaMemcpyDeviceToHost, st));
-    CUDA_CHECK(cudaStreamSynchronize(st));
-    if (flags[1] > 0) throw CudaError("Too many colors");
-    if (flags[0] == 0) break;
+  I.col_info.zero(st);
+  {
+    static const int max_coop = [] {
+      int dev = 0, sms = 0, per = 0;
+      CUDA_CHECK(cudaGetDevice(&dev));
+      CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, jp_grid_kernel, 256, 0));
+      return sms * std::max(per, 1);
+    }();
+    const int grid = std::min(max_coop, std::max(1, div_up(total, 256)));
+    CUDA_CHECK(cudaMemsetAsync(I.jp_flags.p, 0, 3 * sizeof(int), st));
+    CUDA_CHECK(cudaMemsetAsync(I.gs_barrier.p, 0, 2 * sizeof(unsigned), st));
+    const ContactDev* cp = I.contacts.p;
+    const unsigned long long* pp = I.prio.p;
+    int n = total;
+    const int* op = I.inc_off.p;
+    const int* lp = I.inc_list.p;
+    int* colp = I.colors.p;
+    int* infop = I.col_info.p;
+    int* remp = I.jp_flags.p;
+    unsigned* barp = I.gs_barrier.p;
+    long long limit = w_.opt.barrier_spin_limit;
+    void* args[] = {&cp, &pp, &n, &op, &lp, &colp, &infop, &remp, &barp, &limit};
+    CUDA_CHECK(cudaLaunchCooperativeKernel((const void*)jp_grid_kernel, dim3(grid), dim3(256),
+                                           args, 0, st));
+    SILK_LAUNCHED();
   }
-  std::vector<int> col(total);
-  CUDA_CHECK(cudaMemcpy(col.data(), I.colors.p, total * sizeof(int), cudaMemcpyDeviceToHost));
-  int nc = *std::max_element(col.begin(), col.end());
-  std::vector<int> off(nc + 2, 0), grp(total);
-  for (int c : col) off[c]++;
-  // off[c] counts colour c (1-based) -> exclusive prefix over colours 1..nc.
-  std::vector<int> start(nc + 1, 0);
-  for (int c = 1; c <= nc; ++c) start[c] = (c == 1 ? 0 : start[c - 1] + off[c - 1]);
-  std::vector<int> cur(start);
-  for (int i = 0; i < total; ++i) grp[cur[col[i]]++] = i;
-  std::vector<int> goff(nc + 1);
-  I.max_group = 0;
-  for (int c = 1; c <= nc; ++c) {
-    goff[c - 1] = start[c];
-    I.max_group = std::max(I.max_group, off[c]);
-  }
-  goff[nc] = total;
-  I.groups.upload(grp, st);
-  I.group_off.upload(goff, st);
-  I.n_colors = nc;
+  // Groups on the device: a stable sort of the contacts by colour (contact
+  // index order inside a colour) and the group offsets.
+  I.col_sorted.alloc(total);
+  I.grp_in.alloc(total);
+  I.groups.alloc(total);
+  I.group_off.alloc(1026);
+  iota_kernel<<<div_up(total, 256), 256, 0, st>>>(total, I.grp_in.p);
+  SILK_LAUNCHED();
+  size_t sb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, sb, I.colors.p, I.col_sorted.p, I.grp_in.p,
+                                  I.groups.p, total, 0, 11, st);
+  if (I.sort_temp.n < sb) I.sort_temp.alloc(sb);
+  CUDA_CHECK(cub::DeviceRadixSort::SortPairs(I.sort_temp.p, sb, I.colors.p, I.col_sorted.p,
+                                             I.grp_in.p, I.groups.p, total, 0, 11, st));
+  SILK_LAUNCHED();
+  group_offsets_kernel<<<div_up(1026, 256), 256, 0, st>>>(I.col_sorted.p, total, I.col_info.p,
+                                                          I.group_off.p);
+  SILK_LAUNCHED();
   last_dcd_color_ms = lap(t_lap);
   // Colour-ordered contacts on compact vertex slots for the single-block
   // Gauss-Seidel form.
@@ -2251,14 +2326,9 @@ int CollisionSystem::append_active(float time, float dact) {
     CUDA_CHECK(cub::DeviceScan::ExclusiveSum(I.scan_temp.p, tb2, I.gs_flag.p, I.gs_slot.p, nv,
                                              st));
     SILK_LAUNCHED();
-    int last[2] = {0, 0};
-    CUDA_CHECK(cudaMemcpyAsync(&last[0], I.gs_slot.p + nv - 1, sizeof(int),
-                               cudaMemcpyDeviceToHost, st));
-    CUDA_CHECK(cudaMemcpyAsync(&last[1], I.gs_flag.p + nv - 1, sizeof(int),
-                               cudaMemcpyDeviceToHost, st));
-    CUDA_CHECK(cudaStreamSynchronize(st));
-    I.gs_nslots = last[0] + last[1];
-    I.gs_vlist.alloc(std::max(I.gs_nslots, 1));
+    gs_nslots_kernel<<<1, 1, 0, st>>>(I.gs_slot.p, I.gs_flag.p, nv, I.col_info.p);
+    SILK_LAUNCHED();
+    I.gs_vlist.alloc(nv);  // the touched vertices are at most all of them
     gs_vlist_kernel<<<div_up(nv, 256), 256, 0, st>>>(I.gs_flag.p, I.gs_slot.p, nv, I.gs_vlist.p);
     SILK_LAUNCHED();
     I.gs_cc.alloc(total);
@@ -2268,7 +2338,14 @@ int CollisionSystem::append_active(float time, float dact) {
     SILK_LAUNCHED();
     I.gs_ready = true;
   }
+  // The one host read of the contact build's colouring and layout.
+  int info[5] = {0, 0, 0, 0, 0};
+  CUDA_CHECK(cudaMemcpyAsync(info, I.col_info.p, sizeof(info), cudaMemcpyDeviceToHost, st));
   CUDA_CHECK(cudaStreamSynchronize(st));
+  if (info[1] > 0 || info[3] > 0) throw CudaError("Too many colors");
+  I.n_colors = info[0];
+  I.max_group = info[2];
+  I.gs_nslots = info[4];
   last_dcd_layout_ms = lap(t_lap);
   return add;
 }
