@@ -1244,6 +1244,8 @@ __global__ void gs_nslots_kernel(const int* slot, const int* flag, int nv, int* 
   info[4] = slot[nv - 1] + flag[nv - 1];
 }
 
+
+
 __global__ void contact_gs_kernel(const ContactDev* contacts, const int* groups,
                                   const int* group_off, int ncolors, float4* corr,
                                   float4* p, unsigned* barrier, const int* skip) {
@@ -1307,7 +1309,7 @@ __global__ void contact_gs_kernel(const ContactDev* contacts, const int* groups,
 // in the same order as in contact_gs_kernel (contacts of one colour touch
 // disjoint vertices), so both forms give identical results.
 constexpr int kGsBlockThreads = 1024;
-constexpr size_t kGsBlockSmemMax = 200 * 1024;
+constexpr size_t kGsBlockSmemMax = 226 * 1024;
 
 struct GsContact {
   int slot[4];  // compact vertex slot, -1 kinematic
@@ -1361,6 +1363,33 @@ __global__ void gs_gather_kernel(const ContactDev* __restrict__ c, const int* __
       if (g.slot[a] >= 0 && g.slot[a] == g.slot[b]) distinct = false;
   g.ci = ci | (distinct ? (int)0x80000000u : 0);
   out[q] = g;
+}
+
+// Slot incidence of the colour-ordered contacts: entry e = 4 q + s (contact
+// position q, vertex s) keyed by its slot when the vertex moves (gamma != 0),
+// else by a key past every slot.  A stable sort by key leaves each slot's
+// entries in (q, s) order, i.e. in colour order.
+__global__ void gs_inc_keys_kernel(const GsContact* __restrict__ cc, int total, int* key,
+                                   int* val) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 4 * total) return;
+  const GsContact& k = cc[e >> 2];
+  const int s = e & 3;
+  key[e] = k.gamma[s] != 0.0f && k.slot[s] >= 0 ? k.slot[s] : 0x7fffffff;
+  val[e] = e;
+}
+// voff[i] = first entry of slot i in the sorted keys, for i <= nslots (info[4]).
+__global__ void gs_voff_kernel(const int* __restrict__ sorted, int n, const int* info, int nv,
+                               int* voff) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > nv || i > info[4]) return;
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (sorted[mid] < i) lo = mid + 1;
+    else hi = mid;
+  }
+  voff[i] = lo;
 }
 
 __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
@@ -1436,14 +1465,14 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
   for (int i = t; i < nslots; i += blockDim.x) p[vlist[i]] = sp[i];
 }
 
-// Pipelined single-block form: the contact records of the next kGsStages - 1
-// colour phases arrive in shared memory by bulk copies (one per colour: its
+// Pipelined single-block form: the contact records of the next ns - 1 colour
+// phases (ns = 4 staging stages, or 2 when 4 do not fit shared memory)
+// arrive in shared memory by bulk copies (one per colour: its
 // records are contiguous in colour order) while the current phase is
 // processed, each completing on its stage's mbarrier; the corrections and
 // colour offsets stay in shared memory for the whole call, so a phase never
 // waits on a global load.  Same per-contact operations as contact_gs_kernel.
-constexpr int kGsStages = 4;  // a power of two (stage = phase & (kGsStages - 1))
-static_assert((kGsStages & (kGsStages - 1)) == 0, "power of two");
+constexpr int kGsStages = 4;  // most stages (2 when 4 do not fit shared memory)
 static_assert(sizeof(GsContact) % 16 == 0, "bulk copies move whole 16-byte units");
 constexpr int kGsWaitSpins = 1 << 20;  // mbarrier polls before a phase gives up
 
@@ -1492,7 +1521,7 @@ struct GsPipeLayout {
 };
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 __host__ __device__ inline GsPipeLayout gs_pipe_layout(int nslots, int total, int ncolors,
-                                                       int threads) {
+                                                       int threads, int stages) {
   GsPipeLayout L;
   L.sp = 0;
   // Two extra position slots: nslots reads as zero (kinematic vertices),
@@ -1500,18 +1529,20 @@ __host__ __device__ inline GsPipeLayout gs_pipe_layout(int nslots, int total, in
   L.sc = align16(L.sp + (size_t)(nslots + 2) * sizeof(float4));
   L.go = align16(L.sc + (size_t)total * sizeof(float4));
   L.stage = align16(L.go + (size_t)(ncolors + 1) * sizeof(int));
-  L.bytes = L.stage + (size_t)kGsStages * threads * sizeof(GsContact);
+  L.bytes = L.stage + (size_t)stages * threads * sizeof(GsContact);
   return L;
 }
 
 __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
     const GsContact* __restrict__ cc, const int* __restrict__ group_off, int ncolors, int total,
     float4* __restrict__ corr, const int* __restrict__ vlist, int nslots, float4* __restrict__ p,
-    int* __restrict__ fail, const int* __restrict__ skip) {
+    int* __restrict__ fail, const int* __restrict__ skip, const int* __restrict__ voff,
+    const int* __restrict__ vinc, int ns_log) {
   if (skip && *skip) return;  // the ADMM solve already ended
   extern __shared__ __align__(16) unsigned char gs_raw[];
   __shared__ __align__(8) uint64_t bars[kGsStages];
-  const GsPipeLayout L = gs_pipe_layout(nslots, total, ncolors, blockDim.x);
+  const int ns = 1 << ns_log, nmask = ns - 1;  // staging stages: 2 or 4
+  const GsPipeLayout L = gs_pipe_layout(nslots, total, ncolors, blockDim.x, ns);
   float4* sp = reinterpret_cast<float4*>(gs_raw + L.sp);
   float4* sc = reinterpret_cast<float4*>(gs_raw + L.sc);
   int* sgo = reinterpret_cast<int*>(gs_raw + L.go);
@@ -1523,49 +1554,47 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
   for (int q = t; q < total; q += nt) sc[q] = corr[cc[q].ci & 0x7fffffff];
   for (int c = t; c <= ncolors; c += nt) sgo[c] = group_off[c];
   __syncthreads();
-  // Warm start with the saved corrections.
-  for (int col = 0; col < ncolors; ++col) {
-    int q = sgo[col] + t;
-    if (q < sgo[col + 1]) {
-      const GsContact& k = cc[q];
-      float4 r = sc[q];
-      for (int s = 0; s < 4; ++s) {
-        if (k.gamma[s] == 0.0f) continue;
-        float4 x = sp[k.slot[s]];
-        float g = k.gamma[s];
-        sp[k.slot[s]] = gs_move(x, g, make_float3(r.x, r.y, r.z));
-      }
+  // Warm start with the saved corrections: each slot applies those of its
+  // contacts in colour order (its entries of the slot incidence), the same
+  // moves in the same order as colour phases would, without their barriers.
+  for (int i = t; i < nslots; i += nt) {
+    float4 x = sp[i];
+    for (int e = voff[i]; e < voff[i + 1]; ++e) {
+      const int code = vinc[e], q = code >> 2;
+      const float4 r = sc[q];
+      x = gs_move(x, cc[q].gamma[code & 3], make_float3(r.x, r.y, r.z));
     }
-    __syncthreads();
+    sp[i] = x;
   }
+  __syncthreads();
   const int phases = kGsSweeps * ncolors;
   // The copies are issued by the block's last thread: its warp holds no
   // contact in most colours, so the issue stays off the contacts' path.
   const int producer = nt - 1;
   if (t == producer) {
-    for (int s = 0; s < kGsStages; ++s) mbar_init(&bars[s], 1);
+    for (int s = 0; s < ns; ++s) mbar_init(&bars[s], 1);
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   }
   __syncthreads();
-  // Copy the records of phase ph's colour into stage ph % kGsStages.  A
-  // thread reads its record of phase ph at the end of phase ph - 1, so the
-  // stage written at phase ph (for phase ph + kGsStages - 1) was last read in
-  // phase ph - 2, before a block barrier.
+  // Copy the records of phase ph's colour into stage ph % ns.  A thread reads
+  // its record of phase ph at the end of phase ph - 1, so the stage written
+  // at phase ph (for phase ph + ns - 1) was last read in phase ph - 2, before
+  // a block barrier.
   auto issue = [&](int ph, int col) {
     if (t != producer || ph >= phases) return;
-    uint64_t* bar = &bars[ph & (kGsStages - 1)];
+    uint64_t* bar = &bars[ph & nmask];
     const unsigned bytes = (unsigned)((sgo[col + 1] - sgo[col]) * (int)sizeof(GsContact));
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     if (bytes) {
       mbar_arrive_expect(bar, bytes);
-      bulk_copy_g2s(stage + (size_t)(ph & (kGsStages - 1)) * nt, cc + sgo[col], bytes, bar);
+      bulk_copy_g2s(stage + (size_t)(ph & nmask) * nt, cc + sgo[col], bytes, bar);
     } else {
       mbar_arrive(bar);
     }
   };
   int col_issue = 0;
 #pragma unroll
-  for (int s = 0; s < kGsStages - 1; ++s) {
+  for (int s = 0; s < ns - 1; ++s) {
     issue(s, col_issue);
     col_issue = col_issue + 1 == ncolors ? 0 : col_issue + 1;
   }
@@ -1579,10 +1608,10 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
   int qn = -1;
   bool lost = false;  // a copy this thread waited for did not land in time
   auto fetch = [&](int ph, int col) {
-    const bool landed = mbar_wait(&bars[ph & (kGsStages - 1)], (unsigned)(ph / kGsStages) & 1u);
+    const bool landed = mbar_wait(&bars[ph & nmask], (unsigned)(ph >> ns_log) & 1u);
     qn = sgo[col] + t;
     if (landed && qn < sgo[col + 1]) {
-      kn = stage[(size_t)(ph & (kGsStages - 1)) * nt + t];
+      kn = stage[(size_t)(ph & nmask) * nt + t];
       on = sc[qn];
     } else {
       qn = -1;
@@ -1593,7 +1622,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
   if (phases > 0) fetch(0, 0);
   int ph = 0;
   for (; ph < phases; ++ph) {
-    issue(ph + kGsStages - 1, col_issue);
+    issue(ph + ns - 1, col_issue);
     col_issue = col_issue + 1 == ncolors ? 0 : col_issue + 1;
     const int cur = qn;
     const GsContact kc = kn;
@@ -1633,8 +1662,8 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
     // flight, report the failure (the step then returns
     // IterativeSolveFail) and leave the positions untouched.
     if (t == producer) {
-      for (int q = ph; q < ph + kGsStages && q < phases; ++q)
-        mbar_wait(&bars[q & (kGsStages - 1)], (unsigned)(q / kGsStages) & 1u);
+      for (int q = ph; q < ph + ns && q < phases; ++q)
+        mbar_wait(&bars[q & nmask], (unsigned)(q >> ns_log) & 1u);
       if (fail) atomicOr(fail, kFailContactWait);
     }
     return;
@@ -1759,6 +1788,9 @@ struct CollisionImpl {
   // Colouring results read by the host once per contact build: highest
   // colour, overflow, largest group, uncoloured left, Gauss-Seidel slots.
   DevBuf<int> col_info, col_sorted, grp_in;
+  // Slot incidence of the colour-ordered contacts (entries 4 q + s, each
+  // slot's in colour order; gs_voff[slot] = its first entry).
+  DevBuf<int> gs_ikey, gs_ival, gs_ikey_s, gs_vinc, gs_voff;
   DevBuf<char> sort_temp;
   DevBuf<int> pick_d;  // DCD records picked as new contacts (grow-only)
   DevBuf<unsigned> gs_barrier;
@@ -2336,6 +2368,26 @@ int CollisionSystem::append_active(float time, float dact) {
     gs_gather_kernel<<<div_up(total, kCollThreads), kCollThreads, 0, st>>>(
         I.contacts.p, I.groups.p, total, I.gs_slot.p, I.gs_cc.p);
     SILK_LAUNCHED();
+    // Slot incidence in colour order for the pipelined form's warm start.
+    const int ne = 4 * total;
+    I.gs_ikey.alloc(ne);
+    I.gs_ival.alloc(ne);
+    I.gs_ikey_s.alloc(ne);
+    I.gs_vinc.alloc(ne);
+    I.gs_voff.alloc(nv + 1);
+    gs_inc_keys_kernel<<<div_up(ne, 256), 256, 0, st>>>(I.gs_cc.p, total, I.gs_ikey.p,
+                                                        I.gs_ival.p);
+    SILK_LAUNCHED();
+    size_t sb2 = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, sb2, I.gs_ikey.p, I.gs_ikey_s.p, I.gs_ival.p,
+                                    I.gs_vinc.p, ne, 0, 31, st);
+    if (I.sort_temp.n < sb2) I.sort_temp.alloc(sb2);
+    CUDA_CHECK(cub::DeviceRadixSort::SortPairs(I.sort_temp.p, sb2, I.gs_ikey.p, I.gs_ikey_s.p,
+                                               I.gs_ival.p, I.gs_vinc.p, ne, 0, 31, st));
+    SILK_LAUNCHED();
+    gs_voff_kernel<<<div_up(nv + 1, 256), 256, 0, st>>>(I.gs_ikey_s.p, ne, I.col_info.p, nv,
+                                                        I.gs_voff.p);
+    SILK_LAUNCHED();
     I.gs_ready = true;
   }
   // The one host read of the contact build's colouring and layout.
@@ -2367,7 +2419,14 @@ void CollisionSystem::contact_solve_launch() {
     // Only as many warps as the largest colour needs: every colour phase ends
     // in a block barrier, whose cost grows with the number of warps.
     const int threads = std::max(32, div_up(I.max_group, 32) * 32);
-    const GsPipeLayout L = gs_pipe_layout(I.gs_nslots, I.n_contacts, I.n_colors, threads);
+    // Four staging stages where they fit, else two (the copy for a colour is
+    // then issued one phase ahead instead of three).
+    int ns_log = 2;
+    GsPipeLayout L = gs_pipe_layout(I.gs_nslots, I.n_contacts, I.n_colors, threads, 4);
+    if (L.bytes > kGsBlockSmemMax) {
+      ns_log = 1;
+      L = gs_pipe_layout(I.gs_nslots, I.n_contacts, I.n_colors, threads, 2);
+    }
     if (L.bytes <= kGsBlockSmemMax) {
       static const bool pattr = [] {
         CUDA_CHECK(cudaFuncSetAttribute(contact_gs_pipe_kernel,
@@ -2378,7 +2437,7 @@ void CollisionSystem::contact_solve_launch() {
       (void)pattr;
       contact_gs_pipe_kernel<<<1, threads, L.bytes, st>>>(
           I.gs_cc.p, I.group_off.p, I.n_colors, I.n_contacts, I.corr.p, I.gs_vlist.p,
-          I.gs_nslots, w_.contact_p.p, w_.cg_fail.p, gs_skip_);
+          I.gs_nslots, w_.contact_p.p, w_.cg_fail.p, gs_skip_, I.gs_voff.p, I.gs_vinc.p, ns_log);
       SILK_LAUNCHED();
       return;
     }
