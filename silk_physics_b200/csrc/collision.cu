@@ -1465,14 +1465,14 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_block_kernel(
   for (int i = t; i < nslots; i += blockDim.x) p[vlist[i]] = sp[i];
 }
 
-// Pipelined single-block form: the contact records of the next ns - 1 colour
-// phases (ns = 4 staging stages, or 2 when 4 do not fit shared memory)
+// Pipelined single-block form: the contact records of the next ns colour
+// phases (ns = 4 staging stages, or 2 or 1 when 4 do not fit shared memory)
 // arrive in shared memory by bulk copies (one per colour: its
 // records are contiguous in colour order) while the current phase is
 // processed, each completing on its stage's mbarrier; the corrections and
 // colour offsets stay in shared memory for the whole call, so a phase never
 // waits on a global load.  Same per-contact operations as contact_gs_kernel.
-constexpr int kGsStages = 4;  // most stages (2 when 4 do not fit shared memory)
+constexpr int kGsStages = 4;  // most stages (2 or 1 when 4 do not fit shared memory)
 static_assert(sizeof(GsContact) % 16 == 0, "bulk copies move whole 16-byte units");
 constexpr int kGsWaitSpins = 1 << 20;  // mbarrier polls before a phase gives up
 
@@ -1541,7 +1541,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
   if (skip && *skip) return;  // the ADMM solve already ended
   extern __shared__ __align__(16) unsigned char gs_raw[];
   __shared__ __align__(8) uint64_t bars[kGsStages];
-  const int ns = 1 << ns_log, nmask = ns - 1;  // staging stages: 2 or 4
+  const int ns = 1 << ns_log, nmask = ns - 1;  // staging stages: 1, 2 or 4
   const GsPipeLayout L = gs_pipe_layout(nslots, total, ncolors, blockDim.x, ns);
   float4* sp = reinterpret_cast<float4*>(gs_raw + L.sp);
   float4* sc = reinterpret_cast<float4*>(gs_raw + L.sc);
@@ -1577,9 +1577,9 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
   }
   __syncthreads();
   // Copy the records of phase ph's colour into stage ph % ns.  A thread reads
-  // its record of phase ph at the end of phase ph - 1, so the stage written
-  // at phase ph (for phase ph + ns - 1) was last read in phase ph - 2, before
-  // a block barrier.
+  // its record of phase ph at the end of phase ph - 1, before that phase's
+  // block barrier, so at phase ph the stage of phase ph is free again and
+  // receives the records of phase ph + ns.
   auto issue = [&](int ph, int col) {
     if (t != producer || ph >= phases) return;
     uint64_t* bar = &bars[ph & nmask];
@@ -1594,7 +1594,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
   };
   int col_issue = 0;
 #pragma unroll
-  for (int s = 0; s < ns - 1; ++s) {
+  for (int s = 0; s < ns; ++s) {
     issue(s, col_issue);
     col_issue = col_issue + 1 == ncolors ? 0 : col_issue + 1;
   }
@@ -1620,9 +1620,10 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
   };
   int col = 0;
   if (phases > 0) fetch(0, 0);
+  __syncthreads();  // every thread has read stage 0 before phase 0 refills it
   int ph = 0;
   for (; ph < phases; ++ph) {
-    issue(ph + ns - 1, col_issue);
+    issue(ph + ns, col_issue);
     col_issue = col_issue + 1 == ncolors ? 0 : col_issue + 1;
     const int cur = qn;
     const GsContact kc = kn;
@@ -1662,7 +1663,9 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
     // flight, report the failure (the step then returns
     // IterativeSolveFail) and leave the positions untouched.
     if (t == producer) {
-      for (int q = ph; q < ph + ns && q < phases; ++q)
+      // Phase ph's copy completed before phase ph - 1's barrier; ph + 1 ..
+      // ph + ns may still be in flight.
+      for (int q = ph + 1; q <= ph + ns && q < phases; ++q)
         mbar_wait(&bars[q & nmask], (unsigned)(q >> ns_log) & 1u);
       if (fail) atomicOr(fail, kFailContactWait);
     }
@@ -2419,13 +2422,13 @@ void CollisionSystem::contact_solve_launch() {
     // Only as many warps as the largest colour needs: every colour phase ends
     // in a block barrier, whose cost grows with the number of warps.
     const int threads = std::max(32, div_up(I.max_group, 32) * 32);
-    // Four staging stages where they fit, else two (the copy for a colour is
-    // then issued one phase ahead instead of three).
+    // Four staging stages where they fit, else two, else one (the copy for a
+    // colour is then issued 4, 2 or 1 phases ahead).
     int ns_log = 2;
     GsPipeLayout L = gs_pipe_layout(I.gs_nslots, I.n_contacts, I.n_colors, threads, 4);
-    if (L.bytes > kGsBlockSmemMax) {
-      ns_log = 1;
-      L = gs_pipe_layout(I.gs_nslots, I.n_contacts, I.n_colors, threads, 2);
+    while (L.bytes > kGsBlockSmemMax && ns_log > 0) {
+      --ns_log;
+      L = gs_pipe_layout(I.gs_nslots, I.n_contacts, I.n_colors, threads, 1 << ns_log);
     }
     if (L.bytes <= kGsBlockSmemMax) {
       static const bool pattr = [] {
