@@ -1378,6 +1378,14 @@ __global__ void gs_inc_keys_kernel(const GsContact* __restrict__ cc, int total, 
   key[e] = k.gamma[s] != 0.0f && k.slot[s] >= 0 ? k.slot[s] : 0x7fffffff;
   val[e] = e;
 }
+// The sorted entries as (contact position, share bits) pairs.
+__global__ void gs_vent_kernel(const GsContact* __restrict__ cc, const int* __restrict__ code,
+                               int n, int2* __restrict__ vent) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const int c = code[e], q = c >> 2;
+  vent[e] = make_int2(q, __float_as_int(cc[q].gamma[c & 3]));
+}
 // voff[i] = first entry of slot i in the sorted keys, for i <= nslots (info[4]).
 __global__ void gs_voff_kernel(const int* __restrict__ sorted, int n, const int* info, int nv,
                                int* voff) {
@@ -1537,7 +1545,7 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
     const GsContact* __restrict__ cc, const int* __restrict__ group_off, int ncolors, int total,
     float4* __restrict__ corr, const int* __restrict__ vlist, int nslots, float4* __restrict__ p,
     int* __restrict__ fail, const int* __restrict__ skip, const int* __restrict__ voff,
-    const int* __restrict__ vinc, int ns_log) {
+    const int2* __restrict__ vent, int ns_log) {
   if (skip && *skip) return;  // the ADMM solve already ended
   extern __shared__ __align__(16) unsigned char gs_raw[];
   __shared__ __align__(8) uint64_t bars[kGsStages];
@@ -1557,12 +1565,20 @@ __global__ void __launch_bounds__(kGsBlockThreads) contact_gs_pipe_kernel(
   // Warm start with the saved corrections: each slot applies those of its
   // contacts in colour order (its entries of the slot incidence), the same
   // moves in the same order as colour phases would, without their barriers.
+  // A slot's entries (at most 8 per load round) are loaded together.
   for (int i = t; i < nslots; i += nt) {
     float4 x = sp[i];
-    for (int e = voff[i]; e < voff[i + 1]; ++e) {
-      const int code = vinc[e], q = code >> 2;
-      const float4 r = sc[q];
-      x = gs_move(x, cc[q].gamma[code & 3], make_float3(r.x, r.y, r.z));
+    const int e1 = voff[i + 1];
+    for (int e0 = voff[i]; e0 < e1; e0 += 8) {
+      int2 en[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) en[k] = e0 + k < e1 ? vent[e0 + k] : make_int2(0, 0);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (e0 + k >= e1) break;
+        const float4 r = sc[en[k].x];
+        x = gs_move(x, __int_as_float(en[k].y), make_float3(r.x, r.y, r.z));
+      }
     }
     sp[i] = x;
   }
@@ -1794,6 +1810,7 @@ struct CollisionImpl {
   // Slot incidence of the colour-ordered contacts (entries 4 q + s, each
   // slot's in colour order; gs_voff[slot] = its first entry).
   DevBuf<int> gs_ikey, gs_ival, gs_ikey_s, gs_vinc, gs_voff;
+  DevBuf<int2> gs_vent;  // sorted entries as (contact position, share bits)
   DevBuf<char> sort_temp;
   DevBuf<int> pick_d;  // DCD records picked as new contacts (grow-only)
   DevBuf<unsigned> gs_barrier;
@@ -2391,6 +2408,9 @@ int CollisionSystem::append_active(float time, float dact) {
     gs_voff_kernel<<<div_up(nv + 1, 256), 256, 0, st>>>(I.gs_ikey_s.p, ne, I.col_info.p, nv,
                                                         I.gs_voff.p);
     SILK_LAUNCHED();
+    I.gs_vent.alloc(ne);
+    gs_vent_kernel<<<div_up(ne, 256), 256, 0, st>>>(I.gs_cc.p, I.gs_vinc.p, ne, I.gs_vent.p);
+    SILK_LAUNCHED();
     I.gs_ready = true;
   }
   // The one host read of the contact build's colouring and layout.
@@ -2440,7 +2460,7 @@ void CollisionSystem::contact_solve_launch() {
       (void)pattr;
       contact_gs_pipe_kernel<<<1, threads, L.bytes, st>>>(
           I.gs_cc.p, I.group_off.p, I.n_colors, I.n_contacts, I.corr.p, I.gs_vlist.p,
-          I.gs_nslots, w_.contact_p.p, w_.cg_fail.p, gs_skip_, I.gs_voff.p, I.gs_vinc.p, ns_log);
+          I.gs_nslots, w_.contact_p.p, w_.cg_fail.p, gs_skip_, I.gs_voff.p, I.gs_vent.p, ns_log);
       SILK_LAUNCHED();
       return;
     }
