@@ -1462,9 +1462,47 @@ __device__ __forceinline__ float3 dsm_row(const int2* e, int rw, const float4* p
 
 // dsm_row with the row entries read from tensor memory, eight per load (the
 // entries of dsm_row in the same order, so the same sums).
-__device__ __forceinline__ float3 dsm_row_tmem(unsigned taddr, int rw, const float4* pl, float d,
-                                               float3 pv) {
+// 48 columns (24 entries) of this thread's lane in flight at once, one wait.
+__device__ __forceinline__ void tmem_ld48_wait(unsigned taddr, unsigned (&v)[48]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+      "%28, %29, %30, %31}, [%48];\n"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%32, %33, %34, %35, %36, %37, %38, %39, %40, "
+      "%41, %42, %43, %44, %45, %46, %47}, [%49];\n"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+        "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+        "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+        "=r"(v[31]), "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]), "=r"(v[36]),
+        "=r"(v[37]), "=r"(v[38]), "=r"(v[39]), "=r"(v[40]), "=r"(v[41]), "=r"(v[42]),
+        "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47])
+      : "r"(taddr), "r"(taddr + 32u)
+      : "memory");
+}
+
+__device__ __forceinline__ float3 dsm_row_tmem(unsigned taddr, int rw, int tm_rw,
+                                               const float4* pl, float d, float3 pv) {
   float yx = d * pv.x, yy = d * pv.y, yz = d * pv.z;
+  if (rw <= 24 && tm_rw >= 24) {
+    // The whole row behind one wait (rw is the same in the warp; the warp's
+    // columns hold at least 24 entries, so the 48 read are its own).
+    unsigned e[48];
+    tmem_ld48_wait(taddr, e);
+#pragma unroll
+    for (int k = 0; k < 24; ++k) {
+      if (k < rw) {
+        const float val = __uint_as_float(e[2 * k + 1]);
+        const float4 pj = pl[-1 - (int)e[2 * k]];
+        yx = fmaf(val, pj.x, yx);
+        yy = fmaf(val, pj.y, yy);
+        yz = fmaf(val, pj.z, yz);
+      }
+    }
+    return make_float3(yx, yy, yz);
+  }
   for (int j0 = 0; j0 < rw; j0 += 8) {
     unsigned e[16];
     tmem_ld16_wait(taddr + 2 * j0, e);
@@ -1627,7 +1665,7 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     }
   }
   auto row = [&](float3 pv) {
-    return tm ? dsm_row_tmem(taddr, rw, s.pl, d, pv) : dsm_row(erow, rw, s.pl, d, pv);
+    return tm ? dsm_row_tmem(taddr, rw, a.tm_rw, s.pl, d, pv) : dsm_row(erow, rw, s.pl, d, pv);
   };
   // Every warp's tensor-memory accesses are complete before warp 0 frees it.
   auto tm_release = [&]() {
