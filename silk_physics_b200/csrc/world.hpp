@@ -56,9 +56,15 @@ struct DevBuf {
       n = count;
       return;
     }
+    // A growing size (the contact build's buffers follow the contact count
+    // from call to call) takes at least half the capacity more each time, so
+    // it reallocates a logarithmic number of times.
+    const size_t grown = cap + cap / 2;
+    const size_t c = count > grown ? count : grown;
     reset();
-    n = cap = count;
-    if (count) CUDA_CHECK(cudaMalloc(&p, count * sizeof(T)));
+    cap = c;
+    n = count;
+    if (c) CUDA_CHECK(cudaMalloc(&p, c * sizeof(T)));
   }
   void zero(cudaStream_t st) {
     if (n) CUDA_CHECK(cudaMemsetAsync(p, 0, n * sizeof(T), st));
