@@ -715,6 +715,8 @@ struct DfsStack {
     ++n;
     return true;
   }
+  // t.lower of the box pop() would return (n > 0).
+  __device__ __forceinline__ float top_t0() const { return heap ? e[0].t0 : e[n - 1].t0; }
   __device__ IBox pop() {
     if (!heap) return e[--n];
     const IBox top = e[0];
@@ -836,15 +838,28 @@ __device__ int root_finder(bool vf, const float3* Pt, const float* tol,
       first.v1 = mid;
       second.v0 = mid;
     }
+    // The first half, pushed last, is the next box taken whenever no
+    // pending box has a smaller t.lower (it is the most recent of any equal
+    // ones): it then stays the current box instead of going through the
+    // pending store and straight back, which leaves the order of the search
+    // unchanged.
+    auto push_first = [&]() -> bool {
+      if (st.n == 0 || first.t0 <= st.top_t0()) {
+        cur = first;
+        has_cur = true;
+        return true;
+      }
+      return push(first);
+    };
     bool ok = true;
     if (split == 0 || !vf) {
-      ok = push(second) && push(first);
+      ok = push(second) && push_first();
     } else {
       float other_lo = split == 1 ? cur.v0 : cur.u0;
       float s_lo = split == 1 ? second.u0 : second.v0;
       float f_lo = split == 1 ? first.u0 : first.v0;
       if (s_lo + other_lo <= 1.0f) ok = push(second);
-      if (ok && f_lo + other_lo <= 1.0f) ok = push(first);
+      if (ok && f_lo + other_lo <= 1.0f) ok = push_first();
     }
     if (!ok) {
       result = cur;
