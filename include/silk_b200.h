@@ -146,7 +146,8 @@ typedef struct {
   int64_t cg_launches;
   int64_t cg_iterations;
   double cg_algorithmic_bytes;
-  double admm_other_ms;      /* events: face/vertex/contact kernels */
+  double admm_other_ms;      /* events: face/vertex/contact kernels and the
+                                convergence test run by the vertex step */
   double admm_host_ms;       /* host wall time of ADMM control (syncs) */
   double ccd_host_ms;        /* host wall time of refit + CCD */
   double dcd_host_ms;        /* host wall time of DCD + contact rebuild */

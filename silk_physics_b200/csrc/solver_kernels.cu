@@ -124,11 +124,33 @@ __global__ void inertia_kernel(SolverView s) {
   s.inertia[i] = o;
 }
 
+// initialize_aux (contact_constraints.cu:203-215): p <- x - eta / w.
+__device__ __forceinline__ void contact_init(const SolverView& s, int i) {
+  if (i >= s.nv) return;
+  float w = s.contact_w[i];
+  float4 p = s.contact_p[i];
+  s.contact_p_prev[i] = p;
+  float4 x = s.x[i];
+  if (w > 0.0f) {
+    float4 e = s.contact_eta[i];
+    p = make_float4(x.x - e.x / w, x.y - e.y / w, x.z - e.z / w, 0.f);
+  } else {
+    p = x;
+  }
+  s.contact_p[i] = p;
+}
+
 // solve_and_update_elastic_aux (cloth_admm_helper.cu:81-201) without the
-// per-vertex dual scatter, which the vertex kernel gathers instead.
-__global__ void __launch_bounds__(THREADS) face_step_kernel(SolverView s,
-                                                            double* partials) {
+// per-vertex dual scatter, which the vertex kernel gathers instead.  Blocks
+// from face_blocks on initialise the contacts' auxiliary positions instead
+// (they touch none of the faces' arrays), so one launch does both.
+__global__ void __launch_bounds__(THREADS) face_step_kernel(SolverView s, double* partials,
+                                                            int face_blocks) {
   if (s.skip && *s.skip) return;  // the ADMM solve already ended
+  if ((int)blockIdx.x >= face_blocks) {
+    contact_init(s, ((int)blockIdx.x - face_blocks) * blockDim.x + threadIdx.x);
+    return;
+  }
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[3] = {0.0, 0.0, 0.0};
   if (f < s.nf) {
@@ -177,33 +199,20 @@ __global__ void __launch_bounds__(THREADS) face_step_kernel(SolverView s,
   block_reduce_store<3>(acc, partials + (size_t)blockIdx.x * kAdmmSlots);
 }
 
-// initialize_aux (contact_constraints.cu:203-215): p <- x - eta / w.
-__global__ void contact_init_kernel(SolverView s) {
-  if (s.skip && *s.skip) return;  // the ADMM solve already ended
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= s.nv) return;
-  float w = s.contact_w[i];
-  float4 p = s.contact_p[i];
-  s.contact_p_prev[i] = p;
-  float4 x = s.x[i];
-  if (w > 0.0f) {
-    float4 e = s.contact_eta[i];
-    p = make_float4(x.x - e.x / w, x.y - e.y / w, x.z - e.z / w, 0.f);
-  } else {
-    p = x;
-  }
-  s.contact_p[i] = p;
-}
+__device__ void admm_finalize(const AdmmFinalizeArgs& a);
 
 // Per-vertex part of one ADMM iteration: pin multiplier update and primal
 // residual (equality_constraints.cu:49-104), contact multiplier update
 // (contact_constraints.cu:320-374), dual residual gathered over incident
 // faces, finiteness check, and assembly of the next x-update system
 // (cloth_admm_helper.cu:203-271, equality_constraints.cu:66-80,
-// contact_constraints.cu:302-318).
+// contact_constraints.cu:302-318).  The last block to store its partials
+// (a ticket in the control block) then runs the iteration's convergence
+// test, from iteration 1 on (fa.iteration > 0).
 __global__ void __launch_bounds__(THREADS) vertex_step_kernel(SolverView s,
-                                                              double* partials) {
+                                                              AdmmFinalizeArgs fa) {
   if (s.skip && *s.skip) return;  // the ADMM solve already ended
+  double* partials = fa.vertex_partials;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   if (i < s.nv) {
@@ -295,10 +304,25 @@ __global__ void __launch_bounds__(THREADS) vertex_step_kernel(SolverView s,
     s.rhs[i] = make_float4(rhs[0], rhs[1], rhs[2], 0.f);
   }
   block_reduce_store<7>(acc, partials + (size_t)blockIdx.x * kAdmmSlots);
+  // Thread 0 stored this block's partials: fence them, then take a ticket.
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&fa.ctl->ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x == 0) fa.ctl->ticket = 0u;  // for the next iteration's launch
+  if (fa.iteration > 0) admm_finalize(fa);
 }
 
-__global__ void admm_finalize_kernel(AdmmFinalizeArgs a) {
-  if (a.ctl->done) return;  // the ADMM solve already ended
+// Convergence test of one ADMM iteration (admm_solver.cu:209-330): the block
+// sums the face and vertex partials slot by slot in a fixed order (lanes
+// stride the blocks, then a shuffle tree) and thread 0 updates the control
+// block.  Partials are read from L2: the vertex partials come from other
+// blocks of the launch that runs this.
+__device__ void admm_finalize(const AdmmFinalizeArgs& a) {
   __shared__ double sh[kAdmmSlots][32];
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // warp k < 3 sums face slot k, warps 3.. sum vertex slots.
@@ -306,9 +330,9 @@ __global__ void admm_finalize_kernel(AdmmFinalizeArgs a) {
     double s = 0.0;
     if (slot < 3)
       for (int b = lane; b < a.face_blocks; b += 32)
-        s += a.face_partials[(size_t)b * kAdmmSlots + slot];
+        s += __ldcg(a.face_partials + (size_t)b * kAdmmSlots + slot);
     for (int b = lane; b < a.vertex_blocks; b += 32)
-      s += a.vertex_partials[(size_t)b * kAdmmSlots + slot];
+      s += __ldcg(a.vertex_partials + (size_t)b * kAdmmSlots + slot);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if (lane == 0) sh[slot][0] = s;
@@ -420,25 +444,15 @@ void launch_compute_inertia(const SolverView& s, cudaStream_t st) {
   SILK_LAUNCHED();
 }
 
-void launch_face_step(const SolverView& s, double* partials, int nblocks,
+void launch_face_step(const SolverView& s, double* partials, int nblocks, bool contact_init,
                       cudaStream_t st) {
-  face_step_kernel<<<nblocks, THREADS, 0, st>>>(s, partials);
+  const int init_blocks = contact_init ? div_up(s.nv, THREADS) : 0;
+  face_step_kernel<<<nblocks + init_blocks, THREADS, 0, st>>>(s, partials, nblocks);
   SILK_LAUNCHED();
 }
 
-void launch_contact_init(const SolverView& s, cudaStream_t st) {
-  contact_init_kernel<<<div_up(s.nv, THREADS), THREADS, 0, st>>>(s);
-  SILK_LAUNCHED();
-}
-
-void launch_vertex_step(const SolverView& s, double* partials, int nblocks,
-                        cudaStream_t st) {
-  vertex_step_kernel<<<nblocks, THREADS, 0, st>>>(s, partials);
-  SILK_LAUNCHED();
-}
-
-void launch_admm_finalize(const AdmmFinalizeArgs& a, cudaStream_t st) {
-  admm_finalize_kernel<<<1, 256, 0, st>>>(a);
+void launch_vertex_step(const SolverView& s, const AdmmFinalizeArgs& fa, cudaStream_t st) {
+  vertex_step_kernel<<<fa.vertex_blocks, THREADS, 0, st>>>(s, fa);
   SILK_LAUNCHED();
 }
 

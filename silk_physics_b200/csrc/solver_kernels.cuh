@@ -72,32 +72,39 @@ struct AdmmControl {
   // Set with converged or diverged: the iterations the host enqueued beyond
   // this one find it at entry and do nothing.
   int done;
-  int pad[6];
+  // Blocks of the running vertex step that have stored their partials; the
+  // last one runs the convergence test and sets it back to 0.
+  unsigned ticket;
+  int pad[5];
 };
+static_assert(sizeof(AdmmControl) == 64, "one control block of 64 bytes");
 
 void launch_compute_inertia(const SolverView& s, cudaStream_t st);
-void launch_face_step(const SolverView& s, double* partials, int nblocks,
+// Face step (local elastic projection, residual partials) of one ADMM
+// iteration; with contact_init, the same launch also sets the contacts'
+// auxiliary positions (initialize_aux).
+void launch_face_step(const SolverView& s, double* partials, int nblocks, bool contact_init,
                       cudaStream_t st);
 int face_step_blocks(int nf);
 int vertex_step_blocks(int nv);
-void launch_contact_init(const SolverView& s, cudaStream_t st);
-void launch_vertex_step(const SolverView& s, double* partials, int nblocks,
-                        cudaStream_t st);
 struct AdmmFinalizeArgs {
   const double* face_partials;
   int face_blocks;
-  const double* vertex_partials;
+  double* vertex_partials;
   int vertex_blocks;
   int dof_primal_static;     // 6 * faces + pinned dof
   const int* contact_active_dof;  // device scalar (may be null)
   int state_dof;
   float abs_tol, rel_tol;
   float init_lin_rel, lin_rel_min, lin_rel_max, fixed_rel;
-  int iteration;
+  int iteration;  // 0: the first iteration, which has no convergence test
   AdmmControl* ctl;
   const int* cg_fail = nullptr;  // set when a CG barrier wait gave up
 };
-void launch_admm_finalize(const AdmmFinalizeArgs& a, cudaStream_t st);
+// Vertex step (multiplier updates, dual residual, next system's right-hand
+// side) of one ADMM iteration on fa.vertex_blocks blocks; its last block to
+// finish runs the iteration's convergence test into fa.ctl.
+void launch_vertex_step(const SolverView& s, const AdmmFinalizeArgs& fa, cudaStream_t st);
 void launch_enforce(const SolverView& s, cudaStream_t st);
 void launch_predict(int nv, float dt, float4 acc, const float4* x,
                     const float4* v, float4* out, cudaStream_t st);

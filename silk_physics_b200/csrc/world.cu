@@ -1337,21 +1337,19 @@ bool World::admm_solve() {
     }
     std::pair<cudaEvent_t, cudaEvent_t>* oe = opt.profile ? next_event_pair(events_other, events_other_used) : nullptr;
     if (oe) CUDA_CHECK(cudaEventRecord(oe->first, st));
-    launch_face_step(s, face_partials.p, fb, st);
+    launch_face_step(s, face_partials.p, fb, contacts, st);
     if (contacts) {
-      launch_contact_init(s, st);
       std::pair<cudaEvent_t, cudaEvent_t>* ge =
           opt.profile ? next_event_pair(events_gs, events_gs_used) : nullptr;
       if (ge) CUDA_CHECK(cudaEventRecord(ge->first, st));
       coll_->contact_solve(done);
       if (ge) CUDA_CHECK(cudaEventRecord(ge->second, st));
     }
-    launch_vertex_step(s, vertex_partials.p, vb, st);
+    fa.iteration = it;
+    launch_vertex_step(s, fa, st);
     if (oe) CUDA_CHECK(cudaEventRecord(oe->second, st));
     enqueued = it + 1;
     if (it == 0) continue;
-    fa.iteration = it;
-    launch_admm_finalize(fa, st);
     if (it % check_every != 0 && it + 1 < g.max_inner_iteration) continue;
     CUDA_CHECK(cudaMemcpyAsync(&ctl_host_, ctl.p, sizeof(AdmmControl), cudaMemcpyDeviceToHost, st));
     sync();
