@@ -128,6 +128,31 @@ __device__ __forceinline__ double warp_sum_d(double v) {
   return v;
 }
 
+// One lane's share of a fixed-order sum over per-block partials (4 doubles
+// per block, slot `slot`): the values of blocks lane, lane + 32, ... added in
+// that order, as the strided loop would, with the first kLoads of them loaded
+// from L2 before the first add (one round trip instead of one per value).  An
+// absent value adds +0.0, which leaves a sum started at +0.0 unchanged bit
+// for bit (such a sum is never -0.0).
+template <int kLoads>
+__device__ __forceinline__ double lane_partials(const double* partials, int slot, int nblocks,
+                                                int lane) {
+  double v[kLoads];
+#pragma unroll
+  for (int k = 0; k < kLoads; ++k) {
+    const int b = lane + 32 * k;
+    v[k] = b < nblocks ? __ldcg(partials + 4 * b + slot) : 0.0;
+  }
+  double a = 0.0;
+#pragma unroll
+  for (int k = 0; k < kLoads; ++k) a += v[k];
+  for (int b = lane + 32 * kLoads; b < nblocks; b += 32) a += __ldcg(partials + 4 * b + slot);
+  return a;
+}
+// Loads in flight per lane for the resident form's totals: its cooperative
+// grid has one block per SM (148 on B200), at most 160 blocks in one round.
+constexpr int kResPartialLoads = 5;
+
 // Block-level sum of per-thread doubles into out[k] (thread 0 writes).
 template <int N>
 __device__ void block_sum(double (&v)[N], double* out) {
@@ -717,8 +742,7 @@ __device__ void res_block_sum(const double (&v)[N], ResShared& s, double* out) {
 // Sum of slot `slot` of every block's partials, the same in every block.
 __device__ double res_total(const double* partials, int slot, int nblocks, ResShared& s) {
   if (threadIdx.x < 32) {
-    double a = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += 32) a += __ldcg(partials + 4 * b + slot);
+    double a = lane_partials<kResPartialLoads>(partials, slot, nblocks, threadIdx.x);
     a = warp_sum_d(a);
     if (threadIdx.x == 0) s.tot[slot] = a;
   }
@@ -1060,22 +1084,13 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
   };
   // Phase A head: totals and the redundant coarse levels >= 2.
   auto totals = [&](double& rz, double& rr) {
-    // One round trip: warp 0 sums the partials while the other warps load the
-    // residual restricted to the second coarse level.
-    if (warp == 0) {
-      double s0 = 0.0, s1 = 0.0;
-      for (int q = lane; q < nblocks; q += 32) {
-        s0 += __ldcg(a.partials + 4 * q);
-        s1 += __ldcg(a.partials + 4 * q + 1);
-      }
-      s0 = warp_sum_d(s0);
-      s1 = warp_sum_d(s1);
-      if (lane == 0) {
-        s.tot[0] = s0;
-        s.tot[1] = s1;
-      }
+    // One round trip: warps 0 and 1 sum the two totals' partials while the
+    // other warps load the residual restricted to the second coarse level.
+    if (warp < 2) {
+      const double t = warp_sum_d(lane_partials<kResPartialLoads>(a.partials, warp, nblocks, lane));
+      if (lane == 0) s.tot[warp] = t;
     } else if (a.levels > 1) {
-      for (int i = tid - 32; i < a.coarse[1].nnode; i += kResThreads - 32)
+      for (int i = tid - 64; i < a.coarse[1].nnode; i += kResThreads - 64)
         s.rc[i] = ldcg4(a.coarse[0].rout + i);
     }
     __syncthreads();
