@@ -97,7 +97,8 @@ struct CgArgs {
   int* fail = nullptr;          // kFail* bits: a barrier wait gave up
   // Device-decided ADMM iterations: the kernel returns at entry when *skip is
   // set (the ADMM solve already ended) and takes its relative tolerance from
-  // *rel_tol_dev (the finalize kernel's next tolerance) when not null.
+  // *rel_tol_dev (the next tolerance set by the ADMM convergence test) when
+  // not null.
   const int* skip = nullptr;
   const float* rel_tol_dev = nullptr;
   long long barrier_spin_limit = 0;  // > 0: grid-barrier polls before giving up

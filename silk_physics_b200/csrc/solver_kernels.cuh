@@ -59,7 +59,7 @@ enum AdmmSlot {
 };
 
 struct AdmmControl {
-  // Written by the finalize kernel, read by the host each iteration.
+  // Written by the convergence test, read by the host every few iterations.
   int converged;
   int diverged;
   float next_rel_tol;

@@ -1214,8 +1214,9 @@ bool World::admm_solve() {
   float rel = std::min(std::max(g.initial_linear_rel_tol, g.linear_solver_rel_tol_min),
                        g.linear_solver_rel_tol_max);
   if (opt.fixed_linear_rel_tol > 0) rel = opt.fixed_linear_rel_tol;
-  // Iterations are decided on the device: the finalize kernel sets
-  // AdmmControl::done when the solve converges or diverges, and every kernel
+  // Iterations are decided on the device: the convergence test (run by the
+  // vertex step's last block) sets AdmmControl::done when the solve
+  // converges or diverges, and every kernel
   // of a later iteration returns at entry; the host enqueues
   // admm_check_interval iterations between reads of the control block, so
   // the GPU does not idle on a host round trip after every iteration.  The
