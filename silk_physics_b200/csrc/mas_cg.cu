@@ -454,7 +454,7 @@ __device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm
   spmv_phase(a, a.x, a.r, 1);
   if (!bar.sync()) return mark_fail(a);
   // Alternative start (see CgArgs::x_alt): its residual goes to Ap.
-  double rr_judge = -1.0;
+  double rr_plain0 = -1.0;
   if (a.x_alt) {
     spmv_phase(a, a.x_alt, a.Ap, 1);
     if (!bar.sync()) return mark_fail(a);
@@ -473,7 +473,7 @@ __device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm
     const double r_pa = grid_total(a.partials, 1, gridDim.x);
     const double rr_alt = grid_total(a.partials, 2, gridDim.x);
     if (!bar.sync()) return mark_fail(a);
-    rr_judge = rr_plain;
+    rr_plain0 = rr_plain;
     const float w = (float)blend_weight(rr_plain, r_pa, rr_alt);
     if (w > 0.0f) {
       for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nv; i += gridDim.x * blockDim.x) {
@@ -508,7 +508,7 @@ __device__ __forceinline__ void cg_body(const CgArgs& a, Barrier& bar, float* sm
     }
     return;
   }
-  const double rr0 = rr_judge >= 0.0 ? rr_judge : rr;
+  const double rr0 = rr_plain0 >= 0.0 ? rr_plain0 : rr;
   const double abs2 = (double)a.abs_tol * a.abs_tol;
   const float rel_tol = a.rel_tol_dev ? *a.rel_tol_dev : a.rel_tol;
   const double rel2 = (double)rel_tol * rel_tol;
@@ -990,7 +990,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
   // Alternative start: residual of x_alt (published through the Ap buffer),
   // both residual norms summed over the grid, the smaller start taken by
   // every block alike; the plain start's norm stays the stopping reference.
-  double rr_judge = -1.0;
+  double rr_plain0 = -1.0;
   if (a.x_alt) {
     float3 xa = make_float3(0.f, 0.f, 0.f);
     if (own) {
@@ -1018,7 +1018,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     // Every block reads the partials before any block overwrites them in the
     // next phase.
     if (!bar.sync()) return fail();
-    rr_judge = rr_plain;
+    rr_plain0 = rr_plain;
     const float w = (float)blend_weight(rr_plain, r_pa, rr_alt);
     if (w > 0.0f) {
       x = make_float3(x.x + w * (xa.x - x.x), x.y + w * (xa.y - x.y), x.z + w * (xa.z - x.z));
@@ -1234,7 +1234,7 @@ __device__ void res_body(const CgArgs& a, Barrier& bar, ResShared& s) {
     tm_release();
     return;
   }
-  const double rr0 = rr_judge >= 0.0 ? rr_judge : rr;
+  const double rr0 = rr_plain0 >= 0.0 ? rr_plain0 : rr;
   const double abs2 = (double)a.abs_tol * a.abs_tol;
   const float rel_tol = a.rel_tol_dev ? *a.rel_tol_dev : a.rel_tol;
   const double rel2 = (double)rel_tol * rel_tol;
@@ -1722,7 +1722,7 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     float3 y = row(x);
     r = own ? make_float3(b.x - y.x, b.y - y.y, b.z - y.z) : make_float3(0.f, 0.f, 0.f);
   }
-  double rr_judge = -1.0;
+  double rr_plain0 = -1.0;
   if (a.x_alt) {
     float3 xa = make_float3(0.f, 0.f, 0.f);
     if (own) {
@@ -1747,7 +1747,7 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     push_partials(3, t3, 3);
     cl.sync();
     const double rr_plain = total(3), r_pa = total(4), rr_alt = total(5);
-    rr_judge = rr_plain;
+    rr_plain0 = rr_plain;
     const float w = (float)blend_weight(rr_plain, r_pa, rr_alt);
     if (w > 0.0f) {
       x = make_float3(x.x + w * (xa.x - x.x), x.y + w * (xa.y - x.y), x.z + w * (xa.z - x.z));
@@ -1887,7 +1887,7 @@ __global__ void __launch_bounds__(32 * F, 1) cg_dsm_cluster_kernel(CgArgs a) {
     tm_release();
     return;  // every CTA takes the same decision; no store is in flight
   }
-  const double rr0 = rr_judge >= 0.0 ? rr_judge : rr;
+  const double rr0 = rr_plain0 >= 0.0 ? rr_plain0 : rr;
   const double abs2 = (double)a.abs_tol * a.abs_tol;
   const float rel_tol = a.rel_tol_dev ? *a.rel_tol_dev : a.rel_tol;
   const double rel2 = (double)rel_tol * rel_tol;
